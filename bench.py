@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""DGTD throughput benchmark: DOF-stage-updates/s of the fused LSERK4 step.
+
+Workload (the single-GPU configuration the metric is quoted on): the
+48^3 x 6 = 663,552-tet jittered box (+-10% h, seed 2024), order N=4 (Np=35),
+eps_r=4 sphere r=0.25 at the centre, Gaussian E_z pulse (sigma 0.05) at
+(0.3,0.4,0.5), upwind flux, PEC walls, LSERK4.  A step is one LSERK4 step (5
+RHS stages) over the whole mesh; n_dof = 139,345,920, so every step streams
+~2.3 GB per stage, far above the 126 MB L2 (no L2 flush is needed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+`--impl reference` times the CPU restatement of the reference's CPU path
+(oracle/, f64, all host threads) on a bounded sample of the same workload.
+Under torchrun each rank runs one replica of the workload (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_DOF_STAGE = {2: 18.8, 3: 17.4, 4: 16.8, 5: 16.5}
+FLOPS_PER_DOF_STAGE = {n: 6 * (n + 1) * (n + 2) * (n + 3) // 6 + 8 * (n + 1) * (n + 2) // 2 for n in range(1, 6)}
+METRIC = "DOF-stage-updates/s"
+
+
+def _rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic(kernel, order):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(f"{kernel}/N{order}")
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(steps, warmup, n_cells=24, order=4, threads=None):
+    """Oracle (f64 CPU restatement of explicit.rs + rhs.rs apply_into) on the
+    sphere_pulse workload at n_cells^3; returns (DOF-stage/s, info)."""
+    from oracle import oracle as R
+
+    from rapidfem_b200 import workloads as W
+
+    if threads:
+        R.set_threads(threads)
+    wl = W.sphere_pulse(n_cells, order)
+    orc = R.Operator(wl.mesh.nodes, wl.mesh.tets, order, 1.0, materials=wl.materials)
+    prod = wl.build()
+    y = wl.y0(prod)
+    rho, _ = orc.power_rho(8)
+    dt = 0.5 * 2.8 / rho
+    if warmup:
+        y = orc.lserk(y, dt, warmup)
+    t0 = time.perf_counter()
+    y = orc.lserk(y, dt, steps)
+    el = time.perf_counter() - t0
+    rate = orc.n_dof * 5 * steps / el
+    return rate, {"cores": R.threads(), "seconds": el, "n_dof": orc.n_dof, "steps": steps,
+                  "sample": f"sphere_pulse at {n_cells}^3 x 6 = {wl.mesh.n_tets} tets, N={order}, "
+                            f"{steps} LSERK4 steps (f64, OpenMP)"}
+
+
+def run_reference(args):
+    rank, world, _ = _rank()
+    if rank != 0:
+        return 0
+    steps, warmup = args.steps, args.warmup
+    rate, info = cpu_reference_rate(steps, warmup, n_cells=args.ref_cells)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "DOF-stage/s", "n_gpus": args.gpus,
+        "steps": steps, "warmup": warmup, "ms_per_step": info["seconds"] / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "sphere_pulse (jittered 48^3 box, N=4, eps_r=4 sphere, Gaussian Ez pulse)",
+                   "sample_cells": f"{args.ref_cells}^3", "order": 4, "integrator": "LSERK4"},
+        "cpu_baseline": {"value": rate, "unit": "DOF-stage/s", "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": rate, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "The reference's Rust CPU path cannot be built here (no Rust toolchain); timed is the "
+                "oracle's C restatement of explicit.rs:100-135 over rhs.rs:1262-1473.",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import torch
+
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    dist = world > 1
+    if dist:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    wl = W.sphere_pulse(args.cells, 4)
+    op = wl.build()
+    order = wl.order
+    ctx = G.GpuContext(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    gop = G.GpuOperator(ctx, op)
+    if args.engine:
+        gop.set_engine({"fp32": 0, "tf32x3": 1, "bf16x3": 2}[args.engine])
+    n = gop.n_dof()
+    y0 = wl.y0(op).astype(np.float32)
+
+    # spectral radius by power iteration on the device, dt = 0.5 * 2.8 / rho
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device=dev).manual_seed(0)
+        v = torch.randn(n, device=dev, dtype=torch.float32, generator=g)
+        v /= v.norm()
+        av = torch.empty_like(v)
+        rho = 1.0
+        for _ in range(args.power_iters):
+            gop.apply_device(v.data_ptr(), av.data_ptr())
+            rho = float(av.norm())
+            v = av / rho
+    torch.cuda.synchronize()
+    dt = 0.5 * 2.8 / rho
+
+    y_dev = torch.from_numpy(y0).to(dev)
+    gop.load_device(y_dev.data_ptr())
+    gop.run_lserk(dt, args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    gop.reset_launch_count()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    t_start.record(stream)
+    gop.run_lserk(dt, args.steps)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    ms = t_start.elapsed_time(t_end)
+    ck = clocks.stop()
+    launches = gop.launch_count()
+    yf = torch.empty(n, device=dev, dtype=torch.float32)
+    gop.store_device(yf.data_ptr())
+    torch.cuda.synchronize()
+    finite = bool(torch.isfinite(yf).all())
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t)
+
+    total_units = n * 5 * args.steps * world
+    value = total_units / (ms * 1e-3)
+    stage_ms = ms / (5 * args.steps)
+    alg_bytes = BYTES_PER_DOF_STAGE[order] * n
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    traffic = _traffic("rhs_fp32_lserk" if gop.engine == 0 else "rhs_tc_lserk", order)
+
+    # end to end through the public API with pinned host buffers
+    e2e_steps = args.steps
+    y_host = torch.from_numpy(y0).pin_memory().numpy()
+    probes = np.array([op.nearest_node_dof([0.5, 0.5, 0.5], 0, 2), op.nearest_node_dof([0.7, 0.4, 0.5], 1, 1)])
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    series, yfin = gop.transient_probes(y_host, dt, e2e_steps, 1, probes=probes)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t)
+    e2e_value = n * 5 * e2e_steps * world / (e2e_ms * 1e-3)
+    h2d = n * 4
+    d2h = n * 4 + series.nbytes
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sphere_pulse: jittered 48^3x6 box (663,552 tets), N=4, eps_r=4 sphere r=0.25, "
+                               "Gaussian Ez pulse sigma=0.05 at (0.3,0.4,0.5), upwind, PEC, LSERK4",
+                   "cells": f"{args.cells}^3", "order": order, "n_dof": n, "dt": dt,
+                   "engine": ["fp32", "tf32x3", "bf16x3"][gop.engine],
+                   "l2": "state 4*n_dof bytes per buffer >> 126 MB L2; no flush",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "rhs_fp32_kernel<N,LSERK>" if gop.engine == 0 else "rhs_tc_kernel<N,LSERK>",
+                     "alg_bytes_per_dof_stage": BYTES_PER_DOF_STAGE[order],
+                     "stage_ms": stage_ms, "peak_kind": peak_kind,
+                     "flops_per_dof_stage": FLOPS_PER_DOF_STAGE[order],
+                     "achieved_tflops": FLOPS_PER_DOF_STAGE[order] * n / (stage_ms * 1e-3) / 1e12},
+        "clocks": ck,
+        "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": h2d / e2e_steps,
+                "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
+                "api": "GpuOperator.transient_probes (dgtd_transient_probes): y0 in, probe series + final state out"},
+        "finite": finite,
+    }
+    if rank == 0 and not args.no_cpu:
+        rate, info = cpu_reference_rate(args.cpu_steps, 1, n_cells=args.ref_cells)
+        line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": info["cores"], "kind": "port",
+                                "sample": info["sample"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del gop
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=48)
+    ap.add_argument("--engine", default=None, choices=[None, "fp32", "tf32x3", "bf16x3"])
+    ap.add_argument("--power-iters", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--ref-cells", type=int, default=24)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

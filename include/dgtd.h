@@ -1,0 +1,176 @@
+/*
+ * dgtd.h -- C ABI of the B200 DGTD hot path (librapidfem_b200.so).
+ *
+ * The entry points replace rapidfem's OpenCL backend, the `GpuContext` /
+ * `GpuOperator` pair of crates/rapidfem-td/src/gpu/{mod.rs,operator.rs}, one
+ * for one: plain pointers and sizes, no C++ or torch types.  A Rust host binds
+ * them with an `extern "C"` block, a Python host with ctypes.
+ *
+ * State layout at the boundary is the reference's AoS layout
+ * `y[(e*Np + node)*6 + c]`, c = Ex,Ey,Ez,Hx,Hy,Hz (rhs.rs:492-497).  The device
+ * keeps its own element-major SoA copy; conversion happens on the device.
+ *
+ * Every call returns a dgtd_status; on failure `dgtd_last_error` gives the
+ * message (thread-local).  There is no CPU fallback: without a usable CUDA
+ * device the calls fail with DGTD_ERR_NO_DEVICE.
+ *
+ * Threading: one op per host thread at a time, like the reference's
+ * `unsendable` TdSession (python/src/td.rs:163).  All work of an op is
+ * issued on the op's stream (the context's stream by default).
+ */
+#ifndef DGTD_H
+#define DGTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DGTD_OK = 0,
+    DGTD_ERR_BAD_ARG = 1,     /* length / range / shape mismatch (reference: assert! panics) */
+    DGTD_ERR_CUDA = 2,        /* a CUDA runtime error (reference: "kernel launch failed: ...") */
+    DGTD_ERR_NONFINITE = 3,   /* a NaN/Inf met by a checked run */
+    DGTD_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    DGTD_ERR_NO_DEVICE = 5,   /* no CUDA device (reference: "no OpenCL GPU device found") */
+    DGTD_ERR_UNSUPPORTED = 6, /* order / feature outside what the kernels cover */
+    DGTD_ERR_OOM = 7,         /* device allocation failed */
+    DGTD_ERR_COLLAPSE = 8     /* adaptive step collapsed (reference: "GPU KCL: step size collapsed") */
+} dgtd_status;
+
+typedef struct dgtd_ctx dgtd_ctx;
+typedef struct dgtd_op dgtd_op;
+
+/* Copy the calling thread's last error message into buf (NUL-terminated). */
+int dgtd_last_error(char *buf, size_t len);
+
+/* Library / build identification: "rapidfem_b200 <version> sm_100a". */
+const char *dgtd_version(void);
+
+/* ---- context ----------------------------------------------------------
+ * Replaces GpuContext::new (crates/rapidfem-td/src/gpu/mod.rs:49): picks the
+ * CUDA device, creates the stream the ops run on. */
+int dgtd_ctx_create(int device, dgtd_ctx **out);
+int dgtd_ctx_destroy(dgtd_ctx *ctx);
+/* Device name (GpuContext::device_name, gpu/mod.rs:35). */
+int dgtd_ctx_device_name(dgtd_ctx *ctx, char *buf, size_t len);
+/* Run subsequent work of this context's ops on an external cudaStream_t
+ * (NULL restores the context's own stream). */
+int dgtd_ctx_set_stream(dgtd_ctx *ctx, void *cuda_stream);
+/* Block until the context's stream is idle. */
+int dgtd_ctx_synchronize(dgtd_ctx *ctx);
+
+/* ---- operator ---------------------------------------------------------
+ * The arrays GpuOperator::new flattens (gpu/operator.rs:222-292), in f64 as
+ * the CPU operator holds them; the device copy is narrowed / split by the
+ * library.  Np = (N+1)(N+2)(N+3)/6, Nfp = (N+1)(N+2)/2, K = n_elem. */
+typedef struct {
+    int32_t order;               /* N, 1..5 */
+    int32_t n_elem;              /* K */
+    double flux_alpha;           /* 0 central, 1 upwind (session.rs:93-99) */
+    const double *diff_r;        /* Np*Np row-major, dg_basis.rs:100-102 */
+    const double *diff_s;
+    const double *diff_t;
+    const double *lift;          /* Np*(4*Nfp) row-major, dg_basis.rs:383 */
+    const int32_t *face_nodes;   /* 4*Nfp volume-node ids per face, dg_basis.rs:316-323 */
+    const double *jinv;          /* 9K, J^-1[i][k] row-major, geom_factors.rs:81-88 */
+    const double *inv_eps;       /* 3K, rhs.rs:900-926 */
+    const double *inv_mu;        /* 3K */
+    const double *sigma_eps;     /* 3K */
+    const double *sigma_mu;      /* 3K */
+    const double *face_normal;   /* 12K outward unit normals, topology.rs:64-78 */
+    const double *face_fscale;   /* 4K, 2*area/|det J|, rhs.rs:828 */
+    const int32_t *face_neighbor;  /* 4K, -1 = boundary */
+    const int32_t *face_nbr_local; /* 4K */
+    const int32_t *face_port;      /* 4K, -1 = none (non-port boundary = PEC) */
+    const int32_t *face_perm;      /* 4K*Nfp neighbour face-node match, rhs.rs:546-566 */
+} dgtd_op_desc;
+
+/* Contraction engine of the RHS kernels. */
+typedef enum {
+    DGTD_ENGINE_FP32 = 0,      /* FP32 FMA on the CUDA cores (default) */
+    DGTD_ENGINE_TF32X3 = 1,    /* 3xTF32 split products on tcgen05 tensor cores, FP32 accumulate */
+    DGTD_ENGINE_BF16X3 = 2     /* split-BF16 (hi*hi + hi*lo + lo*hi) on tcgen05, FP32 accumulate */
+} dgtd_engine;
+
+/* GpuOperator::new (gpu/operator.rs:207). Uploads the operator once. */
+int dgtd_op_create(dgtd_ctx *ctx, const dgtd_op_desc *desc, dgtd_op **out);
+int dgtd_op_destroy(dgtd_op *op);
+/* GpuOperator::n_dof (gpu/operator.rs:430): 6*Np*K. */
+int dgtd_op_n_dof(const dgtd_op *op, int64_t *n_dof);
+/* Select the contraction engine; fails with DGTD_ERR_UNSUPPORTED if this
+ * order has no kernel for it. */
+int dgtd_op_set_engine(dgtd_op *op, int engine);
+int dgtd_op_get_engine(const dgtd_op *op, int *engine);
+
+/* GpuOperator::apply (gpu/operator.rs:513): dy = A*y, host f32 buffers of
+ * n_dof, AoS layout. */
+int dgtd_apply(dgtd_op *op, const float *y, float *dy);
+
+/* Drive of a transient, session.rs:107-114 (Drive::{Free,Point,Vector}). */
+typedef enum { DGTD_DRIVE_FREE = 0, DGTD_DRIVE_POINT = 1, DGTD_DRIVE_VECTOR = 2 } dgtd_drive;
+
+/* GpuOperator::transient (gpu/operator.rs:906): `steps` frames of `dt`, each
+ * `substeps` LSERK4 steps of dt/substeps, the source b*g held per substep
+ * with g = g_samples[k*substeps + j] (steps*substeps samples; NULL for a
+ * free run).  src_dof is the point DOF (DRIVE_POINT), src_vec the n_dof
+ * pattern (DRIVE_VECTOR).  With record != 0, `out` receives the trajectory
+ * [(steps+1)*n_dof] (row 0 = y0); else the final state [n_dof]. */
+int dgtd_transient(dgtd_op *op, const float *y0, float dt, int64_t steps, int64_t substeps,
+                   int drive, int64_t src_dof, const double *src_vec, const float *g_samples,
+                   int record, float *out);
+
+/* As dgtd_transient, but recording only the DOFs `probes[n_probes]` per frame
+ * into out[(steps+1)*n_probes] and the final state into y_final[n_dof]
+ * (either may be NULL).  The session's Record::Dofs (session.rs:117-124). */
+int dgtd_transient_probes(dgtd_op *op, const float *y0, float dt, int64_t steps,
+                          int64_t substeps, int drive, int64_t src_dof, const double *src_vec,
+                          const float *g_samples, const int64_t *probes, int64_t n_probes,
+                          float *out, float *y_final);
+
+/* GpuOperator::expmv (gpu/operator.rs:1175): exp(t*A)*v by Arnoldi, f64 basis
+ * and CGS2 on the device, sub-stepped into chunks of <= 12 (KRYLOV_CHUNK).
+ * With tol > 0 each chunk also stops on the a-posteriori estimate
+ * h_{j+1,j}*|exp(tH)_{d-1,0}| < tol (propagator.rs:278-294); tol = 0 is the
+ * reference GPU's fixed-dimension behaviour.  `dim_used` (may be NULL)
+ * receives the summed Krylov dimension. */
+int dgtd_expmv(dgtd_op *op, const double *v, double t, int32_t m, double tol, double *out,
+               int32_t *dim_used);
+
+/* GpuOperator::etd_step (gpu/operator.rs:1267): exp(hA)y + h*phi1(hA)*b by the
+ * augmented Arnoldi, the augmented scalar kept on the device. */
+int dgtd_etd_step(dgtd_op *op, const double *y, const double *b, double h, int32_t m,
+                  double tol, double *out, int32_t *dim_used);
+
+/* ---- device-resident state (no host copies) ---------------------------
+ * The op owns a resident f32 state (the reference's `y` buffer). */
+int dgtd_state_upload(dgtd_op *op, const float *y);        /* host AoS -> device state */
+int dgtd_state_download(dgtd_op *op, float *y);            /* device state -> host AoS */
+int dgtd_state_load_device(dgtd_op *op, const float *d_y); /* device AoS pointer -> state */
+int dgtd_state_store_device(dgtd_op *op, float *d_y);      /* state -> device AoS pointer */
+/* `steps` LSERK4 steps of `h` on the resident state; drive as dgtd_transient
+ * with g_samples on the HOST (steps entries, NULL for free). */
+int dgtd_run_lserk(dgtd_op *op, float h, int64_t steps, int drive, int64_t src_dof,
+                   const float *g_samples);
+/* Upload the DRIVE_VECTOR pattern used by dgtd_run_lserk. */
+int dgtd_set_source_vector(dgtd_op *op, const double *src_vec);
+/* dy = A*y on device AoS pointers (f32). */
+int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
+
+/* ---- statistics -------------------------------------------------------- */
+/* Kernel launches issued by this op since creation / the last reset. */
+int dgtd_op_launch_count(const dgtd_op *op, int64_t *count);
+int dgtd_op_reset_launch_count(dgtd_op *op);
+
+/* ---- test hooks --------------------------------------------------------
+ * Dense exp(A) of a d x d row-major matrix (d <= 64) by the device kernel the
+ * Krylov finisher uses (Taylor-18 + scaling and squaring, propagator.rs:69-114). */
+int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGTD_H */

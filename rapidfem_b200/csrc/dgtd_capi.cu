@@ -1,0 +1,807 @@
+// dgtd_capi.cu -- the C ABI of include/dgtd.h: context, device operator,
+// apply / LSERK4 transient / Krylov expmv / ETD step on the B200.
+//
+// Replaces gpu/mod.rs (GpuContext) and gpu/operator.rs (GpuOperator) of
+// crates/rapidfem-td.  The operator arrays are uploaded once
+// (gpu/operator.rs:222-292) into the element-major SoA layout described in
+// dgtd_common.cuh; every run keeps the state resident and converts to the
+// reference's AoS layout only at the boundary.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dgtd.h"
+#include "dgtd_common.cuh"
+#include "host/errors.h"
+#include "krylov.cuh"
+#include "rhs_fp32.cuh"
+
+// ------------------------------------------------------------------ errors
+
+namespace dgtd {
+static thread_local std::string g_last_error;
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+}  // namespace dgtd
+
+using dgtd::set_error;
+
+#define CUDA_TRY(expr)                                                                      \
+  do {                                                                                      \
+    cudaError_t err__ = (expr);                                                             \
+    if (err__ != cudaSuccess)                                                               \
+      return set_error(err__ == cudaErrorMemoryAllocation ? DGTD_ERR_OOM : DGTD_ERR_CUDA,   \
+                       std::string(#expr) + ": " + cudaGetErrorString(err__));              \
+  } while (0)
+
+#define DGTD_TRY(expr)            \
+  do {                            \
+    int st__ = (expr);            \
+    if (st__ != DGTD_OK) return st__; \
+  } while (0)
+
+extern "C" int dgtd_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return DGTD_ERR_BAD_ARG;
+  std::snprintf(buf, len, "%s", dgtd::g_last_error.c_str());
+  return DGTD_OK;
+}
+
+extern "C" const char* dgtd_version(void) { return "rapidfem_b200 0.1.0 sm_100a"; }
+
+// ------------------------------------------------------------------ context
+
+struct dgtd_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  std::string name;
+};
+
+extern "C" int dgtd_ctx_create(int device, dgtd_ctx** out) {
+  if (!out) return set_error(DGTD_ERR_BAD_ARG, "ctx_create: null out");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return set_error(DGTD_ERR_NO_DEVICE, std::string("no CUDA device found") +
+                                             (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : ""));
+  if (device < 0 || device >= count) return set_error(DGTD_ERR_BAD_ARG, "ctx_create: device index out of range");
+  CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return set_error(DGTD_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (built for sm_100a only)");
+  auto* c = new dgtd_ctx;
+  c->device = device;
+  c->num_sms = prop.multiProcessorCount;
+  c->name = prop.name;
+  cudaError_t se = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (se != cudaSuccess) {
+    delete c;
+    return set_error(DGTD_ERR_CUDA, std::string("stream create: ") + cudaGetErrorString(se));
+  }
+  c->stream = c->own;
+  *out = c;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_ctx_destroy(dgtd_ctx* c) {
+  if (!c) return DGTD_OK;
+  cudaSetDevice(c->device);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_ctx_device_name(dgtd_ctx* c, char* buf, size_t len) {
+  if (!c || !buf || !len) return set_error(DGTD_ERR_BAD_ARG, "ctx_device_name: bad argument");
+  std::snprintf(buf, len, "%s", c->name.c_str());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_ctx_set_stream(dgtd_ctx* c, void* s) {
+  if (!c) return set_error(DGTD_ERR_BAD_ARG, "ctx_set_stream: null ctx");
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_ctx_synchronize(dgtd_ctx* c) {
+  if (!c) return set_error(DGTD_ERR_BAD_ARG, "ctx_synchronize: null ctx");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ operator
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (n >= count && p) return DGTD_OK;
+    free();
+    if (count == 0) return DGTD_OK;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return set_error(DGTD_ERR_OOM, std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) +
+                                         " bytes): " + cudaGetErrorString(e));
+    }
+    n = count;
+    return DGTD_OK;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct dgtd_op {
+  dgtd_ctx* ctx = nullptr;
+  int order = 0, np = 0, nfp = 0;
+  int64_t n_elem = 0, n_dof = 0;
+  float alpha = 1.f;
+  int engine = DGTD_ENGINE_FP32;
+  int64_t launches = 0;
+  // operator data
+  DevBuf<float> meta, dT, liftT;
+  DevBuf<uint8_t> fnodes, gtab;
+  int n_gather = 0;
+  // state
+  DevBuf<float> y[2], p, src_vec, aos32;
+  int cur = 0;
+  bool src_vec_set = false;
+  // Krylov
+  DevBuf<double> basis, w, partials, src64, tmp64, vin64;
+  DevBuf<dgtd::KrylovDev> kst;
+  DevBuf<int> skip;
+  int kry_cap = 0;
+
+  cudaStream_t stream() const { return ctx->stream; }
+  ~dgtd_op() {
+    cudaSetDevice(ctx->device);
+    meta.free(); dT.free(); liftT.free(); fnodes.free(); gtab.free();
+    y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
+    basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
+    kst.free(); skip.free();
+  }
+};
+
+namespace {
+
+using namespace dgtd;
+
+// ---- layout conversion (AoS y[(e*Np+i)*6+c] <-> SoA y[(e*6+c)*Np+i])
+template <class TI, class TO>
+__global__ void k_aos_to_soa(const TI* __restrict__ aos, TO* __restrict__ soa, int64_t n, int np) {
+  const int64_t per = 6LL * np;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = idx / per;
+    const int r = (int)(idx - e * per);
+    const int c = r / np, i = r - c * np;
+    soa[idx] = (TO)aos[(e * np + i) * 6 + c];
+  }
+}
+template <class TI, class TO>
+__global__ void k_soa_to_aos(const TI* __restrict__ soa, TO* __restrict__ aos, int64_t n, int np) {
+  const int64_t per = 6LL * np;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = idx / per;
+    const int r = (int)(idx - e * per);
+    const int i = r / 6, c = r - i * 6;
+    aos[idx] = (TO)soa[(e * 6 + c) * np + i];
+  }
+}
+__global__ void k_gather_f32(const float* __restrict__ src, const int64_t* __restrict__ idx,
+                             int64_t n, float* __restrict__ out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    out[k] = src[idx[k]];
+}
+
+int grid_for(int64_t n, int threads, int num_sms) {
+  int64_t g = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)num_sms * 8));
+}
+
+int64_t aos_to_soa_index(int64_t dof, int np) {
+  const int64_t per = 6LL * np;
+  const int64_t e = dof / per;
+  const int r = (int)(dof - e * per);
+  const int i = r / 6, c = r - i * 6;
+  return (e * 6 + c) * np + i;
+}
+
+template <class TI, class TO>
+int to_soa(dgtd_op* op, const TI* aos, TO* soa) {
+  k_aos_to_soa<TI, TO><<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(aos, soa, op->n_dof, op->np);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+template <class TI, class TO>
+int to_aos(dgtd_op* op, const TI* soa, TO* aos) {
+  k_soa_to_aos<TI, TO><<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(soa, aos, op->n_dof, op->np);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+// ---- RHS kernel dispatch
+template <int N, int MODE>
+int launch_rhs_n(dgtd_op* op, const RhsParams& P) {
+  using C = Fp32Cfg<N>;
+  static int blocks_per_sm[8] = {0};
+  auto kern = rhs_fp32_kernel<N, MODE>;
+  int& bps = blocks_per_sm[op->ctx->device & 7];
+  if (bps == 0) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, C::THREADS, C::SMEM));
+    if (bps < 1) return set_error(DGTD_ERR_CUDA, "rhs kernel does not fit on an SM");
+  }
+  OpTables T{op->dT.p, op->liftT.p, op->fnodes.p, op->gtab.p, op->n_gather};
+  const int64_t tiles = (op->n_elem + C::E - 1) / C::E;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms * bps);
+  kern<<<grid, C::THREADS, C::SMEM, op->stream()>>>(P, T);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+template <int MODE>
+int launch_rhs(dgtd_op* op, const RhsParams& P) {
+  switch (op->order) {
+    case 1: return launch_rhs_n<1, MODE>(op, P);
+    case 2: return launch_rhs_n<2, MODE>(op, P);
+    case 3: return launch_rhs_n<3, MODE>(op, P);
+    case 4: return launch_rhs_n<4, MODE>(op, P);
+    case 5: return launch_rhs_n<5, MODE>(op, P);
+    default: return set_error(DGTD_ERR_UNSUPPORTED, "order outside 1..5");
+  }
+}
+
+RhsParams base_params(dgtd_op* op) {
+  RhsParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.meta = op->meta.p;
+  P.n_elem = op->n_elem;
+  P.src_idx = -1;
+  P.alpha = op->alpha;
+  return P;
+}
+
+const double kLserkA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                           -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kLserkB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                           1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                           2277821191437.0 / 14882151754819.0};
+
+// One LSERK4 step of h on the resident state (explicit.rs:100-135; the
+// residual register restarts at zero each step because a_0 = 0).
+int lserk_step(dgtd_op* op, float h, int64_t src_idx, float g, const float* src_vec) {
+  for (int s = 0; s < 5; ++s) {
+    RhsParams P = base_params(op);
+    P.y_in = op->y[op->cur].p;
+    P.out = op->y[op->cur ^ 1].p;
+    P.p = op->p.p;
+    P.a = (float)kLserkA[s];
+    P.b = (float)kLserkB[s];
+    P.dt = h;
+    P.read_p = s > 0;
+    P.write_p = s < 4;
+    P.src_idx = src_idx;
+    P.src_vec = src_vec;
+    P.src_g = g;
+    DGTD_TRY(launch_rhs<kModeLserk>(op, P));
+    op->cur ^= 1;
+  }
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** out) {
+  if (!ctx || !d || !out) return set_error(DGTD_ERR_BAD_ARG, "op_create: null argument");
+  if (d->order < 1 || d->order > 5) return set_error(DGTD_ERR_UNSUPPORTED, "op_create: order must be 1..5");
+  if (d->n_elem < 1) return set_error(DGTD_ERR_BAD_ARG, "op_create: n_elem must be >= 1");
+  if (!d->diff_r || !d->diff_s || !d->diff_t || !d->lift || !d->face_nodes || !d->jinv || !d->inv_eps ||
+      !d->inv_mu || !d->sigma_eps || !d->sigma_mu || !d->face_normal || !d->face_fscale ||
+      !d->face_neighbor || !d->face_nbr_local || !d->face_port || !d->face_perm)
+    return set_error(DGTD_ERR_BAD_ARG, "op_create: a descriptor array is null");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const int N = d->order, np = dgtd::np_of(N), nfp = dgtd::nfp_of(N);
+  const int64_t K = d->n_elem;
+  // Host-side packing: element records, gather tables.
+  std::vector<float> meta((size_t)K * dgtd::kMetaWords, 0.f);
+  std::map<std::vector<uint8_t>, int> table_id;
+  std::vector<uint8_t> gtab;
+  for (int f = 0; f < 4; ++f)
+    for (int m = 0; m < nfp; ++m)
+      if (d->face_nodes[f * nfp + m] < 0 || d->face_nodes[f * nfp + m] >= np)
+        return set_error(DGTD_ERR_BAD_ARG, "op_create: face_nodes entry out of range");
+  for (int64_t e = 0; e < K; ++e) {
+    float* M = &meta[(size_t)e * dgtd::kMetaWords];
+    for (int q = 0; q < 9; ++q) M[q] = (float)d->jinv[9 * e + q];
+    for (int q = 0; q < 12; ++q) M[9 + q] = (float)d->face_normal[12 * e + q];
+    for (int q = 0; q < 4; ++q) M[21 + q] = (float)d->face_fscale[4 * e + q];
+    for (int c = 0; c < 3; ++c) {
+      M[25 + c] = (float)d->inv_eps[3 * e + c];
+      M[28 + c] = (float)d->inv_mu[3 * e + c];
+      M[31 + c] = (float)d->sigma_eps[3 * e + c];
+      M[34 + c] = (float)d->sigma_mu[3 * e + c];
+    }
+    uint32_t codes[4];
+    for (int f = 0; f < 4; ++f) {
+      const int64_t ef = 4 * e + f;
+      const int nbr = d->face_neighbor[ef];
+      int32_t nb_bits = nbr;
+      int kind, id = 0;
+      if (d->face_port[ef] >= 0) {
+        kind = dgtd::kPort;
+      } else if (nbr < 0) {
+        kind = dgtd::kPec;
+        nb_bits = -1;
+      } else {
+        if (nbr >= K) return set_error(DGTD_ERR_BAD_ARG, "op_create: face_neighbor out of range");
+        const int fn = d->face_nbr_local[ef];
+        if (fn < 0 || fn > 3) return set_error(DGTD_ERR_BAD_ARG, "op_create: face_nbr_local out of range");
+        kind = dgtd::kInterior;
+        std::vector<uint8_t> list(nfp);
+        for (int m = 0; m < nfp; ++m) {
+          const int pm = d->face_perm[ef * nfp + m];
+          if (pm < 0 || pm >= nfp) return set_error(DGTD_ERR_BAD_ARG, "op_create: face_perm out of range");
+          list[m] = (uint8_t)d->face_nodes[fn * nfp + pm];
+        }
+        auto it = table_id.find(list);
+        if (it == table_id.end()) {
+          if ((int)table_id.size() >= dgtd::kMaxGather)
+            return set_error(DGTD_ERR_UNSUPPORTED, "op_create: more than 96 distinct face-node matchings");
+          id = (int)table_id.size();
+          table_id.emplace(list, id);
+          gtab.insert(gtab.end(), list.begin(), list.end());
+        } else {
+          id = it->second;
+        }
+      }
+      std::memcpy(&M[37 + f], &nb_bits, 4);
+      codes[f] = (uint32_t)id | ((uint32_t)kind << 8);
+    }
+    const uint32_t w0 = codes[0] | (codes[1] << 16), w1 = codes[2] | (codes[3] << 16);
+    std::memcpy(&M[41], &w0, 4);
+    std::memcpy(&M[42], &w1, 4);
+  }
+  std::vector<float> dT((size_t)3 * np * np), liftT((size_t)4 * nfp * np);
+  const double* D[3] = {d->diff_r, d->diff_s, d->diff_t};
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < np; ++i)
+      for (int j = 0; j < np; ++j) dT[((size_t)k * np + j) * np + i] = (float)D[k][i * np + j];
+  for (int i = 0; i < np; ++i)
+    for (int s = 0; s < 4 * nfp; ++s) liftT[(size_t)s * np + i] = (float)d->lift[i * 4 * nfp + s];
+  std::vector<uint8_t> fnodes(4 * nfp);
+  for (int q = 0; q < 4 * nfp; ++q) fnodes[q] = (uint8_t)d->face_nodes[q];
+  if (gtab.empty()) gtab.assign(nfp, 0);
+
+  auto* op = new dgtd_op;
+  op->ctx = ctx;
+  op->order = N;
+  op->np = np;
+  op->nfp = nfp;
+  op->n_elem = K;
+  op->n_dof = 6 * (int64_t)np * K;
+  op->alpha = (float)d->flux_alpha;
+  op->n_gather = (int)table_id.size();
+  auto fail = [&](int code) { delete op; return code; };
+  int st;
+  if ((st = op->meta.alloc(meta.size())) || (st = op->dT.alloc(dT.size())) || (st = op->liftT.alloc(liftT.size())) ||
+      (st = op->fnodes.alloc(fnodes.size())) || (st = op->gtab.alloc(gtab.size())) ||
+      (st = op->y[0].alloc(op->n_dof + 4)) || (st = op->y[1].alloc(op->n_dof + 4)) || (st = op->p.alloc(op->n_dof + 4)))
+    return fail(st);
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  if (!e) e = cudaMemcpyAsync(op->meta.p, meta.data(), meta.size() * 4, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->dT.p, dT.data(), dT.size() * 4, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->liftT.p, liftT.data(), liftT.size() * 4, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->fnodes.p, fnodes.data(), fnodes.size(), cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->gtab.p, gtab.data(), gtab.size(), cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemsetAsync(op->y[0].p, 0, op->y[0].n * 4, s);
+  if (!e) e = cudaMemsetAsync(op->y[1].p, 0, op->y[1].n * 4, s);
+  if (!e) e = cudaMemsetAsync(op->p.p, 0, op->p.n * 4, s);
+  if (!e) e = cudaStreamSynchronize(s);
+  if (e) {
+    set_error(DGTD_ERR_CUDA, std::string("op_create upload: ") + cudaGetErrorString(e));
+    return fail(DGTD_ERR_CUDA);
+  }
+  *out = op;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_destroy(dgtd_op* op) {
+  delete op;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_n_dof(const dgtd_op* op, int64_t* n) {
+  if (!op || !n) return set_error(DGTD_ERR_BAD_ARG, "op_n_dof: null argument");
+  *n = op->n_dof;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_set_engine(dgtd_op* op, int engine) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_set_engine: null op");
+  if (engine == DGTD_ENGINE_FP32) {
+    op->engine = engine;
+    return DGTD_OK;
+  }
+  return set_error(DGTD_ERR_UNSUPPORTED, "op_set_engine: engine not available for this order");
+}
+
+extern "C" int dgtd_op_get_engine(const dgtd_op* op, int* engine) {
+  if (!op || !engine) return set_error(DGTD_ERR_BAD_ARG, "op_get_engine: null argument");
+  *engine = op->engine;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_launch_count(const dgtd_op* op, int64_t* count) {
+  if (!op || !count) return set_error(DGTD_ERR_BAD_ARG, "op_launch_count: null argument");
+  *count = op->launches;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_reset_launch_count(dgtd_op* op) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_reset_launch_count: null op");
+  op->launches = 0;
+  return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ state
+
+static int ensure_aos32(dgtd_op* op) { return op->aos32.alloc(op->n_dof + 4); }
+
+extern "C" int dgtd_state_load_device(dgtd_op* op, const float* d_y) {
+  if (!op || !d_y) return set_error(DGTD_ERR_BAD_ARG, "state_load_device: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  return to_soa<float, float>(op, d_y, op->y[op->cur].p);
+}
+
+extern "C" int dgtd_state_store_device(dgtd_op* op, float* d_y) {
+  if (!op || !d_y) return set_error(DGTD_ERR_BAD_ARG, "state_store_device: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  return to_aos<float, float>(op, op->y[op->cur].p, d_y);
+}
+
+extern "C" int dgtd_state_upload(dgtd_op* op, const float* y) {
+  if (!op || !y) return set_error(DGTD_ERR_BAD_ARG, "state_upload: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(ensure_aos32(op));
+  CUDA_TRY(cudaMemcpyAsync(op->aos32.p, y, op->n_dof * 4, cudaMemcpyHostToDevice, op->stream()));
+  return to_soa<float, float>(op, op->aos32.p, op->y[op->cur].p);
+}
+
+extern "C" int dgtd_state_download(dgtd_op* op, float* y) {
+  if (!op || !y) return set_error(DGTD_ERR_BAD_ARG, "state_download: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(ensure_aos32(op));
+  DGTD_TRY((to_aos<float, float>(op, op->y[op->cur].p, op->aos32.p)));
+  CUDA_TRY(cudaMemcpyAsync(y, op->aos32.p, op->n_dof * 4, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_set_source_vector(dgtd_op* op, const double* src) {
+  if (!op || !src) return set_error(DGTD_ERR_BAD_ARG, "set_source_vector: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(op->src_vec.alloc(op->n_dof + 4));
+  DGTD_TRY(op->tmp64.alloc(op->n_dof));
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, src, op->n_dof * 8, cudaMemcpyHostToDevice, op->stream()));
+  DGTD_TRY((to_soa<double, float>(op, op->tmp64.p, op->src_vec.p)));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  op->src_vec_set = true;
+  return DGTD_OK;
+}
+
+static int check_drive(dgtd_op* op, int drive, int64_t src_dof, const float* g, int64_t n_samples,
+                       int64_t* src_idx) {
+  *src_idx = -1;
+  if (drive == DGTD_DRIVE_FREE) return DGTD_OK;
+  if (!g && n_samples > 0) return set_error(DGTD_ERR_BAD_ARG, "a driven run needs waveform samples");
+  if (drive == DGTD_DRIVE_POINT) {
+    if (src_dof < 0 || src_dof >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "source DOF " + std::to_string(src_dof) + " out of range (n_dof = " +
+                                             std::to_string(op->n_dof) + ")");
+    *src_idx = aos_to_soa_index(src_dof, op->np);
+    return DGTD_OK;
+  }
+  if (drive == DGTD_DRIVE_VECTOR) {
+    if (!op->src_vec_set) return set_error(DGTD_ERR_BAD_ARG, "vector drive without a source vector");
+    return DGTD_OK;
+  }
+  return set_error(DGTD_ERR_BAD_ARG, "unknown drive kind");
+}
+
+extern "C" int dgtd_run_lserk(dgtd_op* op, float h, int64_t steps, int drive, int64_t src_dof,
+                              const float* g) {
+  if (!op || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "run_lserk: bad argument");
+  if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk: step must be positive");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g, steps, &src_idx));
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  for (int64_t k = 0; k < steps; ++k) {
+    const float gk = drive == DGTD_DRIVE_FREE ? 0.f : g[k];
+    DGTD_TRY(lserk_step(op, h, src_idx, gk, sv));
+  }
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_apply_device(dgtd_op* op, const float* d_y, float* d_dy) {
+  if (!op || !d_y || !d_dy) return set_error(DGTD_ERR_BAD_ARG, "apply_device: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(op->aos32.alloc(op->n_dof + 4));
+  // state scratch: y[cur^1] holds the SoA input, p the SoA output (the
+  // resident state y[cur] is left untouched).
+  DGTD_TRY((to_soa<float, float>(op, d_y, op->y[op->cur ^ 1].p)));
+  RhsParams P = base_params(op);
+  P.y_in = op->y[op->cur ^ 1].p;
+  P.out = op->p.p;
+  DGTD_TRY(launch_rhs<kModeApply>(op, P));
+  return to_aos<float, float>(op, op->p.p, d_dy);
+}
+
+extern "C" int dgtd_apply(dgtd_op* op, const float* y, float* dy) {
+  if (!op || !y || !dy) return set_error(DGTD_ERR_BAD_ARG, "apply: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(op->tmp64.alloc((op->n_dof + 1) / 2 + 2));  // f32 AoS input staging (reuses f64 scratch)
+  float* d_in = reinterpret_cast<float*>(op->tmp64.p);
+  DGTD_TRY(op->aos32.alloc(op->n_dof + 4));
+  CUDA_TRY(cudaMemcpyAsync(d_in, y, op->n_dof * 4, cudaMemcpyHostToDevice, op->stream()));
+  DGTD_TRY(dgtd_apply_device(op, d_in, op->aos32.p));
+  CUDA_TRY(cudaMemcpyAsync(dy, op->aos32.p, op->n_dof * 4, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_transient_probes(dgtd_op* op, const float* y0, float dt, int64_t steps,
+                                     int64_t substeps, int drive, int64_t src_dof,
+                                     const double* src_vec, const float* g,
+                                     const int64_t* probes, int64_t n_probes, float* out,
+                                     float* y_final) {
+  if (!op || !y0 || steps < 0 || n_probes < 0 || (n_probes > 0 && (!probes || !out)))
+    return set_error(DGTD_ERR_BAD_ARG, "transient_probes: bad argument");
+  if (!(std::isfinite(dt) && dt > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "dt must be positive");
+  substeps = std::max<int64_t>(substeps, 1);
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (drive == DGTD_DRIVE_VECTOR) {
+    if (!src_vec) return set_error(DGTD_ERR_BAD_ARG, "vector drive without src_vec");
+    DGTD_TRY(dgtd_set_source_vector(op, src_vec));
+  }
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g, steps * substeps, &src_idx));
+  DevBuf<int64_t> d_probe;
+  DevBuf<float> d_pv;
+  std::vector<int64_t> pidx(n_probes);
+  for (int64_t q = 0; q < n_probes; ++q) {
+    if (probes[q] < 0 || probes[q] >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "probe DOF " + std::to_string(probes[q]) + " out of range");
+    pidx[q] = aos_to_soa_index(probes[q], op->np);
+  }
+  if (n_probes > 0) {
+    DGTD_TRY(d_probe.alloc(n_probes));
+    DGTD_TRY(d_pv.alloc((size_t)(steps + 1) * n_probes));
+    CUDA_TRY(cudaMemcpyAsync(d_probe.p, pidx.data(), n_probes * 8, cudaMemcpyHostToDevice, op->stream()));
+  }
+  DGTD_TRY(dgtd_state_upload(op, y0));
+  auto record = [&](int64_t row) -> int {
+    if (n_probes == 0) return DGTD_OK;
+    k_gather_f32<<<grid_for(n_probes, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(
+        op->y[op->cur].p, d_probe.p, n_probes, d_pv.p + row * n_probes);
+    op->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return DGTD_OK;
+  };
+  int st = record(0);
+  const float h = dt / (float)substeps;
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  for (int64_t k = 0; k < steps && st == DGTD_OK; ++k) {
+    for (int64_t j = 0; j < substeps && st == DGTD_OK; ++j) {
+      const float gk = drive == DGTD_DRIVE_FREE ? 0.f : g[k * substeps + j];
+      st = lserk_step(op, h, src_idx, gk, sv);
+    }
+    if (st == DGTD_OK) st = record(k + 1);
+  }
+  if (st == DGTD_OK && n_probes > 0) {
+    cudaError_t e = cudaMemcpyAsync(out, d_pv.p, (size_t)(steps + 1) * n_probes * 4, cudaMemcpyDeviceToHost, op->stream());
+    if (e) st = set_error(DGTD_ERR_CUDA, std::string("probe download: ") + cudaGetErrorString(e));
+  }
+  if (st == DGTD_OK && y_final) st = dgtd_state_download(op, y_final);
+  cudaError_t e = cudaStreamSynchronize(op->stream());
+  d_probe.free();
+  d_pv.free();
+  if (st != DGTD_OK) return st;
+  CUDA_TRY(e);
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t steps, int64_t substeps,
+                              int drive, int64_t src_dof, const double* src_vec, const float* g,
+                              int record, float* out) {
+  if (!op || !y0 || !out || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "transient: bad argument");
+  if (!(std::isfinite(dt) && dt > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "dt must be positive");
+  substeps = std::max<int64_t>(substeps, 1);
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (drive == DGTD_DRIVE_VECTOR) {
+    if (!src_vec) return set_error(DGTD_ERR_BAD_ARG, "vector drive without src_vec");
+    DGTD_TRY(dgtd_set_source_vector(op, src_vec));
+  }
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g, steps * substeps, &src_idx));
+  DGTD_TRY(dgtd_state_upload(op, y0));
+  const float h = dt / (float)substeps;
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  if (record) std::memcpy(out, y0, op->n_dof * 4);
+  for (int64_t k = 0; k < steps; ++k) {
+    for (int64_t j = 0; j < substeps; ++j) {
+      const float gk = drive == DGTD_DRIVE_FREE ? 0.f : g[k * substeps + j];
+      DGTD_TRY(lserk_step(op, h, src_idx, gk, sv));
+    }
+    if (record) DGTD_TRY(dgtd_state_download(op, out + (k + 1) * op->n_dof));
+  }
+  if (!record) DGTD_TRY(dgtd_state_download(op, out));
+  return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ Krylov
+
+namespace {
+
+int ensure_krylov(dgtd_op* op, int m) {
+  if (m > dgtd::kKrylovMaxDim) return set_error(DGTD_ERR_UNSUPPORTED, "Krylov chunk dimension above 64");
+  if (op->kry_cap < m) {
+    DGTD_TRY(op->basis.alloc((size_t)(m + 1) * op->n_dof));
+    op->kry_cap = m;
+  }
+  DGTD_TRY(op->w.alloc(op->n_dof));
+  DGTD_TRY(op->partials.alloc((size_t)dgtd::kKrylovBlocks * dgtd::kKrylovMaxDim));
+  DGTD_TRY(op->kst.alloc(1));
+  DGTD_TRY(op->skip.alloc(1));
+  DGTD_TRY(op->vin64.alloc(op->n_dof));
+  DGTD_TRY(op->tmp64.alloc(op->n_dof));
+  static bool attr = false;
+  if (!attr) {
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_expm_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
+    attr = true;
+  }
+  return DGTD_OK;
+}
+
+// One Arnoldi chunk: out = first n components of exp(t*Aug)[v; 1] (aug) or
+// exp(t*A) v, from the SoA f64 vector `v` (device).  dim_out gets the dimension.
+int krylov_chunk(dgtd_op* op, const double* v, double t, int m, double tol, bool aug, double* out,
+                 int* dim_out) {
+  using namespace dgtd;
+  cudaStream_t s = op->stream();
+  const int64_t n = op->n_dof;
+  const int nb = kKrylovBlocks, nt = kKrylovThreads;
+  const int gs = grid_for(n, 256, op->ctx->num_sms);
+  KrylovDev* st = op->kst.p;
+  double* V = op->basis.p;
+  CUDA_TRY(cudaMemsetAsync(op->skip.p, 0, sizeof(int), s));
+  k_norm_partials<<<nb, nt, 0, s>>>(v, n, op->partials.p);
+  k_finish_start<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, t, tol, aug ? 1 : 0, m);
+  k_scale<<<gs, 256, 0, s>>>(v, n, &st->inv_beta, V, nullptr);
+  op->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  for (int j = 0; j < m; ++j) {
+    const int cols = j + 1;
+    RhsParams P = base_params(op);
+    P.y_in64 = V + (int64_t)j * n;
+    P.out64 = op->w.p;
+    P.src64 = aug ? op->src64.p : nullptr;
+    P.aug_s = aug ? &st->s[j] : nullptr;
+    P.skip = op->skip.p;
+    DGTD_TRY(launch_rhs<kModeArnoldi>(op, P));
+    k_dots<<<nb, nt, 0, s>>>(V, n, cols, op->w.p, op->partials.p, op->skip.p);
+    k_finish_proj<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, j, 1, op->skip.p);
+    k_update<<<nb, nt, 0, s>>>(V, n, cols, st->proj, op->w.p, nullptr, op->skip.p);
+    k_dots<<<nb, nt, 0, s>>>(V, n, cols, op->w.p, op->partials.p, op->skip.p);
+    k_finish_proj<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, j, 0, op->skip.p);
+    k_update<<<nb, nt, 0, s>>>(V, n, cols, st->proj, op->w.p, op->partials.p, op->skip.p);
+    k_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, op->partials.p, nb, j, op->skip.p);
+    k_scale<<<gs, 256, 0, s>>>(op->w.p, n, &st->inv_h, V + (int64_t)(j + 1) * n, op->skip.p);
+    op->launches += 8;
+    CUDA_TRY(cudaGetLastError());
+  }
+  k_finish_coef<<<1, kExpmThreads, kExpmSmem, s>>>(st);
+  k_lincomb<<<gs, 256, 0, s>>>(V, n, st, out);
+  op->launches += 2;
+  CUDA_TRY(cudaGetLastError());
+  int dim = 0;
+  CUDA_TRY(cudaMemcpyAsync(&dim, &st->dim, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  *dim_out = dim;
+  return DGTD_OK;
+}
+
+// exp(t*A)v or the ETD step, sub-stepped into ceil(m/12) chunks
+// (gpu/operator.rs:1175-1197, :1267-1291).
+int krylov_run(dgtd_op* op, const double* v_host, const double* b_host, double t, int m, double tol,
+               double* out_host, int* dim_used) {
+  if (m < 1) return set_error(DGTD_ERR_BAD_ARG, "Krylov dimension must be >= 1");
+  if (!std::isfinite(t)) return set_error(DGTD_ERR_BAD_ARG, "Krylov time must be finite");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  const int kchunk = 12;
+  const int k = std::max(1, (m + kchunk - 1) / kchunk);
+  const int chunk = (m + k - 1) / k;
+  DGTD_TRY(ensure_krylov(op, chunk));
+  cudaStream_t s = op->stream();
+  const int64_t n = op->n_dof;
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, v_host, n * 8, cudaMemcpyHostToDevice, s));
+  DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->vin64.p)));
+  const bool aug = b_host != nullptr;
+  if (aug) {
+    DGTD_TRY(op->src64.alloc(n));
+    CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, b_host, n * 8, cudaMemcpyHostToDevice, s));
+    DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->src64.p)));
+  }
+  const double tau = t / (double)k;
+  int total = 0;
+  for (int q = 0; q < k; ++q) {
+    int d = 0;
+    DGTD_TRY(krylov_chunk(op, op->vin64.p, tau, chunk, tol, aug, op->w.p, &d));
+    total += d;
+    CUDA_TRY(cudaMemcpyAsync(op->vin64.p, op->w.p, n * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  DGTD_TRY((to_aos<double, double>(op, op->vin64.p, op->tmp64.p)));
+  CUDA_TRY(cudaMemcpyAsync(out_host, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (dim_used) *dim_used = total;
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_expmv(dgtd_op* op, const double* v, double t, int32_t m, double tol, double* out,
+                          int32_t* dim_used) {
+  if (!op || !v || !out) return set_error(DGTD_ERR_BAD_ARG, "expmv: null argument");
+  int d = 0;
+  DGTD_TRY(krylov_run(op, v, nullptr, t, m, tol, out, &d));
+  if (dim_used) *dim_used = d;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_etd_step(dgtd_op* op, const double* y, const double* b, double h, int32_t m,
+                             double tol, double* out, int32_t* dim_used) {
+  if (!op || !y || !b || !out) return set_error(DGTD_ERR_BAD_ARG, "etd_step: null argument");
+  int d = 0;
+  DGTD_TRY(krylov_run(op, y, b, h, m, tol, out, &d));
+  if (dim_used) *dim_used = d;
+  return DGTD_OK;
+}
+
+// Dense exp(A) on the device (d <= 64), for tests of the Hessenberg exponential.
+extern "C" int dgtd_debug_expm(dgtd_ctx* ctx, const double* a, int32_t d, double* out) {
+  if (!ctx || !a || !out || d < 1 || d > dgtd::kKrylovMaxDim) return set_error(DGTD_ERR_BAD_ARG, "debug_expm: bad argument");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  DevBuf<double> da, dout;
+  DGTD_TRY(da.alloc((size_t)d * d));
+  DGTD_TRY(dout.alloc((size_t)d * d));
+  CUDA_TRY(cudaFuncSetAttribute(dgtd::k_expm_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
+  CUDA_TRY(cudaMemcpyAsync(da.p, a, (size_t)d * d * 8, cudaMemcpyHostToDevice, ctx->stream));
+  dgtd::k_expm_dense<<<1, dgtd::kExpmThreads, dgtd::kExpmSmem, ctx->stream>>>(da.p, d, dout.p);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(out, dout.p, (size_t)d * d * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  da.free();
+  dout.free();
+  return DGTD_OK;
+}

@@ -1,0 +1,69 @@
+// dgtd_common.cuh -- shared device-side definitions of the DGTD kernels.
+//
+// Device data layout (HBM):
+//   state      float  y[K][6][Np]     element-major SoA: component c of node i
+//                                     of element e at (e*6 + c)*Np + i, c = Ex,Ey,Ez,Hx,Hy,Hz.
+//   element    float  meta[K][kMetaWords] one 176-byte record per element:
+//                       [0..9)   J^-1 row-major           (geom_factors.rs:81-88)
+//                       [9..21)  4 outward unit normals   (topology.rs:64-78)
+//                       [21..25) 4 face scales 2A/|detJ|  (rhs.rs:828)
+//                       [25..37) 1/eps, 1/mu, sigma/eps, sigma*/mu (rhs.rs:900-926)
+//                       [37..41) 4 neighbour element ids (int bits, -1 boundary)
+//                       [41..43) 4 face codes, 16 bits each (faces 0,1 in word 41):
+//                                bits 0..7 gather-table id, bits 8..9 kind
+//                                (0 interior, 1 PEC wall, 2 port)
+//                       [43]     padding
+//   gather tables (per operator, uint8): gtab[id][m] = volume node of the
+//                       neighbour that matches this face's node m
+//                       (face_nodes[nbr_lf][perm[m]], rhs.rs:1404-1406).
+//   face nodes (uint8):  fnodes[f][m] = own volume node of face f node m.
+//   operators (f32):     dT[k][j][i] = D_k[i][j] (k = r,s,t), liftT[s][i] = LIFT[i][s].
+#pragma once
+#include <cstdint>
+
+namespace dgtd {
+
+constexpr int kMetaWords = 44;
+constexpr int kMaxGather = 96;
+constexpr int kMaxOrder = 5;
+
+enum FaceKind : int { kInterior = 0, kPec = 1, kPort = 2 };
+
+__host__ __device__ constexpr int np_of(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
+__host__ __device__ constexpr int nfp_of(int n) { return (n + 1) * (n + 2) / 2; }
+
+// Epilogue modes of the RHS kernel.
+enum RhsMode : int {
+  kModeApply = 0,    // out = dy (f32 SoA)
+  kModeLserk = 1,    // fused LSERK4 stage: p = a*p + dt*(dy+src); y_out = y_in + b*p
+  kModeArnoldi = 2,  // out64 = dy + s*b64 (f64 SoA), input f64 SoA
+};
+
+struct OpTables {
+  const float* dT;        // 3*Np*Np
+  const float* liftT;     // 4Nfp*Np
+  const uint8_t* fnodes;  // 4*Nfp
+  const uint8_t* gtab;    // n_gather*Nfp
+  int n_gather;
+};
+
+struct RhsParams {
+  const float* y_in;       // f32 state (modes Apply/Lserk)
+  const double* y_in64;    // f64 input (mode Arnoldi)
+  float* out;              // Apply: dy ; Lserk: y_out
+  double* out64;           // Arnoldi: w
+  float* p;                // Lserk residual register
+  const float* meta;
+  const float* src_vec;    // Lserk DRIVE_VECTOR pattern (SoA f32) or null
+  const double* src64;     // Arnoldi augmented column b (SoA f64) or null
+  const double* aug_s;     // Arnoldi: device scalar s_j (augmented component), or null
+  const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop)
+  int64_t n_elem;
+  int64_t src_idx;         // Lserk DRIVE_POINT: SoA index, or -1
+  float src_g;             // held waveform value of the step
+  float a, b, dt;          // LSERK stage coefficients
+  int read_p, write_p;     // stage 0 does not read p; the last stage does not write it
+  float alpha;             // flux blend
+};
+
+}  // namespace dgtd

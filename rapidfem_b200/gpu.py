@@ -1,0 +1,232 @@
+"""The device operator: Python face of include/dgtd.h.
+
+``GpuContext`` and ``GpuOperator`` keep the names, argument meaning and error
+behaviour of crates/rapidfem-td/src/gpu/mod.rs:49-135 and
+gpu/operator.rs:207-1486 (``new``, ``n_dof``, ``apply``, ``transient``,
+``expmv``, ``etd_step``).  Where the reference returns ``Err(String)`` these
+raise :class:`rapidfem_b200._native.DgtdError`; length mismatches the reference
+asserts on raise ``ValueError``.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as nat
+from ._native import check, lib
+from .operator import MaxwellOperator
+
+
+class GpuContext:
+    """GpuContext::new (gpu/mod.rs:49): the CUDA device and its stream."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.dgtd_ctx_create(int(device), C.byref(h)))
+        self._h = h
+        buf = C.create_string_buffer(256)
+        check(lib.dgtd_ctx_device_name(h, buf, 256))
+        self.device_name = buf.value.decode()
+        self.device = device
+        self.fp64 = True
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dgtd_ctx_destroy(h)
+            self._h = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        """Issue work on an external cudaStream_t (e.g. torch's ``stream.cuda_stream``)."""
+        check(lib.dgtd_ctx_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def synchronize(self) -> None:
+        check(lib.dgtd_ctx_synchronize(self._h))
+
+    def expm(self, a) -> np.ndarray:
+        """Dense exp(A), d <= 64, on the device (the Krylov finisher's kernel)."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        out = np.zeros_like(a)
+        check(lib.dgtd_debug_expm(self._h, a.ravel(), a.shape[0], out.ravel()))
+        return out
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32).ravel()
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ravel()
+
+
+class GpuOperator:
+    """GpuOperator::new (gpu/operator.rs:207): the operator resident on the device."""
+
+    def __init__(self, ctx: GpuContext, op: MaxwellOperator):
+        self.ctx = ctx
+        self.host_op = op
+        d = op.desc()
+        h = C.c_void_p()
+        check(lib.dgtd_op_create(ctx.handle, C.byref(d), C.byref(h)))
+        self._h = h
+        n = C.c_int64()
+        check(lib.dgtd_op_n_dof(h, C.byref(n)))
+        self._n = n.value
+        self.order = op.order
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dgtd_op_destroy(h)
+            self._h = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def n_dof(self) -> int:
+        return self._n
+
+    def set_engine(self, engine: int) -> None:
+        check(lib.dgtd_op_set_engine(self._h, int(engine)))
+
+    @property
+    def engine(self) -> int:
+        e = C.c_int()
+        check(lib.dgtd_op_get_engine(self._h, C.byref(e)))
+        return e.value
+
+    def launch_count(self) -> int:
+        c = C.c_int64()
+        check(lib.dgtd_op_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def reset_launch_count(self) -> None:
+        check(lib.dgtd_op_reset_launch_count(self._h))
+
+    def _check_len(self, what, a):
+        if a.size != self._n:
+            raise ValueError(f"{what} has {a.size} entries, expected n_dof = {self._n}")
+
+    def apply(self, y) -> np.ndarray:
+        """dy = A*y in f32 (gpu/operator.rs:513)."""
+        y = _f32(y)
+        self._check_len("state", y)
+        dy = np.empty_like(y)
+        check(lib.dgtd_apply(self._h, y, dy))
+        return dy
+
+    @staticmethod
+    def _drive(drive):
+        """drive: None | ('point', dof) | ('vector', b)."""
+        if drive is None:
+            return nat.DRIVE_FREE, 0, None
+        kind, arg = drive
+        if kind == "point":
+            return nat.DRIVE_POINT, int(arg), None
+        if kind == "vector":
+            return nat.DRIVE_VECTOR, 0, _f64(arg)
+        raise ValueError(f"unknown drive {kind!r}")
+
+    def transient(self, y0, dt, steps, substeps=1, drive=None, g=None, record=False) -> np.ndarray:
+        """LSERK4 transient (gpu/operator.rs:906): `steps` frames of `dt`, each
+        `substeps` steps of dt/substeps, source held per substep."""
+        y0 = _f32(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self._check_len("source", vec)
+        substeps = max(int(substeps), 1)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g)
+            if gs.size != steps * substeps:
+                raise ValueError("wrong number of waveform samples")
+        out = np.empty(((steps + 1) * self._n) if record else self._n, dtype=np.float32)
+        check(lib.dgtd_transient(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
+                                 nat.ptr(gs), 1 if record else 0, out))
+        return out.reshape(steps + 1, self._n) if record else out
+
+    def transient_probes(self, y0, dt, steps, substeps=1, drive=None, g=None, probes=()):
+        """As transient, recording `probes` per frame; returns (series[steps+1, P], y_final)."""
+        y0 = _f32(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        substeps = max(int(substeps), 1)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g)
+            if gs.size != steps * substeps:
+                raise ValueError("wrong number of waveform samples")
+        pr = np.ascontiguousarray(probes, dtype=np.int64)
+        series = np.empty((steps + 1) * max(pr.size, 1), dtype=np.float32)
+        yf = np.empty(self._n, dtype=np.float32)
+        check(lib.dgtd_transient_probes(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
+                                        nat.ptr(gs), nat.ptr(pr) if pr.size else None, pr.size,
+                                        series.ctypes.data, yf.ctypes.data))
+        return series[: (steps + 1) * pr.size].reshape(steps + 1, pr.size), yf
+
+    def expmv(self, v, t, m, tol=0.0):
+        """exp(t*A)*v (gpu/operator.rs:1175); returns (out, dim_used)."""
+        v = _f64(v)
+        self._check_len("state", v)
+        if m < 1:
+            raise ValueError("Krylov dimension must be >= 1")
+        out = np.empty_like(v)
+        dim = C.c_int32()
+        check(lib.dgtd_expmv(self._h, v, float(t), int(m), float(tol), out, C.byref(dim)))
+        return out, dim.value
+
+    def etd_step(self, y, b, h, m, tol=0.0):
+        """exp(hA)y + h*phi1(hA)b (gpu/operator.rs:1267); returns (out, dim_used)."""
+        y = _f64(y)
+        b = _f64(b)
+        self._check_len("state", y)
+        self._check_len("source", b)
+        if m < 1:
+            raise ValueError("Krylov dimension must be >= 1")
+        out = np.empty_like(y)
+        dim = C.c_int32()
+        check(lib.dgtd_etd_step(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim)))
+        return out, dim.value
+
+    # ---- device-resident state
+    def upload(self, y) -> None:
+        y = _f32(y)
+        self._check_len("state", y)
+        check(lib.dgtd_state_upload(self._h, y))
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.float32)
+        check(lib.dgtd_state_download(self._h, out))
+        return out
+
+    def load_device(self, dptr: int) -> None:
+        check(lib.dgtd_state_load_device(self._h, C.c_void_p(dptr)))
+
+    def store_device(self, dptr: int) -> None:
+        check(lib.dgtd_state_store_device(self._h, C.c_void_p(dptr)))
+
+    def set_source_vector(self, b) -> None:
+        b = _f64(b)
+        self._check_len("source", b)
+        check(lib.dgtd_set_source_vector(self._h, b))
+
+    def run_lserk(self, h, steps, drive=None, g=None) -> None:
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self.set_source_vector(vec)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g)
+            if gs.size != steps:
+                raise ValueError("wrong number of waveform samples")
+        check(lib.dgtd_run_lserk(self._h, float(h), int(steps), kind, dof, nat.ptr(gs)))
+
+    def apply_device(self, d_y: int, d_dy: int) -> None:
+        check(lib.dgtd_apply_device(self._h, C.c_void_p(d_y), C.c_void_p(d_dy)))

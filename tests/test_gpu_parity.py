@@ -1,0 +1,209 @@
+"""GPU parity: the CUDA path through the C ABI against the f64 oracle.
+
+Tolerances (relative L2), from the DGTD parity targets and the reference's
+own budget (constants.rs:43-50, GPU_REL_TOL = 1e-3):
+  * one RHS evaluation:         < 1e-5 against the oracle on the same f32 input
+  * LSERK4 transients:          < 1e-4 at the final frame
+  * Krylov expmv / ETD (f64 basis, f32 matvec): < 1e-4
+Fixtures follow gpu/operator.rs:1515-1950: structured boxes, y_i =
+sin(0.3 + 0.017 i), dt = 1/rho(A).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as R
+from rapidfem_b200 import gpu as G
+from rapidfem_b200 import operator as O
+from rapidfem_b200._native import DgtdError
+
+from .conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-5
+RUN_TOL = 1e-4
+KRY_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return G.GpuContext(0)
+
+
+def _pair(mesh, order, alpha=1.0, face_port=None, materials=None):
+    prod = O.MaxwellOperator(mesh, order, alpha, face_port=face_port, materials=materials)
+    orc = R.Operator(mesh.nodes, mesh.tets, order, alpha, face_port=face_port, materials=materials)
+    return prod, orc
+
+
+def _y(n, a=0.3, b=0.017):
+    return np.sin(a + b * np.arange(n))
+
+
+def _rho(orc, iters=30):
+    rho, _ = orc.power_rho(iters)
+    return rho
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
+def test_apply_matches_oracle_vacuum(ctx, order):
+    prod, orc = _pair(O.structured_box(3, 3, 3), order)
+    gop = G.GpuOperator(ctx, prod)
+    y32 = _y(gop.n_dof()).astype(np.float32)
+    got = gop.apply(y32)
+    want = orc.apply(y32.astype(np.float64))
+    assert rel_l2(got, want) < RHS_TOL
+
+
+def test_apply_matches_oracle_dielectric_lossy_central(ctx):
+    m = O.structured_box(3, 3, 3)
+    K = m.n_tets
+    rng = np.random.default_rng(0)
+    mat = O.isotropic_materials(np.full(K, 4.0), rng.uniform(1, 2, K), rng.uniform(0, 3, K), rng.uniform(0, 1, K))
+    for alpha in (1.0, 0.0):
+        prod, orc = _pair(m, 2, alpha, materials=mat)
+        gop = G.GpuOperator(ctx, prod)
+        y32 = _y(gop.n_dof()).astype(np.float32)
+        assert rel_l2(gop.apply(y32), orc.apply(y32.astype(np.float64))) < RHS_TOL
+
+
+def test_apply_matches_oracle_jittered_sphere_ports(ctx):
+    m = O.structured_box_jittered(5, 5, 6, 1.0, 1.0, 1.2, 0.1, 7)
+    cen = m.nodes[m.tets].mean(axis=1)
+    eps = np.where(np.linalg.norm(cen - [0.5, 0.5, 0.6], axis=1) < 0.25, 4.0, 1.0)
+    port = np.where(O.boundary_faces_on_plane(m, 2, 0.0), 0, -1)
+    port[O.boundary_faces_on_plane(m, 2, 1.2)] = 1
+    for order in (3, 4):
+        prod, orc = _pair(m, order, 1.0, face_port=port, materials=O.isotropic_materials(eps))
+        gop = G.GpuOperator(ctx, prod)
+        y32 = _y(gop.n_dof(), 0.1, 0.0123).astype(np.float32)
+        assert rel_l2(gop.apply(y32), orc.apply(y32.astype(np.float64))) < RHS_TOL
+
+
+def test_apply_on_smooth_field_matches_f64_input(ctx):
+    # Same initial data in f64 (not pre-rounded): the f32 path within 1e-5.
+    m = O.structured_box(4, 4, 4)
+    prod, orc = _pair(m, 3)
+    gop = G.GpuOperator(ctx, prod)
+    x = prod.node_coords()
+    y = np.zeros((x.shape[0], 6))
+    y[:, 2] = np.sin(np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1])
+    y[:, 3] = 0.3 * np.cos(np.pi * x[:, 2])
+    y = y.ravel()
+    assert rel_l2(gop.apply(y), orc.apply(y)) < RHS_TOL
+
+
+def test_transient_matches_oracle(ctx):
+    prod, orc = _pair(O.structured_box(3, 3, 3), 2)
+    gop = G.GpuOperator(ctx, prod)
+    n = gop.n_dof()
+    y0 = _y(n, 0.2, 0.011)
+    dt = 1.0 / _rho(orc)
+    steps = 200
+    got = gop.transient(y0, dt, steps, 1)
+    want = orc.lserk(y0.astype(np.float32).astype(np.float64), dt, steps)
+    assert rel_l2(got, want) < RUN_TOL
+
+
+def test_transient_record_and_substeps(ctx):
+    prod, orc = _pair(O.structured_box(2, 2, 2), 3)
+    gop = G.GpuOperator(ctx, prod)
+    y0 = _y(gop.n_dof())
+    dt = 2.0 / _rho(orc)
+    traj = gop.transient(y0, dt, 4, substeps=2, record=True)
+    assert traj.shape == (5, gop.n_dof())
+    assert np.array_equal(traj[0], y0.astype(np.float32))
+    want = y0.astype(np.float32).astype(np.float64)
+    for k in range(4):
+        want = orc.lserk(want, dt / 2, 2)
+        assert rel_l2(traj[k + 1], want) < RUN_TOL
+
+
+def test_driven_point_transient_matches_oracle(ctx):
+    prod, orc = _pair(O.structured_box(3, 3, 3), 2)
+    gop = G.GpuOperator(ctx, prod)
+    n = gop.n_dof()
+    dof = prod.nearest_node_dof([0.5, 0.5, 0.5], 0, 2)
+    dt = 1.0 / _rho(orc)
+    steps = 150
+    t = np.arange(steps) * dt
+    g = np.exp(-((t - 40 * dt) / (12 * dt)) ** 2)
+    got = gop.transient(np.zeros(n), dt, steps, 1, drive=("point", dof), g=g)
+    want = orc.lserk(np.zeros(n), dt, steps, src_dof=dof, vals=g.astype(np.float32).astype(np.float64))
+    assert rel_l2(got, want) < RUN_TOL
+
+
+def test_driven_vector_transient_matches_oracle(ctx):
+    m = O.structured_box(2, 2, 4, 1.0, 0.5, 2.0)
+    port = np.where(O.boundary_faces_on_plane(m, 2, 0.0), 0, -1)
+    port[O.boundary_faces_on_plane(m, 2, 2.0)] = 1
+    prod, orc = _pair(m, 2, 1.0, face_port=port)
+    prof = prod.rect_port_profiles(0, [0, 0, 1.0], (1, 0))
+    b = prod.port_source(0, prof)
+    gop = G.GpuOperator(ctx, prod)
+    dt = 1.0 / _rho(orc)
+    steps = 120
+    t = np.arange(steps) * dt
+    g = np.exp(-((t - 30 * dt) / (10 * dt)) ** 2) * np.cos(2 * np.pi * 1.5 * t)
+    got = gop.transient(np.zeros(gop.n_dof()), dt, steps, 1, drive=("vector", b), g=g)
+    want = orc.lserk(np.zeros(gop.n_dof()), dt, steps, src_vec=b.astype(np.float32).astype(np.float64),
+                     vals=g.astype(np.float32).astype(np.float64))
+    assert rel_l2(got, want) < RUN_TOL
+
+
+def test_transient_probes(ctx):
+    prod, orc = _pair(O.structured_box(2, 2, 2), 2)
+    gop = G.GpuOperator(ctx, prod)
+    y0 = _y(gop.n_dof())
+    dt = 1.0 / _rho(orc)
+    probes = [0, 5, gop.n_dof() - 1]
+    series, yf = gop.transient_probes(y0, dt, 10, 1, probes=probes)
+    traj = gop.transient(y0, dt, 10, 1, record=True)
+    assert np.array_equal(series, traj[:, probes])
+    assert np.array_equal(yf, traj[-1])
+
+
+def test_expmv_matches_oracle(ctx):
+    # gpu/operator.rs:1839: m = 40, t = 0.02 against the CPU propagator.
+    prod, orc = _pair(O.structured_box(3, 3, 3), 2)
+    gop = G.GpuOperator(ctx, prod)
+    v = _y(gop.n_dof())
+    want, _ = orc.expmv(v, 0.02, 40, 0.0)
+    got, dim = gop.expmv(v, 0.02, 40)
+    assert rel_l2(got, want) < KRY_TOL
+    assert dim == 40
+    got_a, dim_a = gop.expmv(v, 0.02, 40, tol=1e-10)
+    assert rel_l2(got_a, want) < KRY_TOL
+    assert dim_a <= 40
+
+
+def test_etd_step_matches_oracle(ctx):
+    prod, orc = _pair(O.structured_box(3, 3, 3), 2)
+    gop = G.GpuOperator(ctx, prod)
+    n = gop.n_dof()
+    y = _y(n, 0.1, 0.007)
+    b = np.zeros(n)
+    b[prod.nearest_node_dof([0.5, 0.5, 0.5], 0, 2)] = 0.7
+    h = 0.05
+    want, _ = orc.etd_step(y, b, h, 40, 0.0)
+    got, dim = gop.etd_step(y, b, h, 24)
+    assert rel_l2(got, want) < KRY_TOL
+
+
+def test_device_expm_matches_oracle(ctx):
+    rng = np.random.default_rng(1)
+    for d in (1, 5, 23, 64):
+        a = rng.normal(size=(d, d)) * (3.0 / np.sqrt(d))
+        assert rel_l2(ctx.expm(a), R.expm(a)) < 1e-12
+
+
+def test_bad_arguments_raise(ctx):
+    prod, _ = _pair(O.structured_box(1, 1, 1), 2)
+    gop = G.GpuOperator(ctx, prod)
+    with pytest.raises(ValueError):
+        gop.apply(np.zeros(3))
+    with pytest.raises(DgtdError):
+        gop.transient(np.zeros(gop.n_dof()), 0.01, 2, 1, drive=("point", gop.n_dof() + 5), g=np.ones(2))
+    with pytest.raises(DgtdError):
+        gop.transient(np.zeros(gop.n_dof()), -1.0, 2)
+    assert gop.launch_count() >= 0

@@ -1,0 +1,171 @@
+"""The oracle pinned against the reference's own golden vectors and analytic
+tests (CPU only).
+
+Golden fixtures in tests/golden/ come from crates/rapidfem-td/tests/*.rs
+(see tests/golden/make_golden.py).  The analytic checks restate
+rhs.rs:1830-1868 (central flux skew), rhs.rs:2113-2148 (cavity pi*sqrt 2),
+dg_basis.rs:524-557 (LIFT integrates face traces) and
+tests/lserk4_convergence_test.rs (fourth order).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as R
+
+from .conftest import rel_l2
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF_TET = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1.0]])
+ONE_TET = np.array([[0, 1, 2, 3]], dtype=np.int32)
+
+
+def _max_rel_err(got, want):
+    want = np.asarray(want)
+    return np.max(np.abs(np.asarray(got) - want)) / max(np.max(np.abs(want)), 1e-300)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_dg_basis_matches_golden(p):
+    tab = json.load(open(os.path.join(GOLD, "dg_basis.json")))["tables"]
+    op = R.Operator(REF_TET, ONE_TET, p)
+    for arr, key in (("mass", "MASS"), ("dr", "DR"), ("ds", "DS"), ("dt", "DT")):
+        assert _max_rel_err(op.get(arr), tab[f"{key}_P{p}"]) < 1e-9, (arr, p)
+
+
+def test_curl_matches_golden():
+    g = json.load(open(os.path.join(GOLD, "rhs_curl.json")))
+    tet = np.array(g["tet"]).reshape(4, 3)
+    op = R.Operator(tet, ONE_TET, g["order"])
+    got = R.curl_single(g["order"], op.get("jinv"), g["field"])
+    assert _max_rel_err(got, g["curl"]) < 1e-9
+
+
+def test_expmv_matches_golden():
+    g = json.load(open(os.path.join(GOLD, "propagator_expm.json")))
+    a = np.array(g["a"]).reshape(g["n"], g["n"])
+    for h, ref in g["cases"]:
+        got, dim = R.expmv_dense(a, g["v0"], h, 12, 0.0)
+        assert rel_l2(got, ref) < 1e-10
+        assert dim <= 6  # lucky breakdown inside the 6-dim space
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_lift_integrates_face_traces(p):
+    op = R.Operator(REF_TET, ONE_TET, p)
+    np_, nfp = op.np, op.nfp
+    lift = op.get("lift").reshape(np_, 4 * nfp)
+    mass = op.get("mass").reshape(np_, np_)
+    for f in range(4):
+        tr = np.zeros(4 * nfp)
+        tr[f * nfp:(f + 1) * nfp] = 1.0
+        assert abs(np.sum(mass @ (lift @ tr)) - 0.5) < 1e-9
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+def test_diff_rows_sum_to_zero(p):
+    op = R.Operator(REF_TET, ONE_TET, p)
+    for k in ("dr", "ds", "dt"):
+        d = op.get(k).reshape(op.np, op.np)
+        assert np.max(np.abs(d.sum(axis=1))) < 1e-8
+
+
+def _dense(op):
+    n = op.n_dof
+    a = np.zeros((n, n))
+    e = np.zeros(n)
+    for j in range(n):
+        e[j] = 1.0
+        a[:, j] = op.apply(e)
+        e[j] = 0.0
+    return a
+
+
+def _energy_mass(op):
+    np_ = op.np
+    mass = op.get("mass").reshape(np_, np_)
+    det = np.abs(op.get("det"))
+    ie = op.get("inv_eps").reshape(-1, 3)
+    im = op.get("inv_mu").reshape(-1, 3)
+    n = op.n_dof
+    m = np.zeros((n, n))
+    for e in range(op.n_elem):
+        w = np.concatenate([1 / ie[e], 1 / im[e]])
+        for c in range(6):
+            idx = (e * np_ + np.arange(np_)) * 6 + c
+            m[np.ix_(idx, idx)] = w[c] * det[e] * mass
+    return m
+
+
+def test_central_flux_is_skew_in_energy_norm():
+    nodes, tets = R.box_mesh(1, 1, 1)
+    op = R.Operator(nodes, tets, 2, flux_alpha=0.0)
+    ma = _energy_mass(op) @ _dense(op)
+    assert np.max(np.abs(ma + ma.T)) < 1e-9 * max(np.max(np.abs(ma)), 1.0)
+
+
+def test_cavity_fundamental_is_pi_sqrt2():
+    nodes, tets = R.box_mesh(2, 2, 2)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    ev = np.linalg.eigvals(_dense(op))
+    phys = ev[np.abs(ev.imag) > 1.0]
+    fund = phys[np.argmax(phys.real)]
+    want = np.pi * np.sqrt(2.0)
+    assert fund.real < 0.0
+    assert abs(abs(fund.imag) - want) / want < 0.05
+
+
+def test_lserk4_is_fourth_order_on_the_dg_operator():
+    nodes, tets = R.box_mesh(1, 1, 1)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    a = _dense(op)
+    y0 = np.sin(0.3 + 0.017 * np.arange(op.n_dof))
+    t = 0.4
+    w, v = np.linalg.eig(a * t)
+    exact = np.real(v @ (np.exp(w) * np.linalg.solve(v, y0)))
+    errs = []
+    for steps in (40, 80, 160):
+        errs.append(rel_l2(op.lserk(y0, t / steps, steps), exact))
+    orders = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert np.all(orders > 3.5), orders
+
+
+def test_krylov_matches_lserk_on_the_dg_operator():
+    # explicit.rs:173-208: one LSERK4 step of 1e-3 vs expmv (m = 40), < 1e-9.
+    nodes, tets = R.box_mesh(2, 2, 2)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    y0 = np.sin(0.3 + 0.017 * np.arange(op.n_dof))
+    h = 1e-3
+    ref = op.lserk(y0, h, 1)
+    got, dim = op.expmv(y0, h, 40, 0.0)
+    assert rel_l2(got, ref) < 1e-9
+    got_adaptive, dim = op.expmv(y0, h, 40, 1e-10)
+    assert rel_l2(got_adaptive, ref) < 1e-9
+    assert dim < 40
+
+
+def test_etd_step_matches_augmented_dense():
+    nodes, tets = R.box_mesh(1, 1, 1)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    n = op.n_dof
+    a = _dense(op)
+    y = np.cos(0.1 + 0.013 * np.arange(n))
+    b = np.zeros(n)
+    b[7] = 1.0
+    h = 0.05
+    aug = np.zeros((n + 1, n + 1))
+    aug[:n, :n] = a
+    aug[:n, n] = b
+    ref = R.expm(aug * h)[:n] @ np.concatenate([y, [1.0]])
+    got, _ = op.etd_step(y, b, h, 40, 0.0)
+    assert rel_l2(got, ref) < 1e-9
+
+
+def test_expm_identities():
+    z = R.expm(np.zeros((3, 3)))
+    assert np.allclose(z, np.eye(3))
+    a = np.array([[0.0, 1.0], [-1.0, 0.0]]) * 3.0
+    e = R.expm(a)
+    assert np.allclose(e, [[np.cos(3), np.sin(3)], [-np.sin(3), np.cos(3)]], atol=1e-13)
