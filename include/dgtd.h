@@ -86,6 +86,8 @@ typedef struct {
     const int32_t *face_nbr_local; /* 4K */
     const int32_t *face_port;      /* 4K, -1 = none (non-port boundary = PEC) */
     const int32_t *face_perm;      /* 4K*Nfp neighbour face-node match, rhs.rs:546-566 */
+    const double *mass;            /* Np*Np reference mass matrix (dg_basis.rs:95), or NULL;
+                                      needed only by the energy entry points */
 } dgtd_op_desc;
 
 /* Contraction engine of the RHS kernels. */
@@ -158,6 +160,22 @@ int dgtd_run_lserk(dgtd_op *op, float h, int64_t steps, int drive, int64_t src_d
 int dgtd_set_source_vector(dgtd_op *op, const double *src_vec);
 /* dy = A*y on device AoS pointers (f32). */
 int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
+
+/* ---- session helpers --------------------------------------------------
+ * TdSession::cfl_dt (session.rs:514-569) on the device: rho(A) by 40 power
+ * iterations from the reference's deterministic start vector (splitmix64 +
+ * Box-Muller, seed 0, session.rs:415-431), then the LSERK4 stability bracket
+ * z in [3, 15] widened as needed, 7 bisections of 64-step probes from the
+ * dominant vector (growth rate <= 1e-3 per step, norm <= 10x).  Outputs the
+ * stable step h = 0.8*z/rho (operator time), rho and z; any may be NULL. */
+int dgtd_cfl_dt(dgtd_op *op, double *h, double *rho, double *z);
+/* Spectral radius only: `iters` power iterations (session.rs:522-534). */
+int dgtd_power_rho(dgtd_op *op, int32_t iters, double *rho);
+/* field_energy (rhs.rs:1509-1544): 1/2 sum_e |det J_e| sum_c w_c f_c^T M f_c,
+ * w = eps (E) or mu (H), accumulated in f64 on the device.  `y` is a host AoS
+ * f64 state; dgtd_state_energy uses the resident f32 state.  Needs desc.mass. */
+int dgtd_field_energy(dgtd_op *op, const double *y, double *energy);
+int dgtd_state_energy(dgtd_op *op, double *energy);
 
 /* ---- statistics -------------------------------------------------------- */
 /* Kernel launches issued by this op since creation / the last reset. */

@@ -57,7 +57,7 @@ class OpDesc(C.Structure):
         ("diff_r", _vp), ("diff_s", _vp), ("diff_t", _vp), ("lift", _vp), ("face_nodes", _vp),
         ("jinv", _vp), ("inv_eps", _vp), ("inv_mu", _vp), ("sigma_eps", _vp), ("sigma_mu", _vp),
         ("face_normal", _vp), ("face_fscale", _vp), ("face_neighbor", _vp),
-        ("face_nbr_local", _vp), ("face_port", _vp), ("face_perm", _vp),
+        ("face_nbr_local", _vp), ("face_port", _vp), ("face_perm", _vp), ("mass", _vp),
     ]
 
 
@@ -96,6 +96,10 @@ _sig("dgtd_apply_device", C.c_int, _vp, _vp, _vp)
 _sig("dgtd_op_launch_count", C.c_int, _vp, C.POINTER(_i64))
 _sig("dgtd_op_reset_launch_count", C.c_int, _vp)
 _sig("dgtd_debug_expm", C.c_int, _vp, _pd, _i32, _pd)
+_sig("dgtd_cfl_dt", C.c_int, _vp, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_f64))
+_sig("dgtd_power_rho", C.c_int, _vp, _i32, C.POINTER(_f64))
+_sig("dgtd_field_energy", C.c_int, _vp, _pd, C.POINTER(_f64))
+_sig("dgtd_state_energy", C.c_int, _vp, C.POINTER(_f64))
 # host side
 _sig("dgtd_mesh_box", C.c_int, _i32, _i32, _i32, _f64, _f64, _f64, _pd, _pi)
 _sig("dgtd_mesh_box_jittered", C.c_int, _i32, _i32, _i32, _f64, _f64, _f64, _f64, _u64, _pd, _pi)

@@ -166,6 +166,9 @@ struct dgtd_op {
   DevBuf<dgtd::KrylovDev> kst;
   DevBuf<int> skip;
   int kry_cap = 0;
+  // energy: reference mass matrix (f64) and |det J| per element
+  DevBuf<double> mass, absdet;
+  bool has_mass = false;
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
@@ -173,7 +176,7 @@ struct dgtd_op {
     meta.free(); dT.free(); liftT.free(); fnodes.free(); gtab.free();
     y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
-    kst.free(); skip.free();
+    kst.free(); skip.free(); mass.free(); absdet.free();
   }
 };
 
@@ -415,6 +418,21 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   if (!e) e = cudaMemsetAsync(op->y[0].p, 0, op->y[0].n * 4, s);
   if (!e) e = cudaMemsetAsync(op->y[1].p, 0, op->y[1].n * 4, s);
   if (!e) e = cudaMemsetAsync(op->p.p, 0, op->p.n * 4, s);
+  if (!e && d->mass) {
+    // |det J| = 1/|det J^-1| from the f64 J^-1 of the descriptor.
+    std::vector<double> absdet((size_t)K);
+    for (int64_t q = 0; q < K; ++q) {
+      const double* m = d->jinv + 9 * q;
+      const double dj = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                        m[2] * (m[3] * m[7] - m[4] * m[6]);
+      absdet[q] = 1.0 / std::fabs(dj);
+    }
+    if ((st = op->mass.alloc((size_t)np * np)) || (st = op->absdet.alloc((size_t)K))) return fail(st);
+    e = cudaMemcpyAsync(op->mass.p, d->mass, (size_t)np * np * 8, cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaMemcpyAsync(op->absdet.p, absdet.data(), (size_t)K * 8, cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaStreamSynchronize(s);
+    op->has_mass = true;
+  }
   if (!e) e = cudaStreamSynchronize(s);
   if (e) {
     set_error(DGTD_ERR_CUDA, std::string("op_create upload: ") + cudaGetErrorString(e));
@@ -804,4 +822,245 @@ extern "C" int dgtd_debug_expm(dgtd_ctx* ctx, const double* a, int32_t d, double
   da.free();
   dout.free();
   return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ session helpers
+
+namespace {
+
+__global__ void k_norm2_f32(const float* __restrict__ x, int64_t n, double* __restrict__ partials) {
+  __shared__ double acc[8];
+  double sq = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const double v = x[k];
+    sq += v * v;
+  }
+  sq = dgtd::warp_sum(sq);
+  if ((threadIdx.x & 31) == 0) acc[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += acc[q];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_all_finite_f32(const float* __restrict__ x, int64_t n, int* __restrict__ bad) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(x[k])) { *bad = 1; return; }
+}
+
+__global__ void k_scale_f32(const float* __restrict__ x, int64_t n, float s, float* __restrict__ out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    out[k] = x[k] * s;
+}
+
+// One warp per element: 1/2 |det J| sum_c w_c f_c^T M f_c (rhs.rs:1509-1544).
+template <class T>
+__global__ void k_energy(const T* __restrict__ y, const double* __restrict__ mass, const double* __restrict__ absdet,
+                         const float* __restrict__ meta, int64_t n_elem, int np, double* __restrict__ partials) {
+  extern __shared__ double sMass[];
+  __shared__ double acc[8];
+  for (int i = threadIdx.x; i < np * np; i += blockDim.x) sMass[i] = mass[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double local = 0.0;
+  for (int64_t e = (int64_t)blockIdx.x * nw + warp; e < n_elem; e += (int64_t)gridDim.x * nw) {
+    const T* Y = y + e * 6 * np;
+    const float* M = meta + e * dgtd::kMetaWords;
+    double w[6];
+    for (int c = 0; c < 3; ++c) {
+      w[c] = 1.0 / (double)M[25 + c];
+      w[3 + c] = 1.0 / (double)M[28 + c];
+    }
+    double el = 0.0;
+    for (int i = lane; i < np; i += 32)
+      for (int c = 0; c < 6; ++c) {
+        double t = 0.0;
+        for (int j = 0; j < np; ++j) t += sMass[i * np + j] * (double)Y[c * np + j];
+        el += w[c] * (double)Y[c * np + i] * t;
+      }
+    local += absdet[e] * el;
+  }
+  local = dgtd::warp_sum(local);
+  if (lane == 0) acc[warp] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < nw; ++q) t += acc[q];
+    partials[blockIdx.x] = t;
+  }
+}
+
+constexpr int kRedBlocks = 296;
+
+int norm2_f32(dgtd_op* op, const float* x, double* out) {
+  DGTD_TRY(op->partials.alloc((size_t)dgtd::kKrylovBlocks * dgtd::kKrylovMaxDim));
+  k_norm2_f32<<<kRedBlocks, 256, 0, op->stream()>>>(x, op->n_dof, op->partials.p);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> h(kRedBlocks);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), op->partials.p, kRedBlocks * 8, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  double t = 0.0;
+  for (double v : h) t += v;
+  *out = std::sqrt(t);
+  return DGTD_OK;
+}
+
+// Deterministic standard normals, splitmix64 + Box-Muller (session.rs:415-431).
+void normal_vector(std::vector<double>& out, uint64_t seed) {
+  uint64_t state = seed;
+  auto uniform = [&]() {
+    state += 0x9e3779b97f4a7c15ULL;
+    uint64_t z = state;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    z ^= z >> 31;
+    return (double(z >> 11) + 0.5) / double(1ULL << 53);
+  };
+  for (auto& v : out) {
+    const double u = uniform(), w = uniform();
+    v = std::sqrt(-2.0 * std::log(u)) * std::cos(2.0 * 3.14159265358979323846 * w);
+  }
+}
+
+// Power iteration on the resident SoA state slot `v` (normalised in place);
+// `tmp` receives A v.  Returns rho of the last iteration.
+int power_iterate(dgtd_op* op, float* v, float* tmp, int iters, double* rho) {
+  double r = 1.0;
+  for (int it = 0; it < iters; ++it) {
+    RhsParams P = base_params(op);
+    P.y_in = v;
+    P.out = tmp;
+    DGTD_TRY(launch_rhs<kModeApply>(op, P));
+    DGTD_TRY(norm2_f32(op, tmp, &r));
+    if (!(r > 0.0) || !std::isfinite(r)) return set_error(DGTD_ERR_NONFINITE, "power iteration: norm is zero or non-finite");
+    k_scale_f32<<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(tmp, op->n_dof, (float)(1.0 / r), v);
+    op->launches++;
+    CUDA_TRY(cudaGetLastError());
+  }
+  *rho = r;
+  return DGTD_OK;
+}
+
+int start_vector(dgtd_op* op, float* soa) {
+  std::vector<double> v((size_t)op->n_dof);
+  normal_vector(v, 0);
+  double nrm = 0.0;
+  for (double x : v) nrm += x * x;
+  nrm = 1.0 / std::sqrt(nrm);
+  std::vector<float> f(v.size());
+  for (size_t i = 0; i < v.size(); ++i) f[i] = (float)(v[i] * nrm);
+  DGTD_TRY(op->aos32.alloc(op->n_dof + 4));
+  CUDA_TRY(cudaMemcpyAsync(op->aos32.p, f.data(), op->n_dof * 4, cudaMemcpyHostToDevice, op->stream()));
+  DGTD_TRY((to_soa<float, float>(op, op->aos32.p, soa)));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_power_rho(dgtd_op* op, int32_t iters, double* rho) {
+  if (!op || !rho || iters < 1) return set_error(DGTD_ERR_BAD_ARG, "power_rho: bad argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DevBuf<float> v, t;
+  DGTD_TRY(v.alloc(op->n_dof + 4));
+  DGTD_TRY(t.alloc(op->n_dof + 4));
+  int st = start_vector(op, v.p);
+  if (st == DGTD_OK) st = power_iterate(op, v.p, t.p, iters, rho);
+  cudaStreamSynchronize(op->stream());
+  v.free();
+  t.free();
+  return st;
+}
+
+extern "C" int dgtd_cfl_dt(dgtd_op* op, double* h_out, double* rho_out, double* z_out) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "cfl_dt: null op");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DevBuf<float> probe, tmp;
+  DevBuf<int> bad;
+  DGTD_TRY(probe.alloc(op->n_dof + 4));
+  DGTD_TRY(tmp.alloc(op->n_dof + 4));
+  DGTD_TRY(bad.alloc(1));
+  double rho = 0.0;
+  int st = start_vector(op, probe.p);
+  if (st == DGTD_OK) st = power_iterate(op, probe.p, tmp.p, 40, &rho);
+  if (st != DGTD_OK) return st;
+  double n0 = 0.0;
+  DGTD_TRY(norm2_f32(op, probe.p, &n0));
+  // Probe: 64 LSERK4 steps of z/rho from the dominant vector on the resident
+  // state; stable when finite, norm <= 10 n0 and rate <= 1 + 1e-3.
+  auto stable = [&](double z, bool* ok) -> int {
+    const float h = (float)(z / rho);
+    CUDA_TRY(cudaMemcpyAsync(op->y[op->cur].p, probe.p, op->n_dof * 4, cudaMemcpyDeviceToDevice, op->stream()));
+    for (int s = 0; s < 64; ++s) DGTD_TRY(lserk_step(op, h, -1, 0.f, nullptr));
+    CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), op->stream()));
+    k_all_finite_f32<<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(op->y[op->cur].p, op->n_dof, bad.p);
+    op->launches++;
+    CUDA_TRY(cudaGetLastError());
+    int hb = 0;
+    CUDA_TRY(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, op->stream()));
+    CUDA_TRY(cudaStreamSynchronize(op->stream()));
+    if (hb) { *ok = false; return DGTD_OK; }
+    double nf = 0.0;
+    DGTD_TRY(norm2_f32(op, op->y[op->cur].p, &nf));
+    if (!std::isfinite(nf) || nf > 10.0 * n0) { *ok = false; return DGTD_OK; }
+    const double rate = nf > 0.0 ? std::pow(nf / n0, 1.0 / 64.0) : 0.0;
+    *ok = rate <= 1.0 + 1e-3;
+    return DGTD_OK;
+  };
+  double lo = 3.0, hi = 15.0;
+  bool ok = false;
+  for (;;) { DGTD_TRY(stable(lo, &ok)); if (ok || !(lo > 0.1)) break; lo *= 0.5; }
+  for (;;) { DGTD_TRY(stable(hi, &ok)); if (!ok || !(hi < 1e3)) break; hi *= 1.5; }
+  for (int it = 0; it < 7; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    DGTD_TRY(stable(mid, &ok));
+    if (ok) lo = mid; else hi = mid;
+  }
+  probe.free(); tmp.free(); bad.free();
+  if (h_out) *h_out = 0.8 * lo / rho;
+  if (rho_out) *rho_out = rho;
+  if (z_out) *z_out = lo;
+  return DGTD_OK;
+}
+
+template <class T>
+static int energy_of(dgtd_op* op, const T* y_soa, double* energy) {
+  if (!op->has_mass) return set_error(DGTD_ERR_UNSUPPORTED, "energy: operator created without the mass matrix");
+  DGTD_TRY(op->partials.alloc((size_t)dgtd::kKrylovBlocks * dgtd::kKrylovMaxDim));
+  const size_t sm = (size_t)op->np * op->np * 8;
+  static bool attr = false;
+  if (!attr) {
+    CUDA_TRY(cudaFuncSetAttribute(k_energy<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    attr = true;
+  }
+  k_energy<T><<<kRedBlocks, 256, sm, op->stream()>>>(y_soa, op->mass.p, op->absdet.p, op->meta.p, op->n_elem,
+                                                     op->np, op->partials.p);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> h(kRedBlocks);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), op->partials.p, kRedBlocks * 8, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  double t = 0.0;
+  for (double v : h) t += v;
+  *energy = 0.5 * t;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_field_energy(dgtd_op* op, const double* y, double* energy) {
+  if (!op || !y || !energy) return set_error(DGTD_ERR_BAD_ARG, "field_energy: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(op->tmp64.alloc(op->n_dof));
+  DGTD_TRY(op->vin64.alloc(op->n_dof));
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, y, op->n_dof * 8, cudaMemcpyHostToDevice, op->stream()));
+  DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->vin64.p)));
+  return energy_of<double>(op, op->vin64.p, energy);
+}
+
+extern "C" int dgtd_state_energy(dgtd_op* op, double* energy) {
+  if (!op || !energy) return set_error(DGTD_ERR_BAD_ARG, "state_energy: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  return energy_of<float>(op, op->y[op->cur].p, energy);
 }

@@ -514,6 +514,7 @@ extern "C" int dgtd_host_op_desc(const dgtd_host_op* h, dgtd_op_desc* d) {
   d->face_nbr_local = o.nbr_lf.data();
   d->face_port = o.port.data();
   d->face_perm = o.perm.data();
+  d->mass = o.re.mass.a.data();
   return DGTD_OK;
 }
 

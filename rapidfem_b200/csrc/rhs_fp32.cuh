@@ -29,15 +29,20 @@ struct Fp32Cfg {
   static constexpr int E = N == 1 ? 64 : N == 2 ? 24 : N == 3 ? 12 : N == 4 ? 8 : 4;
   static constexpr int THREADS = ((E * NP + 31) / 32) * 32;
   static constexpr int TILE = E * 6 * NP;  // floats of state per tile
-  // shared memory layout (floats)
+  // shared memory layout (floats); every region starts on a 16-byte boundary
+  // because the state tile and the element records are filled with float4.
+  static constexpr int al4(int x) { return (x + 3) & ~3; }
   static constexpr int OFF_D = 0;
-  static constexpr int OFF_L = OFF_D + 3 * NP * NP;
-  static constexpr int OFF_Y = OFF_L + NF * NP;
-  static constexpr int OFF_F = OFF_Y + TILE;
-  static constexpr int OFF_M = OFF_F + E * 6 * NF;
-  static constexpr int OFF_B = OFF_M + E * kMetaWords;  // byte tables start (as floats)
+  static constexpr int OFF_L = al4(OFF_D + 3 * NP * NP);
+  static constexpr int OFF_Y = al4(OFF_L + NF * NP);
+  static constexpr int OFF_F = al4(OFF_Y + TILE);
+  static constexpr int OFF_M = al4(OFF_F + E * 6 * NF);
+  static constexpr int OFF_B = al4(OFF_M + E * kMetaWords);  // byte tables start (as floats)
   static constexpr int BYTES_TAB = 4 * NFP + kMaxGather * NFP;
   static constexpr int SMEM = OFF_B * 4 + ((BYTES_TAB + 15) / 16) * 16;
+  static_assert(OFF_Y % 4 == 0 && OFF_M % 4 == 0, "float4 regions must be 16-byte aligned");
+  static_assert((TILE % 4) == 0 || (E % 2) == 0, "tile start must stay 16-byte aligned");
+  static_assert(((E * 6 * NP) % 4) == 0, "consecutive tiles must start 16-byte aligned");
 };
 
 __device__ __forceinline__ void cross3f(float ax, float ay, float az, float bx, float by, float bz,

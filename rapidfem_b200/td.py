@@ -1,0 +1,300 @@
+"""The time-domain session and problem API on the B200 path.
+
+``TdSession`` mirrors ``PyTdSession`` (python/src/td.rs:163-426) and
+``ProblemTD`` mirrors rapidfem.problem.td.ProblemTD (problem/td.py:195-750)
+for the parts on the DGTD hot path: the operator, ``apply``, the Krylov
+``step``, ``step_explicit``, ``cfl_dt``, ``nearest_node_dof``, ``field_energy``
+and ``transient`` with point / port drives and probes, for the exponential and
+explicit (LSERK4) integrators.  Runs go to the GPU; ``device="cpu"`` is refused
+(there is no CPU path in this package).  The run logic follows
+TdSession::transient (crates/rapidfem-td/src/session.rs:620-777): LSERK4 is
+sub-stepped to the CFL limit with the source held per substep, the exponential
+integrator takes one ETD step per frame with the source held per frame.
+"""
+from __future__ import annotations
+
+import math
+import sys
+
+import numpy as np
+
+from . import gpu as G
+from . import operator as O
+
+C_LIGHT = 299_792_458.0
+KRYLOV_TOL = 1e-10
+_CTX = {}
+
+
+def _log(verbose, msg):
+    if verbose:
+        print(f"  [rapidfem-td] {msg}", file=sys.stderr, flush=True)
+
+
+def _ctx(device_index=0):
+    if device_index not in _CTX:
+        _CTX[device_index] = G.GpuContext(device_index)
+    return _CTX[device_index]
+
+
+def flux_alpha(flux: str) -> float:
+    """session.rs:93-99."""
+    if flux == "upwind":
+        return 1.0
+    if flux == "central":
+        return 0.0
+    raise ValueError(f"flux must be one of ['central', 'upwind'], got {flux!r}")
+
+
+class GaussianPulse:
+    """g(t) = exp(-((t-t0)/tau)^2) * cos(2 pi f0 (t-t0)) (session.rs:242-261)."""
+
+    def __init__(self, t0, tau, f0=None):
+        self.t0, self.tau, self.f0 = float(t0), float(tau), None if f0 is None else float(f0)
+
+    def __call__(self, t):
+        t = np.asarray(t, dtype=np.float64)
+        x = (t - self.t0) / self.tau
+        env = np.exp(-(x * x))
+        if self.f0 is None:
+            return env
+        return env * np.cos(2.0 * np.pi * self.f0 * (t - self.t0))
+
+
+def _sample(waveform, t):
+    try:
+        v = waveform(np.asarray(t, dtype=np.float64))
+        v = np.asarray(v, dtype=np.float64)
+        if v.shape == np.shape(t):
+            return v
+    except Exception:
+        pass
+    return np.array([float(waveform(float(x))) for x in np.ravel(t)])
+
+
+class TdSession:
+    """The DGTD operator on the GPU with its steppers and runs (td.rs:163)."""
+
+    def __init__(self, op: O.MaxwellOperator, c: float = 1.0, device: int = 0, ports=None):
+        self.op = op
+        self.c = float(c)
+        self.ctx = _ctx(device)
+        self.gop = G.GpuOperator(self.ctx, op)
+        self._cfl_h = None
+        self._ports = ports or {}
+
+    # ---- construction (td.rs:191-208)
+    @staticmethod
+    def box_cavity(nx, ny, nz, lx, ly, lz, order, flux="upwind", c=1.0):
+        mesh = O.structured_box(nx, ny, nz, lx, ly, lz)
+        return TdSession(O.MaxwellOperator(mesh, order, flux_alpha(flux)), c)
+
+    @staticmethod
+    def from_mesh(mesh: O.Mesh, order, flux="upwind", c=1.0, materials=None, ports=None):
+        """An operator on an arbitrary tet mesh.  `ports` maps a port name to
+        {"faces": bool [K,4], "inward_normal": (x,y,z), "mode": (m,n) or None}."""
+        face_port = None
+        port_ids = {}
+        if ports:
+            face_port = -np.ones((mesh.n_tets, 4), dtype=np.int32)
+            for k, (name, spec) in enumerate(ports.items()):
+                face_port[np.asarray(spec["faces"], dtype=bool)] = k
+                port_ids[name] = (k, spec)
+        op = O.MaxwellOperator(mesh, order, flux_alpha(flux), face_port=face_port, materials=materials)
+        return TdSession(op, c, ports=port_ids)
+
+    # ---- sizes
+    def n_dofs(self) -> int:
+        return self.op.n_dof
+
+    def n_tets(self) -> int:
+        return self.op.n_elem
+
+    def gpu_available(self) -> bool:
+        return True
+
+    def _check(self, what, y):
+        y = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        if y.size != self.n_dofs():
+            raise ValueError(f"{what} has {y.size} entries, expected n_dof = {self.n_dofs()}")
+        return y
+
+    # ---- the ODE
+    def apply(self, y) -> np.ndarray:
+        """A*y (f32 on the device, returned as f64)."""
+        return self.gop.apply(self._check("y", y)).astype(np.float64)
+
+    def field_energy(self, y) -> float:
+        from ._native import check, lib
+        import ctypes as C
+        e = C.c_double()
+        check(lib.dgtd_field_energy(self.gop.handle, self._check("y", y), C.byref(e)))
+        return e.value
+
+    # ---- steps
+    def step(self, y, h, krylov_dim=40, tol=None):
+        """exp(h A) y by the device Krylov propagator (td.rs:235-239)."""
+        tol = KRYLOV_TOL if tol is None else float(tol)
+        out, _ = self.gop.expmv(self._check("y", y), self.c * float(h), int(krylov_dim), tol)
+        return out
+
+    def step_explicit(self, y, h):
+        """One LSERK4 step of h (td.rs:242-244)."""
+        return self.gop.transient(self._check("y", y), self.c * float(h), 1, 1).astype(np.float64)
+
+    def cfl_dt(self, recompute=False) -> float:
+        """The largest stable LSERK4 step in physical time (session.rs:514-569)."""
+        if self._cfl_h is None or recompute:
+            from ._native import check, lib
+            import ctypes as C
+            h = C.c_double()
+            check(lib.dgtd_cfl_dt(self.gop.handle, C.byref(h), None, None))
+            self._cfl_h = h.value
+        return self._cfl_h / self.c
+
+    def nearest_node_dof(self, point, field, component) -> int:
+        f = {"E": 0, "H": 1}.get(field)
+        if f is None:
+            raise ValueError(f"field must be 'E' or 'H', got {field!r}")
+        cpt = {"x": 0, "y": 1, "z": 2}.get(component)
+        if cpt is None:
+            raise ValueError(f"component must be 'x', 'y' or 'z', got {component!r}")
+        return self.op.nearest_node_dof(point, f, cpt)
+
+    def port_source(self, name):
+        k, spec = self._ports[name]
+        if spec.get("mode") is None:
+            return np.zeros(self.n_dofs())
+        prof = self.op.rect_port_profiles(k, spec["inward_normal"], spec["mode"])
+        return self.op.port_source(k, prof)
+
+    # ---- runs
+    def transient(self, y0=None, *, dt, steps, source_dof=None, port=None, waveform=None, probes=None,
+                  method=None, device="gpu", krylov_dim=40, warmup=0, verbose=True):
+        """A run of `steps` frames of `dt` (td.rs:281-324, session.rs:620-777).
+        Returns (frames [steps+1, n_dof or len(probes)], None)."""
+        if device not in ("gpu", "cuda"):
+            raise ValueError("rapidfem_b200 runs the DGTD path on the GPU only (device='gpu')")
+        method = method or "explicit"
+        if method not in ("exponential", "explicit"):
+            raise ValueError("method must be 'exponential' or 'explicit'")
+        if not (math.isfinite(dt) and dt > 0.0):
+            raise ValueError(f"dt must be positive, got {dt}")
+        if source_dof is not None and port is not None:
+            raise ValueError("pass either source= (point) or port= (modal port), not both")
+        n = self.n_dofs()
+        if source_dof is not None and not 0 <= source_dof < n:
+            raise ValueError(f"source DOF {source_dof} out of range (n_dof = {n})")
+        drive = None
+        if source_dof is not None:
+            drive = ("point", int(source_dof))
+        elif port is not None:
+            drive = ("vector", self.port_source(port))
+        if drive is not None and waveform is None:
+            raise ValueError("a driven run needs a waveform")
+        if probes is not None:
+            probes = [int(p) for p in probes]
+            bad = [p for p in probes if not 0 <= p < n]
+            if bad:
+                raise ValueError(f"probe DOF {bad[0]} out of range (n_dof = {n})")
+        warmup = min(int(warmup), steps)
+        y = np.zeros(n) if y0 is None else self._check("y0", y0)
+        rows = [y[probes] if probes is not None else y.copy()]
+
+        def push(v):
+            rows.append(v[probes] if probes is not None else np.asarray(v, dtype=np.float64).copy())
+
+        exp_frames = steps if method == "exponential" else warmup
+        for k in range(exp_frames):
+            g = 0.0 if drive is None else float(_sample(waveform, np.array([k * dt]))[0])
+            if drive is None:
+                y, _ = self.gop.expmv(y, self.c * dt, krylov_dim, KRYLOV_TOL)
+            else:
+                b = np.zeros(n)
+                if drive[0] == "point":
+                    b[drive[1]] = g
+                else:
+                    b = drive[1] * g
+                y, _ = self.gop.etd_step(y, b, self.c * dt, krylov_dim, KRYLOV_TOL)
+            push(y)
+        if method == "explicit" and warmup < steps:
+            nsub = max(1, math.ceil(dt / self.cfl_dt()))
+            _log(verbose, f"transient: explicit LSERK4 on the GPU ({nsub} substeps/step)")
+            h_sub = dt / nsub
+            kk = steps - warmup
+            g = None
+            if drive is not None:
+                t = (warmup * nsub + np.arange(kk * nsub)) * h_sub
+                g = _sample(waveform, t)
+            if probes is not None:
+                series, yf = self.gop.transient_probes(y, self.c * dt, kk, nsub, drive=drive, g=g, probes=probes)
+                rows.extend(list(series[1:].astype(np.float64)))
+                y = yf.astype(np.float64)
+            else:
+                traj = self.gop.transient(y, self.c * dt, kk, nsub, drive=drive, g=g, record=True)
+                rows.extend(list(traj[1:].astype(np.float64)))
+                y = traj[-1].astype(np.float64)
+        return np.array(rows), None
+
+
+class ProblemTD:
+    """problem/td.py:195-750 on the B200 path (box cavities and tet meshes)."""
+
+    def __init__(self, mesh: O.Mesh, *, order=2, flux="upwind", c=C_LIGHT, materials=None, ports=None):
+        self.c = float(c)
+        self._op = TdSession.from_mesh(mesh, order, flux, self.c, materials, ports)
+        self.order = order
+        self.flux = flux
+
+    @classmethod
+    def box(cls, *, size, cells, order=2, flux="upwind", c=1.0):
+        lx, ly, lz = size
+        nx, ny, nz = cells
+        obj = cls.__new__(cls)
+        obj._op = TdSession.box_cavity(nx, ny, nz, lx, ly, lz, order, flux, float(c))
+        obj.order, obj.flux, obj.c = order, flux, float(c)
+        obj.size, obj.cells = tuple(size), tuple(cells)
+        return obj
+
+    @property
+    def n_dofs(self):
+        return self._op.n_dofs()
+
+    @property
+    def n_tets(self):
+        return self._op.n_tets()
+
+    def rhs(self, y):
+        return self._op.apply(y)
+
+    def field_energy(self, state):
+        return self._op.field_energy(state)
+
+    def step(self, y, h, krylov_dim=40, tol=None):
+        return self._op.step(y, float(h), int(krylov_dim), tol)
+
+    def step_explicit(self, y, h):
+        return self._op.step_explicit(y, float(h))
+
+    def cfl_dt(self, *, recompute=False):
+        return self._op.cfl_dt(recompute)
+
+    def probe_dof(self, point, *, field="E", component="z"):
+        return self._op.nearest_node_dof(tuple(float(x) for x in point), field, component)
+
+    def driven_transient(self, *, source, waveform, probes, dt, steps, krylov_dim=40, device="gpu",
+                         method="explicit", verbose=True):
+        src = self.probe_dof(source[0], field=source[1], component=source[2])
+        pr = [self.probe_dof(p[0], field=p[1], component=p[2]) for p in probes]
+        frames, _ = self._op.transient(None, dt=float(dt), steps=int(steps), source_dof=src, waveform=waveform,
+                                       probes=pr, device=device, method=method, krylov_dim=int(krylov_dim),
+                                       verbose=verbose)
+        return np.arange(steps + 1) * dt, frames.T
+
+    def transient(self, y0=None, *, dt, steps, source=None, waveform=None, port=None, krylov_dim=40,
+                  method="exponential", warmup=0, device="gpu", verbose=True):
+        src = None if source is None else self.probe_dof(source[0], field=source[1], component=source[2])
+        frames, _ = self._op.transient(y0, dt=float(dt), steps=int(steps), source_dof=src, port=port,
+                                       waveform=waveform, method=method, device=device,
+                                       krylov_dim=int(krylov_dim), warmup=int(warmup), verbose=verbose)
+        return frames
