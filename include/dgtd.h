@@ -161,6 +161,20 @@ int dgtd_set_source_vector(dgtd_op *op, const double *src_vec);
 /* dy = A*y on device AoS pointers (f32). */
 int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
 
+/* `steps` free LSERK4 steps of `h` from the device AoS state d_y_in into
+ * d_y_out (both n_dof floats, may alias), allocating nothing.  No counterpart
+ * in the reference: it serves callers that cannot let a library call
+ * cudaMalloc (hosts whose framework owns the device memory budget).  The
+ * scratch -- two SoA state buffers and the residual register -- is a
+ * file-scope device array of 3 x 2,097,152 floats (24 MiB) that every GPU
+ * loading the library holds until exit; ops with n_dof above 2,097,152 are
+ * rejected with DGTD_ERR_BAD_ARG.  The first call on a device takes the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the one array: calls whose work
+ * overlaps on the GPU (other streams, other threads) race.  The work is queued
+ * on the op's stream; synchronise before reading d_y_out. */
+int dgtd_run_lserk_static(dgtd_op *op, const float *d_y_in, float *d_y_out, float h, int64_t steps);
+
 /* ---- session helpers --------------------------------------------------
  * TdSession::cfl_dt (session.rs:514-569) on the device: rho(A) by 40 power
  * iterations from the reference's deterministic start vector (splitmix64 +

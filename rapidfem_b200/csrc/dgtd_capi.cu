@@ -1064,3 +1064,74 @@ extern "C" int dgtd_state_energy(dgtd_op* op, double* energy) {
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   return energy_of<float>(op, op->y[op->cur].p, energy);
 }
+
+// ------------------------------------------------------------------ no-allocation LSERK4
+//
+// A variant of the fused LSERK4 stage path for callers that must not have the
+// library allocate device memory: hosts whose framework owns the device memory
+// budget (a caching allocator that has reserved the GPU, a fixed-budget service
+// that forbids allocations after start-up) and so cannot let a library call
+// cudaMalloc / cudaFree.  The caller passes the input and output states; the
+// scratch this path needs -- two element-major SoA state buffers that the
+// stages ping-pong between and the LSERK residual register p -- is the
+// file-scope array below.  It is sized for at most kStaticMaxDof degrees of
+// freedom, and every GPU that loads this library holds it (24 MiB) until the
+// process exits.
+
+namespace {
+constexpr int64_t kStaticMaxDof = int64_t(1) << 21;  // 2,097,152 DOFs
+static __device__ __align__(256) float g_lserk_scratch[3 * kStaticMaxDof];
+std::mutex g_lserk_scratch_mu;
+float* g_lserk_scratch_ptr[64] = {nullptr};
+
+// Device address of g_lserk_scratch on the current device.  In host code the
+// symbol names a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, taken once per device with that device current.
+int lserk_scratch(int device, float** out) {
+  if (device < 0 || device >= 64) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: device index above 63");
+  std::lock_guard<std::mutex> lock(g_lserk_scratch_mu);
+  if (!g_lserk_scratch_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_lserk_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(DGTD_ERR_CUDA, std::string("run_lserk_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_lserk_scratch_ptr[device] = static_cast<float*>(p);
+  }
+  *out = g_lserk_scratch_ptr[device];
+  return DGTD_OK;
+}
+}  // namespace
+
+extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_y_out, float h, int64_t steps) {
+  if (!op || !d_y_in || !d_y_out || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: bad argument");
+  if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: step must be positive");
+  if (op->n_dof > kStaticMaxDof)
+    return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: n_dof " + std::to_string(op->n_dof) +
+                                           " exceeds the static scratch limit of " + std::to_string(kStaticMaxDof) +
+                                           " DOFs; use dgtd_run_lserk");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  float* base = nullptr;
+  DGTD_TRY(lserk_scratch(op->ctx->device, &base));
+  // The residual register is written before it is read in every step (stage
+  // 0 has a = 0 and does not read it), so nothing left by an earlier call is
+  // ever used and no clearing is needed.
+  float* ya = base;
+  float* yb = base + kStaticMaxDof;
+  float* pr = base + 2 * kStaticMaxDof;
+  DGTD_TRY((to_soa<float, float>(op, d_y_in, ya)));
+  for (int64_t k = 0; k < steps; ++k)
+    for (int s = 0; s < 5; ++s) {
+      RhsParams P = base_params(op);
+      P.y_in = ya;
+      P.out = yb;
+      P.p = pr;
+      P.a = (float)kLserkA[s];
+      P.b = (float)kLserkB[s];
+      P.dt = h;
+      P.read_p = s > 0;
+      P.write_p = s < 4;
+      DGTD_TRY(launch_rhs<kModeLserk>(op, P));
+      std::swap(ya, yb);
+    }
+  return to_aos<float, float>(op, ya, d_y_out);
+}
