@@ -22,6 +22,7 @@
 #include "host/errors.h"
 #include "krylov.cuh"
 #include "rhs_fp32.cuh"
+#include "tc_selftest.cuh"
 
 // ------------------------------------------------------------------ errors
 
@@ -1134,4 +1135,36 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
       std::swap(ya, yb);
     }
   return to_aos<float, float>(op, ya, d_y_out);
+}
+
+// ------------------------------------------------------------------ tensor-core self test
+
+extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b, float* c, int32_t n, int32_t k,
+                                  int32_t split3) {
+  if (!ctx || !a || !b || !c || n < 16 || n > dgtd::kSelftestMaxN || (n % 16) || k < 8 ||
+      k > dgtd::kSelftestMaxK || (k % 8))
+    return set_error(DGTD_ERR_BAD_ARG, "debug_tc_gemm: need 16 <= N <= 256 (N % 16 == 0), 8 <= K <= 64 (K % 8 == 0)");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  DevBuf<float> da, db, dc;
+  DevBuf<int> derr;
+  DGTD_TRY(da.alloc((size_t)128 * k));
+  DGTD_TRY(db.alloc((size_t)n * k));
+  DGTD_TRY(dc.alloc((size_t)128 * n));
+  DGTD_TRY(derr.alloc(1));
+  cudaStream_t s = ctx->stream;
+  CUDA_TRY(cudaMemcpyAsync(da.p, a, (size_t)128 * k * 4, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(db.p, b, (size_t)n * k * 4, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemsetAsync(dc.p, 0, (size_t)128 * n * 4, s));
+  CUDA_TRY(cudaMemsetAsync(derr.p, 0, 4, s));
+  const size_t smem = (size_t)(2 * 128 * k + 2 * n * k) * 4;
+  CUDA_TRY(cudaFuncSetAttribute(dgtd::k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dgtd::k_tc_selftest<<<1, 128, smem, s>>>(da.p, db.p, dc.p, n, k, split3, derr.p);
+  CUDA_TRY(cudaGetLastError());
+  int herr = 0;
+  CUDA_TRY(cudaMemcpyAsync(c, dc.p, (size_t)128 * n * 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&herr, derr.p, 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  da.free(); db.free(); dc.free(); derr.free();
+  if (herr) return set_error(DGTD_ERR_TIMEOUT, "debug_tc_gemm: MMA completion wait timed out");
+  return DGTD_OK;
 }

@@ -1,0 +1,89 @@
+// tc_selftest.cuh -- a one-CTA tcgen05 GEMM through the same operand layout,
+// descriptors, TMEM allocation and TMEM loads as the tensor-core RHS kernel:
+// C[128 x N] = A[128 x K] * B[N x K]^T, with the 3xTF32 split products
+// (hi*hi + hi*lo + lo*hi) or a single tf32 product.  Test hook only.
+#pragma once
+#include <cstdint>
+
+#include "tc_util.cuh"
+
+namespace dgtd {
+
+constexpr int kSelftestMaxK = 64;
+constexpr int kSelftestMaxN = 256;
+
+__global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A, const float* __restrict__ B,
+                                                     float* __restrict__ C, int N, int K, int split3,
+                                                     int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_sm[];
+  const int M = 128;
+  float* a_hi = reinterpret_cast<float*>(tc_sm);
+  float* a_lo = a_hi + M * K;
+  float* b_hi = a_lo + M * K;
+  float* b_lo = b_hi + N * K;
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t s_bar;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto put = [&](float* base, int R, int r, int k, float v) {
+    *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(base) + tc::kmajor_off(r, k, R)) = v;
+  };
+  for (int idx = tid; idx < M * K; idx += blockDim.x) {
+    const int r = idx / K, k = idx - r * K;
+    const float v = A[idx];
+    const float h = tc::to_tf32(v);
+    put(a_hi, M, r, k, h);
+    put(a_lo, M, r, k, tc::to_tf32(v - h));
+  }
+  for (int idx = tid; idx < N * K; idx += blockDim.x) {
+    const int r = idx / K, k = idx - r * K;
+    const float v = B[idx];
+    const float h = tc::to_tf32(v);
+    put(b_hi, N, r, k, h);
+    put(b_lo, N, r, k, tc::to_tf32(v - h));
+  }
+  uint32_t ncols = 32;
+  while ((int)ncols < N) ncols <<= 1;
+  if (warp == 0) tc::tmem_alloc(&s_tmem, ncols);
+  if (tid == 0) {
+    tc::mbar_init(&s_bar, 1);
+    tc::mbar_fence_init();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    const uint32_t id = tc::idesc_tf32(M, N);
+    const uint32_t ah = tc::smem_u32(a_hi), al = tc::smem_u32(a_lo);
+    const uint32_t bh = tc::smem_u32(b_hi), bl = tc::smem_u32(b_lo);
+    for (int ks = 0; ks < K / 8; ++ks) {
+      tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
+      if (split3) {
+        tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, N, ks), id, 1u);
+        tc::mma_tf32(tmem, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, N, ks), id, 1u);
+      }
+    }
+    tc::mma_commit(&s_bar);
+  }
+  __syncwarp();
+  const bool ok = tc::mbar_wait(&s_bar, 0, 1u << 24);
+  if (!ok && lane == 0) atomicExch(err, 1);
+  tc::tc_fence_after();
+  if (ok) {
+    const int row = warp * 32 + lane;
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      float v[8];
+      tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (c0 + q < N) C[row * N + c0 + q] = v[q];
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+}  // namespace dgtd
