@@ -206,6 +206,10 @@ int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
  * 16 <= n <= 256 (n % 16 == 0), 8 <= k <= 64 (k % 8 == 0). */
 int dgtd_debug_tc_gemm(dgtd_ctx *ctx, const float *a, const float *b, float *c, int32_t n, int32_t k,
                        int32_t split3);
+/* Per-phase cycle counters of the tensor-core RHS kernel (8 u64 in device
+ * memory, accumulated by thread 0 of every CTA); recorded only by builds
+ * compiled with -DDGTD_TC_PHASE_TIMERS, ignored otherwise.  NULL detaches. */
+int dgtd_debug_set_phase_clock(dgtd_op *op, void *d_counters);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "_lib", "librapidfem_b200.so")
+LIB_PATH = os.environ.get("DGTD_LIB_PATH") or os.path.join(_PKG, "_lib", "librapidfem_b200.so")
 
 DGTD_OK = 0
 ERR_NAMES = {

@@ -22,6 +22,7 @@
 #include "host/errors.h"
 #include "krylov.cuh"
 #include "rhs_fp32.cuh"
+#include "rhs_tc.cuh"
 #include "tc_selftest.cuh"
 
 // ------------------------------------------------------------------ errors
@@ -170,6 +171,11 @@ struct dgtd_op {
   // energy: reference mass matrix (f64) and |det J| per element
   DevBuf<double> mass, absdet;
   bool has_mass = false;
+  // tensor-core engine: element count padded to whole tiles, pre-split operands
+  int64_t n_elem_pad = 0;
+  DevBuf<float> tc_bvol, tc_blift;
+  DevBuf<int> err;
+  unsigned long long* phase_clk = nullptr;  // instrumented builds: per-phase cycle counters
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
@@ -178,6 +184,7 @@ struct dgtd_op {
     y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
     kst.free(); skip.free(); mass.free(); absdet.free();
+    tc_bvol.free(); tc_blift.free(); err.free();
   }
 };
 
@@ -216,6 +223,9 @@ int grid_for(int64_t n, int threads, int num_sms) {
   int64_t g = (n + threads - 1) / threads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)num_sms * 8));
 }
+
+// Length of a device state buffer: whole tensor-core tiles plus 4 floats of slack.
+size_t state_len(const dgtd_op* op) { return (size_t)op->n_elem_pad * 6 * op->np + 4; }
 
 int64_t aos_to_soa_index(int64_t dof, int np) {
   const int64_t per = 6LL * np;
@@ -261,8 +271,37 @@ int launch_rhs_n(dgtd_op* op, const RhsParams& P) {
   return DGTD_OK;
 }
 
+template <int N, int MODE>
+int launch_rhs_tc_n(dgtd_op* op, const RhsParams& P) {
+  using C = TcCfg<N>;
+  static bool attr[8] = {false};
+  auto kern = rhs_tc_kernel<N, MODE>;
+  if (!attr[op->ctx->device & 7]) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    attr[op->ctx->device & 7] = true;
+  }
+  TcTables T{op->tc_bvol.p, op->tc_blift.p, op->fnodes.p, op->gtab.p, op->n_gather};
+  const int64_t tiles = op->n_elem_pad / C::E;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms);
+  kern<<<grid, kTcThreadsAll, C::SMEM, op->stream()>>>(P, T, tiles, op->err.p);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
 template <int MODE>
 int launch_rhs(dgtd_op* op, const RhsParams& P) {
+  if constexpr (MODE == kModeApply || MODE == kModeLserk) {
+    if (op->engine == DGTD_ENGINE_TF32X3) {
+      switch (op->order) {
+        case 1: return launch_rhs_tc_n<1, MODE>(op, P);
+        case 2: return launch_rhs_tc_n<2, MODE>(op, P);
+        case 3: return launch_rhs_tc_n<3, MODE>(op, P);
+        case 4: return launch_rhs_tc_n<4, MODE>(op, P);
+        default: return set_error(DGTD_ERR_UNSUPPORTED, "tensor-core engine covers orders 1..4");
+      }
+    }
+  }
   switch (op->order) {
     case 1: return launch_rhs_n<1, MODE>(op, P);
     case 2: return launch_rhs_n<2, MODE>(op, P);
@@ -280,6 +319,7 @@ RhsParams base_params(dgtd_op* op) {
   P.n_elem = op->n_elem;
   P.src_idx = -1;
   P.alpha = op->alpha;
+  P.phase_clk = op->phase_clk;
   return P;
 }
 
@@ -325,7 +365,20 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   const int N = d->order, np = dgtd::np_of(N), nfp = dgtd::nfp_of(N);
   const int64_t K = d->n_elem;
   // Host-side packing: element records, gather tables.
-  std::vector<float> meta((size_t)K * dgtd::kMetaWords, 0.f);
+  const int64_t Kpad = ((K + dgtd::kTcTileE - 1) / dgtd::kTcTileE) * dgtd::kTcTileE;
+  std::vector<float> meta((size_t)Kpad * dgtd::kMetaWords, 0.f);
+  {
+    // inert padding records: every face a PEC wall with zero normal / scale / metric
+    const uint32_t pec = (uint32_t)dgtd::kPec << 8;
+    const uint32_t w = pec | (pec << 16);
+    const int32_t none = -1;
+    for (int64_t e = K; e < Kpad; ++e) {
+      float* M = &meta[(size_t)e * dgtd::kMetaWords];
+      for (int f = 0; f < 4; ++f) std::memcpy(&M[37 + f], &none, 4);
+      std::memcpy(&M[41], &w, 4);
+      std::memcpy(&M[42], &w, 4);
+    }
+  }
   std::map<std::vector<uint8_t>, int> table_id;
   std::vector<uint8_t> gtab;
   for (int f = 0; f < 4; ++f)
@@ -403,11 +456,14 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   op->n_dof = 6 * (int64_t)np * K;
   op->alpha = (float)d->flux_alpha;
   op->n_gather = (int)table_id.size();
+  op->n_elem_pad = Kpad;
+  const size_t nstate = (size_t)Kpad * 6 * np + 4;
   auto fail = [&](int code) { delete op; return code; };
   int st;
   if ((st = op->meta.alloc(meta.size())) || (st = op->dT.alloc(dT.size())) || (st = op->liftT.alloc(liftT.size())) ||
       (st = op->fnodes.alloc(fnodes.size())) || (st = op->gtab.alloc(gtab.size())) ||
-      (st = op->y[0].alloc(op->n_dof + 4)) || (st = op->y[1].alloc(op->n_dof + 4)) || (st = op->p.alloc(op->n_dof + 4)))
+      (st = op->y[0].alloc(nstate)) || (st = op->y[1].alloc(nstate)) || (st = op->p.alloc(nstate)) ||
+      (st = op->err.alloc(1)))
     return fail(st);
   cudaStream_t s = ctx->stream;
   cudaError_t e = cudaSuccess;
@@ -419,6 +475,50 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   if (!e) e = cudaMemsetAsync(op->y[0].p, 0, op->y[0].n * 4, s);
   if (!e) e = cudaMemsetAsync(op->y[1].p, 0, op->y[1].n * 4, s);
   if (!e) e = cudaMemsetAsync(op->p.p, 0, op->p.n * 4, s);
+  if (!e) e = cudaMemsetAsync(op->err.p, 0, sizeof(int), s);
+  if (!e && N <= 4) {
+    // 3xTF32 constant operands: tf32 hi/lo of D_k (rows (k,i), K = node j) and
+    // LIFT (rows i, K = face node s), chunk-major K-major layout.
+    auto tf32 = [](double x) {
+      float f = (float)x;
+      uint32_t b;
+      std::memcpy(&b, &f, 4);
+      if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x1000u) & 0xffffe000u;
+      std::memcpy(&f, &b, 4);
+      return f;
+    };
+    auto build = [&](int R, int Kc, auto value, std::vector<float>& out) {
+      out.assign((size_t)2 * R * Kc, 0.f);
+      for (int r = 0; r < R; ++r)
+        for (int k = 0; k < Kc; ++k) {
+          const double v = value(r, k);
+          const float h = tf32(v);
+          const float l = tf32(v - (double)h);
+          const size_t o = dgtd::tc::kmajor_off(r, k, R) / 4;
+          out[o] = h;
+          out[(size_t)R * Kc + o] = l;
+        }
+    };
+    // LIFT K is laid out per face, each face padded to KLF = Nfp rounded up to 8,
+    // so the MMAs of a face pair can start while the other pair's flux is formed.
+    const int KV = dgtd::tc_r8(np), NV = dgtd::tc_r16(3 * np), KLF = dgtd::tc_r8(nfp), KL = 4 * KLF;
+    const int NL = dgtd::tc_r16(np);
+    std::vector<float> bv, bl;
+    build(NV, KV, [&](int r, int k) -> double {
+      if (r >= 3 * np || k >= np) return 0.0;
+      const int kk = r / np, i = r - kk * np;
+      return D[kk][i * np + k];
+    }, bv);
+    build(NL, KL, [&](int r, int k) -> double {
+      const int f = k / KLF, m = k - f * KLF;
+      if (r >= np || m >= nfp) return 0.0;
+      return d->lift[r * 4 * nfp + f * nfp + m];
+    }, bl);
+    if ((st = op->tc_bvol.alloc(bv.size())) || (st = op->tc_blift.alloc(bl.size()))) return fail(st);
+    e = cudaMemcpyAsync(op->tc_bvol.p, bv.data(), bv.size() * 4, cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaMemcpyAsync(op->tc_blift.p, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaStreamSynchronize(s);
+  }
   if (!e && d->mass) {
     // |det J| = 1/|det J^-1| from the f64 J^-1 of the descriptor.
     std::vector<double> absdet((size_t)K);
@@ -456,7 +556,7 @@ extern "C" int dgtd_op_n_dof(const dgtd_op* op, int64_t* n) {
 
 extern "C" int dgtd_op_set_engine(dgtd_op* op, int engine) {
   if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_set_engine: null op");
-  if (engine == DGTD_ENGINE_FP32) {
+  if (engine == DGTD_ENGINE_FP32 || (engine == DGTD_ENGINE_TF32X3 && op->order <= 4)) {
     op->engine = engine;
     return DGTD_OK;
   }
@@ -485,6 +585,18 @@ extern "C" int dgtd_op_reset_launch_count(dgtd_op* op) {
 
 static int ensure_aos32(dgtd_op* op) { return op->aos32.alloc(op->n_dof + 4); }
 
+// A tensor-core kernel that gave up a bounded wait leaves a flag; report it.
+static int check_kernel_flag(dgtd_op* op) {
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, op->err.p, sizeof(int), cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  if (h) {
+    cudaMemsetAsync(op->err.p, 0, sizeof(int), op->stream());
+    return set_error(DGTD_ERR_TIMEOUT, "a tensor-core kernel gave up waiting for its copies / MMAs");
+  }
+  return DGTD_OK;
+}
+
 extern "C" int dgtd_state_load_device(dgtd_op* op, const float* d_y) {
   if (!op || !d_y) return set_error(DGTD_ERR_BAD_ARG, "state_load_device: null argument");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
@@ -512,13 +624,14 @@ extern "C" int dgtd_state_download(dgtd_op* op, float* y) {
   DGTD_TRY((to_aos<float, float>(op, op->y[op->cur].p, op->aos32.p)));
   CUDA_TRY(cudaMemcpyAsync(y, op->aos32.p, op->n_dof * 4, cudaMemcpyDeviceToHost, op->stream()));
   CUDA_TRY(cudaStreamSynchronize(op->stream()));
-  return DGTD_OK;
+  return check_kernel_flag(op);
 }
 
 extern "C" int dgtd_set_source_vector(dgtd_op* op, const double* src) {
   if (!op || !src) return set_error(DGTD_ERR_BAD_ARG, "set_source_vector: null argument");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
-  DGTD_TRY(op->src_vec.alloc(op->n_dof + 4));
+  DGTD_TRY(op->src_vec.alloc(state_len(op)));
+  CUDA_TRY(cudaMemsetAsync(op->src_vec.p, 0, state_len(op) * 4, op->stream()));
   DGTD_TRY(op->tmp64.alloc(op->n_dof));
   CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, src, op->n_dof * 8, cudaMemcpyHostToDevice, op->stream()));
   DGTD_TRY((to_soa<double, float>(op, op->tmp64.p, op->src_vec.p)));
@@ -585,7 +698,7 @@ extern "C" int dgtd_apply(dgtd_op* op, const float* y, float* dy) {
   DGTD_TRY(dgtd_apply_device(op, d_in, op->aos32.p));
   CUDA_TRY(cudaMemcpyAsync(dy, op->aos32.p, op->n_dof * 4, cudaMemcpyDeviceToHost, op->stream()));
   CUDA_TRY(cudaStreamSynchronize(op->stream()));
-  return DGTD_OK;
+  return check_kernel_flag(op);
 }
 
 extern "C" int dgtd_transient_probes(dgtd_op* op, const float* y0, float dt, int64_t steps,
@@ -966,8 +1079,10 @@ extern "C" int dgtd_power_rho(dgtd_op* op, int32_t iters, double* rho) {
   if (!op || !rho || iters < 1) return set_error(DGTD_ERR_BAD_ARG, "power_rho: bad argument");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   DevBuf<float> v, t;
-  DGTD_TRY(v.alloc(op->n_dof + 4));
-  DGTD_TRY(t.alloc(op->n_dof + 4));
+  DGTD_TRY(v.alloc(state_len(op)));
+  DGTD_TRY(t.alloc(state_len(op)));
+  CUDA_TRY(cudaMemsetAsync(v.p, 0, state_len(op) * 4, op->stream()));
+  CUDA_TRY(cudaMemsetAsync(t.p, 0, state_len(op) * 4, op->stream()));
   int st = start_vector(op, v.p);
   if (st == DGTD_OK) st = power_iterate(op, v.p, t.p, iters, rho);
   cudaStreamSynchronize(op->stream());
@@ -981,8 +1096,10 @@ extern "C" int dgtd_cfl_dt(dgtd_op* op, double* h_out, double* rho_out, double* 
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   DevBuf<float> probe, tmp;
   DevBuf<int> bad;
-  DGTD_TRY(probe.alloc(op->n_dof + 4));
-  DGTD_TRY(tmp.alloc(op->n_dof + 4));
+  DGTD_TRY(probe.alloc(state_len(op)));
+  DGTD_TRY(tmp.alloc(state_len(op)));
+  CUDA_TRY(cudaMemsetAsync(probe.p, 0, state_len(op) * 4, op->stream()));
+  CUDA_TRY(cudaMemsetAsync(tmp.p, 0, state_len(op) * 4, op->stream()));
   DGTD_TRY(bad.alloc(1));
   double rho = 0.0;
   int st = start_vector(op, probe.p);
@@ -1106,7 +1223,8 @@ int lserk_scratch(int device, float** out) {
 extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_y_out, float h, int64_t steps) {
   if (!op || !d_y_in || !d_y_out || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: bad argument");
   if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: step must be positive");
-  if (op->n_dof > kStaticMaxDof)
+  const int64_t padded = op->n_elem_pad * 6 * op->np;  // the kernels touch whole tiles
+  if (padded > kStaticMaxDof)
     return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: n_dof " + std::to_string(op->n_dof) +
                                            " exceeds the static scratch limit of " + std::to_string(kStaticMaxDof) +
                                            " DOFs; use dgtd_run_lserk");
@@ -1119,6 +1237,11 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
   float* ya = base;
   float* yb = base + kStaticMaxDof;
   float* pr = base + 2 * kStaticMaxDof;
+  if (padded > op->n_dof) {
+    // the padding of whole tiles must hold finite values (zeros)
+    CUDA_TRY(cudaMemsetAsync(ya + op->n_dof, 0, (padded - op->n_dof) * 4, op->stream()));
+    CUDA_TRY(cudaMemsetAsync(yb + op->n_dof, 0, (padded - op->n_dof) * 4, op->stream()));
+  }
   DGTD_TRY((to_soa<float, float>(op, d_y_in, ya)));
   for (int64_t k = 0; k < steps; ++k)
     for (int s = 0; s < 5; ++s) {
@@ -1166,5 +1289,13 @@ extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b,
   CUDA_TRY(cudaStreamSynchronize(s));
   da.free(); db.free(); dc.free(); derr.free();
   if (herr) return set_error(DGTD_ERR_TIMEOUT, "debug_tc_gemm: MMA completion wait timed out");
+  return DGTD_OK;
+}
+
+// Point the tensor-core kernel's phase counters (8 x u64, device memory) at
+// `d_counters`; only builds compiled with -DDGTD_TC_PHASE_TIMERS record them.
+extern "C" int dgtd_debug_set_phase_clock(dgtd_op* op, void* d_counters) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "debug_set_phase_clock: null op");
+  op->phase_clk = static_cast<unsigned long long*>(d_counters);
   return DGTD_OK;
 }

@@ -64,6 +64,7 @@ struct RhsParams {
   float a, b, dt;          // LSERK stage coefficients
   int read_p, write_p;     // stage 0 does not read p; the last stage does not write it
   float alpha;             // flux blend
+  unsigned long long* phase_clk;  // per-phase cycle counters (instrumented builds only), or null
 };
 
 }  // namespace dgtd
