@@ -200,12 +200,13 @@ int dgtd_op_reset_launch_count(dgtd_op *op);
  * Dense exp(A) of a d x d row-major matrix (d <= 64) by the device kernel the
  * Krylov finisher uses (Taylor-18 + scaling and squaring, propagator.rs:69-114). */
 int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
-/* One-CTA tcgen05 GEMM C[128 x n] = A[128 x k] * B[n x k]^T (row-major f32) with
- * the 3xTF32 split products (split3 != 0) or one tf32 product, through the
- * operand layout, descriptors and TMEM path of the tensor-core RHS kernel.
+/* One-CTA tcgen05 GEMM C[128 x n] = A[128 x k] * B[n x k]^T (row-major f32)
+ * through the operand layout, descriptors and TMEM path of the tensor-core RHS
+ * kernel.  flags bit 0: 3xTF32 split products (else one tf32 product); bit 1:
+ * A operand in TMEM (else shared memory).
  * 16 <= n <= 256 (n % 16 == 0), 8 <= k <= 64 (k % 8 == 0). */
 int dgtd_debug_tc_gemm(dgtd_ctx *ctx, const float *a, const float *b, float *c, int32_t n, int32_t k,
-                       int32_t split3);
+                       int32_t flags);
 /* Per-phase cycle counters of the tensor-core RHS kernel (8 u64 in device
  * memory, accumulated by thread 0 of every CTA); recorded only by builds
  * compiled with -DDGTD_TC_PHASE_TIMERS, ignored otherwise.  NULL detaches. */

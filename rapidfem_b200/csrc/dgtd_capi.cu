@@ -509,11 +509,23 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
       const int kk = r / np, i = r - kk * np;
       return D[kk][i * np + k];
     }, bv);
-    build(NL, KL, [&](int r, int k) -> double {
-      const int f = k / KLF, m = k - f * KLF;
-      if (r >= np || m >= nfp) return 0.0;
-      return d->lift[r * 4 * nfp + f * nfp + m];
-    }, bl);
+    // LIFT B operand: hi rows over lo rows in one 2NL-row operand (the kernel's
+    // MMA of an A half forms both products at once).
+    {
+      std::vector<float> hl;
+      build(NL, KL, [&](int r, int k) -> double {
+        const int f = k / KLF, m = k - f * KLF;
+        if (r >= np || m >= nfp) return 0.0;
+        return d->lift[r * 4 * nfp + f * nfp + m];
+      }, hl);
+      bl.assign((size_t)2 * NL * KL, 0.f);
+      for (int r = 0; r < NL; ++r)
+        for (int k = 0; k < KL; ++k) {
+          const size_t src = dgtd::tc::kmajor_off(r, k, NL) / 4;
+          bl[dgtd::tc::kmajor_off(r, k, 2 * NL) / 4] = hl[src];
+          bl[dgtd::tc::kmajor_off(NL + r, k, 2 * NL) / 4] = hl[(size_t)NL * KL + src];
+        }
+    }
     if ((st = op->tc_bvol.alloc(bv.size())) || (st = op->tc_blift.alloc(bl.size()))) return fail(st);
     e = cudaMemcpyAsync(op->tc_bvol.p, bv.data(), bv.size() * 4, cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemcpyAsync(op->tc_blift.p, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice, s);
@@ -1263,7 +1275,7 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
 // ------------------------------------------------------------------ tensor-core self test
 
 extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b, float* c, int32_t n, int32_t k,
-                                  int32_t split3) {
+                                  int32_t flags) {
   if (!ctx || !a || !b || !c || n < 16 || n > dgtd::kSelftestMaxN || (n % 16) || k < 8 ||
       k > dgtd::kSelftestMaxK || (k % 8))
     return set_error(DGTD_ERR_BAD_ARG, "debug_tc_gemm: need 16 <= N <= 256 (N % 16 == 0), 8 <= K <= 64 (K % 8 == 0)");
@@ -1281,7 +1293,7 @@ extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b,
   CUDA_TRY(cudaMemsetAsync(derr.p, 0, 4, s));
   const size_t smem = (size_t)(2 * 128 * k + 2 * n * k) * 4;
   CUDA_TRY(cudaFuncSetAttribute(dgtd::k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dgtd::k_tc_selftest<<<1, 128, smem, s>>>(da.p, db.p, dc.p, n, k, split3, derr.p);
+  dgtd::k_tc_selftest<<<1, 128, smem, s>>>(da.p, db.p, dc.p, n, k, flags, derr.p);
   CUDA_TRY(cudaGetLastError());
   int herr = 0;
   CUDA_TRY(cudaMemcpyAsync(c, dc.p, (size_t)128 * n * 4, cudaMemcpyDeviceToHost, s));
@@ -1299,3 +1311,16 @@ extern "C" int dgtd_debug_set_phase_clock(dgtd_op* op, void* d_counters) {
   op->phase_clk = static_cast<unsigned long long*>(d_counters);
   return DGTD_OK;
 }
+
+#ifdef DGTD_TC_PHASE_TIMERS
+// Instrumented builds only: mbarrier polls of the three timed threads.
+extern "C" int dgtd_debug_tc_polls(unsigned long long* host3, int reset) {
+  if (reset) {
+    unsigned long long z[3] = {0, 0, 0};
+    CUDA_TRY(cudaMemcpyToSymbol(dgtd::g_tc_polls, z, sizeof(z)));
+    return DGTD_OK;
+  }
+  CUDA_TRY(cudaMemcpyFromSymbol(host3, dgtd::g_tc_polls, sizeof(unsigned long long) * 3));
+  return DGTD_OK;
+}
+#endif

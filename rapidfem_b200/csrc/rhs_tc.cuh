@@ -2,33 +2,31 @@
 // on the tcgen05 tensor cores (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulate
 // in TMEM).  Orders 1..4.
 //
-// One persistent CTA (24 compute warps + 1 control warp) per SM walks tiles of E = 20
-// elements.  The MMA M dimension is the 128 rows (element, component): warp
-// quarter w holds elements 5w..5w+4 in rows 32w + 6*(e%5) + c (rows 30, 31 of
-// each quarter are padding), so the six components of an element sit in one
-// warp's TMEM lanes and the curl can be combined with warp shuffles.
+// One persistent CTA per SM walks tiles of E = 20 elements.  The MMA M
+// dimension is the 128 rows (element, component): lane quarter q holds elements
+// 5q..5q+4 in rows 32q + 6*(e%5) + c (rows 30, 31 of each quarter are padding),
+// so the six components of an element sit in one warp's TMEM lanes and the
+// curl can be combined with warp shuffles.
 //
 //   volume:  C_v[(e,c)][(k,i)] = sum_j F[(e,c)][j] * D_k[i][j]        (rhs.rs:39-85)
 //   LIFT:    C_l[(e,c)][i]     = sum_s Flux[(e,c)][s] * LIFT[i][s]    (rhs.rs:1433-1439)
-// The LIFT K axis is laid out face by face, each face padded to a multiple of
-// 8, so the LIFT MMAs of faces 0-1 run while the fluxes of faces 2-3 are formed.
 //
-// Per tile:
-//   0. the tile's state (E*6*Np f32, contiguous) and element records arrive by
-//      bulk async copies issued one tile ahead (double buffered); the residual
-//      register p of the tile is bulk-copied at the start of the tile;
-//   1. the state is split into tf32 hi/lo K-major operands and the volume MMAs
-//      are issued asynchronously;
-//   2. fluxes of faces 0-1, then 2-3 (rhs.rs:1370-1441) fill the LIFT operand,
-//      each half followed by its MMAs; the last ones are committed to an mbarrier;
-//   3. each TMEM lane (one row) reads its reference derivatives and LIFT sum,
-//      forms its two curl contributions, exchanges them by shuffle, applies the
-//      material scaling (rhs.rs:1443-1454) and stages dy in shared memory;
-//   4. the mode's epilogue runs in shared memory (dy, or the LSERK4 stage update
-//      of explicit.rs:122-133 in place) and the results leave by bulk async
-//      stores, so the writes overlap the next tile.
-// The element count is padded on the device to a multiple of E with inert
-// records (PEC faces, zero metric), so every tile is full.
+// The CTA is warp-specialised so that two tiles are in flight:
+//   flux warps      build tile t's volume operand (tf32 hi/lo of the state,
+//                   written to TMEM by tcgen05.st) and its numerical fluxes
+//                   (rhs.rs:1370-1441) into the LIFT operand in shared memory;
+//   epilogue warps  finish tile t-1 from its TMEM accumulators: reference
+//                   derivatives -> curl by shuffles, LIFT sum, material scaling
+//                   (rhs.rs:1443-1454) and the mode's update in place (dy, or the
+//                   LSERK4 stage of explicit.rs:122-133 on y and p);
+//   control lane    issues the bulk async loads (state + element records three
+//                   tiles deep, residual register two deep), the MMAs of both
+//                   contractions into one of two TMEM accumulator sets, and the
+//                   bulk async stores.
+// All hand-offs are mbarriers; every wait is bounded and an expired wait stops
+// the CTA cleanly with an error flag.  The element count is padded on the
+// device to a multiple of E with inert records (PEC faces, zero metric), so
+// every tile is full.
 #pragma once
 #include <cstdint>
 
@@ -36,11 +34,11 @@
 #include "tc_util.cuh"
 
 // Phase timers: compiled in only with -DDGTD_TC_PHASE_TIMERS (an instrumented
-// build); otherwise the marks are empty.
+// build); otherwise the marks are empty.  One thread per role records.
 #ifdef DGTD_TC_PHASE_TIMERS
 #define DGTD_TC_MARK(i)                                     \
   do {                                                      \
-    if (tid == 0) {                                         \
+    if (timer_thread) {                                     \
       const long long now__ = clock64();                    \
       clk_acc[i] += (unsigned long long)(now__ - clk_last); \
       clk_last = now__;                                     \
@@ -55,15 +53,20 @@
 namespace dgtd {
 
 constexpr int kTcTileE = 20;
-constexpr int kTcThreads = 768;      // compute threads (24 warps)
-constexpr int kTcThreadsAll = 800;   // + one control warp
-constexpr int kTcGroups = kTcThreads / 128;  // epilogue node groups per TMEM lane quarter
+constexpr int kTcFluxWarps = 16;                          // warps 0..15
+constexpr int kTcEpiWarps = 8;                            // warps 16..23
+constexpr int kTcCtlWarp = kTcFluxWarps + kTcEpiWarps;    // warp 24, lane 0
+constexpr int kTcThreadsAll = (kTcCtlWarp + 1) * 32;
+constexpr int kTcFluxThreads = kTcFluxWarps * 32;
+constexpr int kTcVolGroups = kTcFluxWarps / 4;            // column groups per lane quarter
+constexpr int kTcEpiGroups = kTcEpiWarps / 4;
 constexpr uint32_t kTcWaitLimit = 1u << 24;
+static_assert(kTcFluxWarps % 4 == 0 && kTcEpiWarps % 4 == 0, "roles cover whole TMEM lane quarters");
 
 __host__ __device__ constexpr int tc_r8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int tc_r16(int x) { return (x + 15) & ~15; }
+__host__ __device__ constexpr int tc_r32(int x) { return (x + 31) & ~31; }
 __host__ __device__ constexpr int tc_r128(int x) { return (x + 127) & ~127; }
-__host__ __device__ constexpr int tc_pow2(int x) { return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ? 128 : x <= 256 ? 256 : 512; }
 
 template <int N>
 struct TcCfg {
@@ -75,48 +78,55 @@ struct TcCfg {
   static constexpr int KLF = tc_r8(NFP);      // LIFT K per face
   static constexpr int KL = 4 * KLF;          // LIFT K (face nodes, per-face padded)
   static constexpr int NL = tc_r16(NP);       // LIFT N (nodes)
-  static constexpr int TMEM_COLS = tc_pow2(NV + NL);
+  // The LIFT B operand stacks LIFT hi (rows 0..NL-1) over LIFT lo (rows NL..2NL-1),
+  // so one MMA forms both products of an A half: N = 2 NL.
+  static constexpr int NL2 = 2 * NL;
+  // TMEM columns: two accumulator sets [vol | lift hi | lift lo], then the volume
+  // A operand (hi, lo)
+  static constexpr int ACC = NV + NL2;
+  static constexpr int T_AHI = 2 * ACC;
+  static constexpr int T_ALO = T_AHI + KV;
+  static constexpr int TMEM_COLS = 512;
   static constexpr int TILE_F = E * 6 * NP;   // floats of state per tile
   static constexpr int TILE_B = TILE_F * 4;
   static constexpr int META_B = E * kMetaWords * 4;
-  // per-thread work items
-  static constexpr int ITEMS_A = (M * (KV / 4) + kTcThreads - 1) / kTcThreads;   // volume operand chunks
-  static constexpr int HALF_SLOTS = E * 2 * (KLF / 4) * 4;                       // flux slots per face pair
-  static constexpr int ITEMS_F = (HALF_SLOTS + kTcThreads - 1) / kTcThreads;
-  // byte sizes of the operands (hi or lo)
+  // per-thread work
+  static constexpr int SLOTS = E * KL;                                         // flux slots, all faces
+  static constexpr int ITEMS_F = (SLOTS + kTcFluxThreads - 1) / kTcFluxThreads;
+  static constexpr int VCH = KV / 8;                                           // volume-operand column chunks
+  static constexpr int VCH_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
+  static constexpr int ECH = (NP + 3) / 4;                                     // epilogue node chunks of 4
+  static constexpr int ECH_PER = (ECH + kTcEpiGroups - 1) / kTcEpiGroups;
+  // byte sizes of the shared-memory operands (hi or lo)
   static constexpr int BV_B = NV * KV * 4;
-  static constexpr int BL_B = NL * KL * 4;
-  static constexpr int AV_B = M * KV * 4;
+  static constexpr int BL_B = NL2 * KL * 4;   // stacked hi/lo
   static constexpr int AL_B = M * KL * 4;
+  static constexpr int YS_B = tc_r128(TILE_B);
+  static constexpr int MS_B = tc_r128(META_B);
   // shared-memory map (bytes)
   static constexpr int O_BVH = 0;
   static constexpr int O_BVL = O_BVH + tc_r128(BV_B);
-  static constexpr int O_BLH = O_BVL + tc_r128(BV_B);
-  static constexpr int O_BLL = O_BLH + tc_r128(BL_B);
-  static constexpr int O_AVH = O_BLL + tc_r128(BL_B);
-  static constexpr int O_AVL = O_AVH + tc_r128(AV_B);
-  static constexpr int O_ALH = O_AVL + tc_r128(AV_B);
+  static constexpr int O_BL = O_BVL + tc_r128(BV_B);
+  static constexpr int O_ALH = O_BL + tc_r128(BL_B);
   static constexpr int O_ALL = O_ALH + tc_r128(AL_B);
-  static constexpr int O_Y0 = O_ALL + tc_r128(AL_B);
-  static constexpr int O_Y1 = O_Y0 + tc_r128(TILE_B);
-  static constexpr int O_M0 = O_Y1 + tc_r128(TILE_B);
-  static constexpr int O_M1 = O_M0 + tc_r128(META_B);
-  static constexpr int O_P = O_M1 + tc_r128(META_B);  // residual register tile (LSERK)
-  static constexpr int O_TAB = O_P + tc_r128(TILE_B);
+  static constexpr int O_Y = O_ALL + tc_r128(AL_B);  // 3 state slots
+  static constexpr int O_M = O_Y + 3 * YS_B;           // 3 element-record slots
+  static constexpr int O_P = O_M + 3 * MS_B;           // 2 residual / output slots
+  static constexpr int O_TAB = O_P + 2 * YS_B;
   static constexpr int TAB_B = 4 * NFP + kMaxGather * NFP;
   static constexpr int SMEM = O_TAB + tc_r128(TAB_B);
-  static_assert(AL_B >= TILE_B, "dy / p staging reuses the LIFT A operand (hi half)");
+  static_assert(SMEM <= 232448 - 1024, "shared memory per CTA (dynamic + static)");
+  static_assert(T_ALO + KV <= TMEM_COLS, "TMEM columns");
   static_assert((TILE_B % 16) == 0 && (META_B % 16) == 0, "bulk copies need 16-byte sizes");
-  static_assert(NV <= 256 && NL <= 256 && NV + NL <= 512, "MMA N / TMEM limits");
-  static_assert(ITEMS_A <= 4 && ITEMS_F <= 2, "per-thread item tables");
-  static_assert((kTcThreads % 128) == 0, "compute warps cover whole TMEM lane quarters");
+  static_assert(NV <= 256 && NL2 <= 256 && (NV % 16) == 0 && (NL2 % 16) == 0, "MMA N limits");
+  static_assert(ITEMS_F <= 4 && VCH_PER <= 4 && ECH_PER <= 8, "per-thread work tables");
 };
 
 // Constant operands prepared by the host: tf32 hi/lo of D (volume B) and LIFT,
 // already in the chunk-major K-major byte layout (tc_util.cuh).
 struct TcTables {
   const float* b_vol;    // [hi | lo], each NV*KV
-  const float* b_lift;   // [hi | lo], each NL*KL (per-face padded K)
+  const float* b_lift;   // stacked [hi ; lo] rows, 2NL x KL (per-face padded K)
   const uint8_t* fnodes;
   const uint8_t* gtab;
   int n_gather;
@@ -124,6 +134,30 @@ struct TcTables {
 
 // Row of (element le, component c) in the 128-row MMA tile.
 __device__ __forceinline__ int tc_row(int le, int c) { return (le / 5) * 32 + (le % 5) * 6 + c; }
+
+// Bounded waits.  A wait gives up after kTcWaitLimit polls or once another
+// role has raised the abort flag; the warp form is warp-uniform.
+#ifdef DGTD_TC_PHASE_TIMERS
+__device__ unsigned long long g_tc_polls[3];
+#endif
+__device__ __forceinline__ bool tc_wait1(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kTcWaitLimit; ++i) {
+    if (tc::mbar_try_wait(bar, parity)) {
+#ifdef DGTD_TC_PHASE_TIMERS
+      const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+      if (l == 0 && (w == 0 || w == kTcFluxWarps || w == kTcCtlWarp))
+        atomicAdd(&g_tc_polls[w == 0 ? 0 : w == kTcFluxWarps ? 1 : 2], (unsigned long long)(i + 1));
+#endif
+      return true;
+    }
+    if ((i & 255u) == 255u && *abort_flag) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ bool tc_waitw(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  const bool ok = tc_wait1(bar, parity, abort_flag);
+  return __all_sync(0xffffffffu, ok);
+}
 
 template <int N, int MODE>
 __global__ void __launch_bounds__(kTcThreadsAll, 1)
@@ -133,36 +167,44 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   constexpr int KV = C::KV, NV = C::NV, KLF = C::KLF, NL = C::NL;
   extern __shared__ __align__(1024) unsigned char tsm[];
   __shared__ uint32_t s_tmem;
-  __shared__ __align__(8) uint64_t s_bar_ld[2];
-  __shared__ __align__(8) uint64_t s_bar_mma;
-  __shared__ __align__(8) uint64_t s_bar_p;
+  __shared__ __align__(8) uint64_t bar_ld[3];   // state + records of a slot landed
+  __shared__ __align__(8) uint64_t bar_p[2];    // residual register of a slot landed
+  __shared__ __align__(8) uint64_t bar_avol;    // flux warps: volume operand in TMEM
+  __shared__ __align__(8) uint64_t bar_alift;   // flux warps: LIFT operand in shared memory
+  __shared__ __align__(8) uint64_t bar_vdone;   // volume MMAs done (TMEM operand free)
+  __shared__ __align__(8) uint64_t bar_mma[2];  // all MMAs of an accumulator set done
+  __shared__ __align__(8) uint64_t bar_epi[2];  // epilogue of a tile done (results staged)
   __shared__ int s_abort;
+  volatile int* const abort_flag = &s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // warps 0..23 compute; warp 24 is the control warp, its lane 0 issues the
-  // MMAs and the bulk copies
-  const bool ctl = warp == kTcThreads / 32;
-  const bool ctl0 = ctl && lane == 0;
-  float* const sY0 = reinterpret_cast<float*>(tsm + C::O_Y0);
-  float* const sM0 = reinterpret_cast<float*>(tsm + C::O_M0);
-  constexpr int kYStride = (C::O_Y1 - C::O_Y0) / 4, kMStride = (C::O_M1 - C::O_M0) / 4;
-  float* const sP = reinterpret_cast<float*>(tsm + C::O_P);
-  const bool use_p = MODE == kModeLserk && P.read_p;
-  unsigned char* const avh = tsm + C::O_AVH;
-  unsigned char* const avl = tsm + C::O_AVL;
+  const bool is_flux = warp < kTcFluxWarps;
+  const bool is_epi = !is_flux && warp < kTcCtlWarp;
+  const bool ctl0 = warp == kTcCtlWarp && lane == 0;
   unsigned char* const alh = tsm + C::O_ALH;
   unsigned char* const all = tsm + C::O_ALL;
-  float* const sStage = reinterpret_cast<float*>(alh);  // p_out (or dy) staging after the MMAs
+  float* const sY0 = reinterpret_cast<float*>(tsm + C::O_Y);
+  float* const sM0 = reinterpret_cast<float*>(tsm + C::O_M);
+  float* const sP0 = reinterpret_cast<float*>(tsm + C::O_P);
+  constexpr int kYStride = C::YS_B / 4, kMStride = C::MS_B / 4;
   uint8_t* const sFn = tsm + C::O_TAB;
   uint8_t* const sG = sFn + 4 * NFP;
+  const bool use_p = MODE == kModeLserk && P.read_p;
+  const int64_t n_my =
+      n_tiles > (int64_t)blockIdx.x ? (n_tiles - (int64_t)blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
   // ---- set-up: TMEM, barriers, constant operands, tables
   if (warp == 0) tc::tmem_alloc(&s_tmem, C::TMEM_COLS);
   if (tid == 0) {
-    tc::mbar_init(&s_bar_ld[0], 1);
-    tc::mbar_init(&s_bar_ld[1], 1);
-    tc::mbar_init(&s_bar_mma, 1);
-    tc::mbar_init(&s_bar_p, 1);
+    for (int i = 0; i < 3; ++i) tc::mbar_init(&bar_ld[i], 1);
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&bar_p[i], 1);
+      tc::mbar_init(&bar_mma[i], 1);
+      tc::mbar_init(&bar_epi[i], kTcEpiWarps);
+    }
+    tc::mbar_init(&bar_avol, kTcFluxWarps);
+    tc::mbar_init(&bar_alift, kTcFluxWarps);
+    tc::mbar_init(&bar_vdone, 1);
     tc::mbar_fence_init();
     s_abort = 0;
   }
@@ -173,13 +215,9 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       reinterpret_cast<uint4*>(tsm + C::O_BVL)[i] = src[C::BV_B / 16 + i];
     }
     src = reinterpret_cast<const uint4*>(T.b_lift);
-    for (int i = tid; i < C::BL_B / 16; i += kTcThreadsAll) {
-      reinterpret_cast<uint4*>(tsm + C::O_BLH)[i] = src[i];
-      reinterpret_cast<uint4*>(tsm + C::O_BLL)[i] = src[C::BL_B / 16 + i];
-    }
+    for (int i = tid; i < C::BL_B / 16; i += kTcThreadsAll) reinterpret_cast<uint4*>(tsm + C::O_BL)[i] = src[i];
     // LIFT operand padding (rows 30/31 of each quarter, face-padding columns)
-    // must hold finite values: start from zero.  The staging that later
-    // shares the hi half writes only finite numbers.
+    // must hold finite values and is never written again: start from zero.
     for (int i = tid; i < C::AL_B / 16; i += kTcThreadsAll) {
       reinterpret_cast<uint4*>(alh)[i] = make_uint4(0, 0, 0, 0);
       reinterpret_cast<uint4*>(all)[i] = make_uint4(0, 0, 0, 0);
@@ -192,187 +230,102 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t idv = tc::idesc_tf32(M, NV), idl = tc::idesc_tf32(M, NL);
 
-  // ---- tile-invariant per-thread tables (compute threads)
-  // volume operand chunks: source offset in the state tile (-1: padding row,
-  // -2: no item), destination byte offset, K chunk
-  int a_src[C::ITEMS_A], a_dst[C::ITEMS_A], a_kc[C::ITEMS_A];
-#pragma unroll
-  for (int u = 0; u < C::ITEMS_A; ++u) {
-    const int idx = tid + u * kTcThreads;
-    a_src[u] = -2;
-    a_dst[u] = 0;
-    a_kc[u] = 0;
-    if (!ctl && idx < M * (KV / 4)) {
-      const int r = idx & (M - 1), kc = idx >> 7;
-      const int q = r >> 5, rr = r & 31;
-      a_src[u] = rr < 30 ? ((q * 5 + rr / 6) * 6 + rr % 6) * NP + kc * 4 : -1;
-      a_dst[u] = (int)tc::kmajor_off(r, kc * 4, M);
-      a_kc[u] = kc;
-    }
-  }
-  // flux slots of a face pair: (le, face within the pair, node m); le = -1 idle
-  int f_le[C::ITEMS_F], f_fl[C::ITEMS_F], f_m[C::ITEMS_F];
-#pragma unroll
-  for (int u = 0; u < C::ITEMS_F; ++u) {
-    const int q = tid + u * kTcThreads;
-    f_le[u] = -1;
-    f_fl[u] = 0;
-    f_m[u] = 0;
-    if (!ctl && q < C::HALF_SLOTS) {
-      const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = fl * (KLF/4) + mg
-      const int fl = rest / (KLF / 4), mg = rest % (KLF / 4);
-      const int m = mg * 4 + s4;
-      if (m < NFP) {
-        f_le[u] = le;
-        f_fl[u] = fl;
-        f_m[u] = m;
-      }
-    }
-  }
-  // epilogue lane: row (le, c) of warp quarter qtr; rows 30, 31 are padding.
-  // Node group grp covers nodes [grp*NPG, grp*NPG + NPG).
-  constexpr int NPG = (NP + kTcGroups - 1) / kTcGroups;
-  const int qtr = warp & 3, grp = (warp >> 2) % kTcGroups;
-  const bool lane_real = lane < 30;
-  const int e_le = qtr * 5 + (lane_real ? lane / 6 : 4);
-  const int e_c = lane_real ? lane % 6 : 5;
-  const int e_fld = e_c / 3, e_t = e_c % 3;
-  const int e_srcA = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
-  const int e_srcB = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
-  const float e_sign = e_fld == 0 ? 1.f : -1.f;
-  const int e_cA = (e_t + 2) % 3, e_cB = (e_t + 1) % 3;
-  const int e_row_off = (e_le * 6 + e_c) * NP;
-  const uint32_t e_taddr = tmem + ((uint32_t)(qtr * 32) << 16);
-
-  uint32_t ld_phase = 0u, pending = 0u, mma_phase = 0u, p_phase = 0u;
-  bool p_pending = false, mma_out = false;
 #ifdef DGTD_TC_PHASE_TIMERS
+  const bool timer_thread = lane == 0 && (warp == 0 || warp == kTcFluxWarps || warp == kTcCtlWarp);
   unsigned long long clk_acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   long long clk_last = clock64();
 #endif
 
-  int64_t tile = blockIdx.x;
-  if (ctl0 && tile < n_tiles) {
-    tc::mbar_expect_tx(&s_bar_ld[0], C::TILE_B + C::META_B);
-    tc::bulk_g2s(sY0, P.y_in + tile * C::TILE_F, C::TILE_B, &s_bar_ld[0]);
-    tc::bulk_g2s(sM0, P.meta + tile * E * kMetaWords, C::META_B, &s_bar_ld[0]);
-  }
-  if (tile < n_tiles) pending = 1u;
-
-  for (int it = 0; tile < n_tiles; tile += gridDim.x, ++it) {
-    const int buf = it & 1;
-    const int64_t next = tile + gridDim.x;
-    float* const sY = sY0 + buf * kYStride;
-    const float* const sM = sM0 + buf * kMStride;
-    const int64_t e0 = tile * E;
-    p_pending = use_p;
-    if (ctl) {
-      if (ctl0) {
-        if (use_p) {
-          tc::fence_proxy_async_smem();
-          tc::mbar_expect_tx(&s_bar_p, C::TILE_B);
-          tc::bulk_g2s(sP, P.p + tile * C::TILE_F, C::TILE_B, &s_bar_p);
-        }
-        // the previous tile's bulk stores must have finished reading the
-        // staging and state buffers before they are written again
-        tc::bulk_wait_read0();
-      }
-      __syncwarp();
-    } else {
-      DGTD_TC_MARK(0);
-      if (!tc::mbar_wait(&s_bar_ld[buf], (ld_phase >> buf) & 1u, kTcWaitLimit)) s_abort = 1;
-      DGTD_TC_MARK(1);
-      // ---- 1. volume operand: tf32 hi/lo of the state, rows (e,c), K = nodes
+  if (is_flux) {
+    // ================= flux warps: volume operand -> TMEM, fluxes -> LIFT operand
+    const int q4 = warp & 3, vg = warp >> 2;
+    const bool lane_real = lane < 30;
+    const int v_src = lane_real ? ((q4 * 5 + lane / 6) * 6 + lane % 6) * NP : 0;
+    const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
+    // flux slots q = (le, face, node-group, node-in-group); packed le | f<<8 | m<<16, -1 idle
+    int f_item[C::ITEMS_F];
 #pragma unroll
-      for (int u = 0; u < C::ITEMS_A; ++u) {
-        if (a_src[u] == -2) continue;
-        float v[4] = {0.f, 0.f, 0.f, 0.f};
-        if (a_src[u] >= 0) {
-#pragma unroll
-          for (int w = 0; w < 4; ++w)
-            if (a_kc[u] * 4 + w < NP) v[w] = sY[a_src[u] + w];
-        }
-        float4 h, l;
-        h.x = tc::to_tf32(v[0]); l.x = tc::to_tf32(v[0] - h.x);
-        h.y = tc::to_tf32(v[1]); l.y = tc::to_tf32(v[1] - h.y);
-        h.z = tc::to_tf32(v[2]); l.z = tc::to_tf32(v[2] - h.z);
-        h.w = tc::to_tf32(v[3]); l.w = tc::to_tf32(v[3] - h.w);
-        *reinterpret_cast<float4*>(avh + a_dst[u]) = h;
-        *reinterpret_cast<float4*>(avl + a_dst[u]) = l;
+    for (int u = 0; u < C::ITEMS_F; ++u) {
+      const int q = tid + u * kTcFluxThreads;
+      f_item[u] = -1;
+      if (q < C::SLOTS) {
+        const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = f * (KLF/4) + mg
+        const int f = rest / (KLF / 4), m = (rest % (KLF / 4)) * 4 + s4;
+        if (m < NFP) f_item[u] = le | (f << 8) | (m << 16);
       }
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    DGTD_TC_MARK(2);
-    if (s_abort) break;
-    ld_phase ^= 1u << buf;
-    pending &= ~(1u << buf);
-    if (next < n_tiles) pending |= 1u << (buf ^ 1);  // issued by the control warp below
-
-    // ---- 2. numerical flux into the LIFT operand, faces 0-1 then 2-3
+    int ys = 0;
+    uint32_t ld_par = 0u;  // bit s: parity of the next wait on bar_ld[s]
+    for (int64_t it = 0; it < n_my; ++it) {
+      const int64_t tile = blockIdx.x + it * gridDim.x;
+      const int64_t e0 = tile * E;
+      const float* const sY = sY0 + ys * kYStride;
+      const float* const sM = sM0 + ys * kMStride;
+      bool ok = tc_waitw(&bar_ld[ys], (ld_par >> ys) & 1u, abort_flag);
+      ld_par ^= 1u << ys;
+      if (ok && it > 0) ok = tc_waitw(&bar_vdone, (uint32_t)((it - 1) & 1), abort_flag);
+      if (!ok) {
+        *abort_flag = 1;
+        break;
+      }
+      tc::tc_fence_after();
+      DGTD_TC_MARK(0);
+      // ---- volume operand: row (e,c) of this lane, K = nodes, tf32 hi/lo -> TMEM
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      if (ctl) {
-        if (ctl0) {
-          tc::tc_fence_after();
-          if (half == 0) {
-            const uint32_t ah = tc::smem_u32(avh), al = tc::smem_u32(avl);
-            const uint32_t bh = tc::smem_u32(tsm + C::O_BVH), bl = tc::smem_u32(tsm + C::O_BVL);
-#pragma unroll 1
-            for (int ks = 0; ks < KV / 8; ++ks) {
-              tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, NV, ks), idv,
-                           ks > 0 ? 1u : 0u);
-              tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, NV, ks), idv, 1u);
-              tc::mma_tf32(tmem, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, NV, ks), idv, 1u);
-            }
-            // prefetch the next tile into the other buffer (its last reader,
-            // the previous tile's state store, has finished)
-            if (next < n_tiles) {
-              uint64_t* bar = &s_bar_ld[buf ^ 1];
-              tc::mbar_expect_tx(bar, C::TILE_B + C::META_B);
-              tc::bulk_g2s(sY0 + (buf ^ 1) * kYStride, P.y_in + next * C::TILE_F, C::TILE_B, bar);
-              tc::bulk_g2s(sM0 + (buf ^ 1) * kMStride, P.meta + next * E * kMetaWords, C::META_B, bar);
-            }
-          } else {
-            const uint32_t ah = tc::smem_u32(alh), al = tc::smem_u32(all);
-            const uint32_t bh = tc::smem_u32(tsm + C::O_BLH), bl = tc::smem_u32(tsm + C::O_BLL);
-            const uint32_t tl = tmem + (uint32_t)NV;
-            constexpr int KS_HALF = 2 * KLF / 8;
-#pragma unroll 1
-            for (int ks = 0; ks < KS_HALF; ++ks) {
-              tc::mma_tf32(tl, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, NL, ks), idl,
-                           ks > 0 ? 1u : 0u);
-              tc::mma_tf32(tl, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, NL, ks), idl, 1u);
-              tc::mma_tf32(tl, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, NL, ks), idl, 1u);
-            }
+      for (int cc = 0; cc < C::VCH_PER; ++cc) {
+        const int ch = vg + kTcVolGroups * cc;
+        if (ch < C::VCH) {
+          float h[8], l[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int k = ch * 8 + q;
+            const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+            h[q] = tc::tf32_round(v);
+            l[q] = tc::tf32_round(v - h[q]);
           }
+          tc::tmem_st8(v_taddr + (uint32_t)(C::T_AHI + ch * 8), h);
+          tc::tmem_st8(v_taddr + (uint32_t)(C::T_ALO + ch * 8), l);
         }
-        __syncwarp();
-      } else {
+      }
+      tc::tmem_st_wait();
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&bar_avol);
+      DGTD_TC_MARK(1);
+      // ---- the LIFT operand is free once the previous tile's MMAs are done
+      if (it > 0 && !tc_waitw(&bar_mma[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      DGTD_TC_MARK(2);
+      // ---- numerical flux of all four faces (rhs.rs:1370-1441), two slots at a time
+#pragma unroll
+      for (int u0 = 0; u0 < C::ITEMS_F; u0 += 2) {
+        float nb[2][6];
         // out-of-tile neighbour traces first: independent L2 requests in flight together
-        float nb[C::ITEMS_F][6];
 #pragma unroll
-        for (int u = 0; u < C::ITEMS_F; ++u) {
+        for (int v = 0; v < 2; ++v) {
 #pragma unroll
-          for (int c = 0; c < 6; ++c) nb[u][c] = 0.f;
-          if (f_le[u] < 0) continue;
-          const int f = 2 * half + f_fl[u];
-          const float* Me = sM + f_le[u] * kMetaWords;
+          for (int c = 0; c < 6; ++c) nb[v][c] = 0.f;
+          const int u = u0 + v;
+          if (u >= C::ITEMS_F || f_item[u] < 0) continue;
+          const int le = f_item[u] & 0xff, f = (f_item[u] >> 8) & 0xff, m = f_item[u] >> 16;
+          const float* Me = sM + le * kMetaWords;
           const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
           const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
           const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
           if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
-            const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + f_m[u]];
+            const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) nb[u][c] = __ldg(Z + c * NP);
+            for (int c = 0; c < 6; ++c) nb[v][c] = __ldg(Z + c * NP);
           }
         }
 #pragma unroll
-        for (int u = 0; u < C::ITEMS_F; ++u) {
-          if (f_le[u] < 0) continue;
-          const int le = f_le[u], f = 2 * half + f_fl[u], m = f_m[u];
+        for (int v = 0; v < 2; ++v) {
+          const int u = u0 + v;
+          if (u >= C::ITEMS_F || f_item[u] < 0) continue;
+          const int le = f_item[u] & 0xff, f = (f_item[u] >> 8) & 0xff, m = f_item[u] >> 16;
           const float* Me = sM + le * kMetaWords;
           const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
           const float coef = 0.5f * Me[21 + f];
@@ -395,8 +348,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
             jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
           } else {
-            float px = nb[u][0], py = nb[u][1], pz = nb[u][2];
-            float qx = nb[u][3], qy = nb[u][4], qz = nb[u][5];
+            float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
+            float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
             const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
             if (lo >= 0 && lo < E) {
               const float* Z = sY + lo * 6 * NP + sG[(code & 0xff) * NFP + m];
@@ -422,139 +375,215 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           const uint32_t off = (uint32_t)((s >> 2) * (M / 8) * 128 + (s & 3) * 4 + tc_row(le, 0) * 16);
 #pragma unroll
           for (int c = 0; c < 6; ++c) {
-            const float h = tc::to_tf32(fl[c]);
+            const float h = tc::tf32_round(fl[c]);
             *reinterpret_cast<float*>(alh + off + c * 16) = h;
-            *reinterpret_cast<float*>(all + off + c * 16) = tc::to_tf32(fl[c] - h);
+            *reinterpret_cast<float*>(all + off + c * 16) = tc::tf32_round(fl[c] - h);
           }
         }
       }
       tc::fence_proxy_async_smem();
-      __syncthreads();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&bar_alift);
       DGTD_TC_MARK(3);
+      ys = ys == 2 ? 0 : ys + 1;
     }
-    if (ctl0) {
-      tc::tc_fence_after();
-      const uint32_t ah = tc::smem_u32(alh), al = tc::smem_u32(all);
-      const uint32_t bh = tc::smem_u32(tsm + C::O_BLH), bl = tc::smem_u32(tsm + C::O_BLL);
-      const uint32_t tl = tmem + (uint32_t)NV;
-      constexpr int KS_HALF = 2 * KLF / 8;
-#pragma unroll 1
-      for (int ks = KS_HALF; ks < 2 * KS_HALF; ++ks) {
-        tc::mma_tf32(tl, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, NL, ks), idl, 1u);
-        tc::mma_tf32(tl, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, NL, ks), idl, 1u);
-        tc::mma_tf32(tl, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, NL, ks), idl, 1u);
+  } else if (is_epi) {
+    // ================= epilogue warps: TMEM -> dy -> mode update, in place
+    const int q4 = warp & 3, eg = (warp - kTcFluxWarps) >> 2;
+    const bool lane_real = lane < 30;
+    const int e_le = q4 * 5 + (lane_real ? lane / 6 : 4);
+    const int e_c = lane_real ? lane % 6 : 5;
+    const int e_fld = e_c / 3, e_t = e_c % 3;
+    const int e_srcA = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
+    const int e_srcB = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
+    const float e_sign = e_fld == 0 ? 1.f : -1.f;
+    const int e_cA = (e_t + 2) % 3, e_cB = (e_t + 1) % 3;
+    const int e_row_off = (e_le * 6 + e_c) * NP;
+    int ys = 0;
+    uint32_t ld_par = 0u;
+    for (int64_t it = 0; it < n_my; ++it) {
+      const int64_t tile = blockIdx.x + it * gridDim.x;
+      const int ps = (int)(it & 1);
+      const uint32_t ppar = (uint32_t)((it >> 1) & 1);
+      bool ok = tc_waitw(&bar_mma[ps], ppar, abort_flag);
+      if (ok) ok = tc_waitw(&bar_ld[ys], (ld_par >> ys) & 1u, abort_flag);
+      ld_par ^= 1u << ys;
+      if (ok && use_p) ok = tc_waitw(&bar_p[ps], ppar, abort_flag);
+      if (!ok) {
+        *abort_flag = 1;
+        break;
       }
-      tc::mma_commit(&s_bar_mma);
-    }
-    __syncwarp();
-    mma_out = true;
-
-    // ---- 3. epilogue from TMEM: curl by shuffles, LIFT, materials -> dy staging
-    if (!ctl) {
-      if (!tc::mbar_wait(&s_bar_mma, mma_phase, kTcWaitLimit)) s_abort = 1;
       tc::tc_fence_after();
       DGTD_TC_MARK(4);
-      const float* Me = sM + e_le * kMetaWords;
+      const float* Me = sM0 + ys * kMStride + e_le * kMetaWords;
+      // curl partials (the B one negated) and material scaling with the curl sign folded in
       const float gA0 = Me[0 * 3 + e_cA], gA1 = Me[1 * 3 + e_cA], gA2 = Me[2 * 3 + e_cA];
-      const float gB0 = Me[0 * 3 + e_cB], gB1 = Me[1 * 3 + e_cB], gB2 = Me[2 * 3 + e_cB];
+      const float gB0 = -Me[0 * 3 + e_cB], gB1 = -Me[1 * 3 + e_cB], gB2 = -Me[2 * 3 + e_cB];
       const float inv_w = Me[25 + 3 * e_fld + e_t];
+      const float w_curl = e_sign * inv_w;
       const float sig_w = Me[31 + 3 * e_fld + e_t];
-      const float* yrow = sY + e_row_off;
-      float* drow = sStage + e_row_off;
-      constexpr int NCH = (NP + 7) / 8;
-      for (int ch = grp; ch < NCH; ch += kTcGroups) {
-        const int i0 = ch * 8;
-        float r0[8], r1[8], r2[8], lf[8];
-        tc::tmem_ld8(e_taddr + (uint32_t)i0, r0);
-        tc::tmem_ld8(e_taddr + (uint32_t)(NP + i0), r1);
-        tc::tmem_ld8(e_taddr + (uint32_t)(2 * NP + i0), r2);
-        tc::tmem_ld8(e_taddr + (uint32_t)(NV + i0), lf);
-        tc::tmem_ld_wait();
+      float* const yrow = sY0 + ys * kYStride + e_row_off;
+      float* const prow = sP0 + ps * kYStride + e_row_off;  // p in, p out (LSERK) / dy out (Apply)
+      const int64_t t0 = tile * C::TILE_F;
+      // do the step's sources reach this tile? (uniform per tile)
+      const bool src_here =
+          MODE == kModeLserk && (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
+      const int64_t g_row = t0 + e_row_off;  // SoA index of node 0 of this row
+      const uint32_t acc = tmem + (uint32_t)(ps * C::ACC) + ((uint32_t)(q4 * 32) << 16);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          // my contributions: A to curl component (t+1)%3, B to (t+2)%3
-          const float A = gA0 * r0[u] + gA1 * r1[u] + gA2 * r2[u];
-          const float B = -(gB0 * r0[u] + gB1 * r1[u] + gB2 * r2[u]);
-          const float pa = __shfl_sync(0xffffffffu, A, e_srcA);
-          const float pb = __shfl_sync(0xffffffffu, B, e_srcB);
-          const int i = i0 + u;
-          if (lane_real && i < NP) drow[i] = inv_w * (e_sign * (pa + pb) + lf[u]) - sig_w * yrow[i];
+      for (int cc = 0; cc < C::ECH_PER; ++cc) {
+        const int ch = eg + kTcEpiGroups * cc;
+        if (ch < C::ECH) {
+          const int i0 = ch * 4;
+          float r0[4], r1[4], r2[4], lf[4], lg[4];
+          tc::tmem_ldw<4>(acc + (uint32_t)i0, r0);
+          tc::tmem_ldw<4>(acc + (uint32_t)(NP + i0), r1);
+          tc::tmem_ldw<4>(acc + (uint32_t)(2 * NP + i0), r2);
+          tc::tmem_ldw<4>(acc + (uint32_t)(NV + i0), lf);
+          tc::tmem_ldw<4>(acc + (uint32_t)(NV + NL + i0), lg);
+          tc::tmem_ld_wait();
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            // my contributions: A to curl component (t+1)%3, B to (t+2)%3
+            const float A = fmaf(gA2, r2[u], fmaf(gA1, r1[u], gA0 * r0[u]));
+            const float B = fmaf(gB2, r2[u], fmaf(gB1, r1[u], gB0 * r0[u]));
+            const float pa = __shfl_sync(0xffffffffu, A, e_srcA);
+            const float pb = __shfl_sync(0xffffffffu, B, e_srcB);
+            const int i = i0 + u;
+            if (lane_real && i < NP) {
+              const float yv = yrow[i];
+              const float dy = fmaf(w_curl, pa + pb, fmaf(inv_w, lf[u] + lg[u], -sig_w * yv));
+              if (MODE == kModeLserk) {
+                // LSERK4 stage (explicit.rs:122-133): p = a p + dt (dy + src); y += b p
+                float k = dy;
+                if (src_here) {
+                  if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g_row + i), k);
+                  if (P.src_idx == g_row + i) k += P.src_g;
+                }
+                float pv = P.dt * k;
+                if (P.read_p) pv = fmaf(P.a, prow[i], pv);
+                prow[i] = pv;
+                yrow[i] = fmaf(P.b, pv, yv);
+              } else {
+                prow[i] = dy;
+              }
+            }
+          }
         }
       }
       tc::tc_fence_before();
-      if (p_pending && !tc::mbar_wait(&s_bar_p, p_phase, kTcWaitLimit)) s_abort = 1;
+      tc::fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&bar_epi[ps]);
+      DGTD_TC_MARK(5);
+      ys = ys == 2 ? 0 : ys + 1;
     }
-    __syncthreads();
-    DGTD_TC_MARK(5);
-    if (s_abort) break;
-
-    // ---- 4. epilogue in shared memory: the mode's update in place
-    if (!ctl && MODE == kModeLserk) {
-      float4* const d4 = reinterpret_cast<float4*>(sStage);
-      float4* const y4 = reinterpret_cast<float4*>(sY);
-      const float4* const p4 = reinterpret_cast<const float4*>(sP);
-      const int64_t gb = tile * C::TILE_F;
-      for (int idx = tid; idx < C::TILE_F / 4; idx += kTcThreads) {
-        const float4 dy = d4[idx];
-        const int64_t g = gb + 4 * (int64_t)idx;
-        float k0 = dy.x, k1 = dy.y, k2 = dy.z, k3 = dy.w;
-        if (P.src_vec != nullptr) {
-          const float4 sv = __ldg(reinterpret_cast<const float4*>(P.src_vec + g));
-          k0 = fmaf(P.src_g, sv.x, k0); k1 = fmaf(P.src_g, sv.y, k1);
-          k2 = fmaf(P.src_g, sv.z, k2); k3 = fmaf(P.src_g, sv.w, k3);
-        }
-        const int64_t ds = P.src_idx - g;
-        if (ds == 0) k0 += P.src_g;
-        if (ds == 1) k1 += P.src_g;
-        if (ds == 2) k2 += P.src_g;
-        if (ds == 3) k3 += P.src_g;
-        float4 pv = make_float4(P.dt * k0, P.dt * k1, P.dt * k2, P.dt * k3);
-        if (P.read_p) {
-          const float4 po = p4[idx];
-          pv.x = fmaf(P.a, po.x, pv.x); pv.y = fmaf(P.a, po.y, pv.y);
-          pv.z = fmaf(P.a, po.z, pv.z); pv.w = fmaf(P.a, po.w, pv.w);
-        }
-        d4[idx] = pv;  // p_out staged in place of dy
-        const float4 yo = y4[idx];
-        y4[idx] = make_float4(fmaf(P.b, pv.x, yo.x), fmaf(P.b, pv.y, yo.y), fmaf(P.b, pv.z, yo.z),
-                              fmaf(P.b, pv.w, yo.w));
-      }
-    }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    mma_phase ^= 1u;
-    mma_out = false;
-    if (p_pending) p_phase ^= 1u;
-    p_pending = false;
-    if (ctl0) {
-      const int64_t gb = tile * C::TILE_F;
+  } else if (ctl0) {
+    // ================= control lane: loads, MMAs, stores
+    uint32_t n_ld[3] = {0u, 0u, 0u}, n_p[2] = {0u, 0u}, n_mma[2] = {0u, 0u}, n_vd = 0u;
+    const uint32_t idv = tc::idesc_tf32(M, NV), idl = tc::idesc_tf32(M, C::NL2);
+    const uint32_t bvh = tc::smem_u32(tsm + C::O_BVH), bvl = tc::smem_u32(tsm + C::O_BVL);
+    const uint32_t bl = tc::smem_u32(tsm + C::O_BL);
+    const uint32_t ah = tc::smem_u32(alh), al = tc::smem_u32(all);
+    auto load_y = [&](int64_t j) {  // tile j of this CTA -> slot j % 3
+      const int s = (int)(j % 3);
+      const int64_t tile = blockIdx.x + j * gridDim.x;
+      tc::mbar_expect_tx(&bar_ld[s], C::TILE_B + C::META_B);
+      tc::bulk_g2s(sY0 + s * kYStride, P.y_in + tile * C::TILE_F, C::TILE_B, &bar_ld[s]);
+      tc::bulk_g2s(sM0 + s * kMStride, P.meta + tile * E * kMetaWords, C::META_B, &bar_ld[s]);
+      ++n_ld[s];
+    };
+    auto load_p = [&](int64_t j) {  // residual register of tile j -> slot j & 1
+      const int s = (int)(j & 1);
+      const int64_t tile = blockIdx.x + j * gridDim.x;
+      tc::mbar_expect_tx(&bar_p[s], C::TILE_B);
+      tc::bulk_g2s(sP0 + s * kYStride, P.p + tile * C::TILE_F, C::TILE_B, &bar_p[s]);
+      ++n_p[s];
+    };
+    auto store = [&](int64_t j) {
+      const int64_t gb = ((int64_t)blockIdx.x + j * gridDim.x) * C::TILE_F;
+      const float* sy = sY0 + (int)(j % 3) * kYStride;
+      const float* sp = sP0 + (int)(j & 1) * kYStride;
       if (MODE == kModeApply) {
-        tc::bulk_s2g(P.out + gb, sStage, C::TILE_B);
+        tc::bulk_s2g(P.out + gb, sp, C::TILE_B);
       } else {
-        tc::bulk_s2g(P.out + gb, sY, C::TILE_B);
-        if (P.write_p) tc::bulk_s2g(P.p + gb, sStage, C::TILE_B);
+        tc::bulk_s2g(P.out + gb, sy, C::TILE_B);
+        if (P.write_p) tc::bulk_s2g(P.p + gb, sp, C::TILE_B);
       }
       tc::bulk_commit();
+    };
+    if (n_my > 0) load_y(0);
+    if (n_my > 1) load_y(1);
+    if (n_my > 0 && use_p) load_p(0);
+    bool ok = true;
+    for (int64_t it = 0; it < n_my && ok; ++it) {
+      const int as = (int)(it & 1);
+      const uint32_t acc = tmem + (uint32_t)(as * C::ACC);
+      // volume MMAs: A = state hi/lo (TMEM), B = D hi/lo (shared)
+      ok = tc_wait1(&bar_avol, (uint32_t)(it & 1), abort_flag);
+      if (!ok) break;
+      tc::tc_fence_after();
+      DGTD_TC_MARK(6);
+#pragma unroll 1
+      for (int ks = 0; ks < KV / 8; ++ks) {
+        const uint32_t a_h = tmem + (uint32_t)(C::T_AHI + 8 * ks), a_l = tmem + (uint32_t)(C::T_ALO + 8 * ks);
+        tc::mma_tf32_ta(acc, a_h, tc::tf32_step_desc(bvh, NV, ks), idv, ks > 0 ? 1u : 0u);
+        tc::mma_tf32_ta(acc, a_h, tc::tf32_step_desc(bvl, NV, ks), idv, 1u);
+        tc::mma_tf32_ta(acc, a_l, tc::tf32_step_desc(bvh, NV, ks), idv, 1u);
+      }
+      tc::mma_commit(&bar_vdone);
+      ++n_vd;
+      // LIFT MMAs: A = flux hi/lo (shared), B = stacked LIFT hi/lo (shared):
+      // columns [NV, NV+NL) collect hi*hi + lo*hi, [NV+NL, NV+2NL) hi*lo + lo*lo
+      ok = tc_wait1(&bar_alift, (uint32_t)(it & 1), abort_flag);
+      if (!ok) break;
+      tc::tc_fence_after();
+      DGTD_TC_MARK(6);
+#pragma unroll 1
+      for (int ks = 0; ks < C::KL / 8; ++ks) {
+        const uint64_t bd = tc::tf32_step_desc(bl, C::NL2, ks);
+        tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(ah, M, ks), bd, idl, ks > 0 ? 1u : 0u);
+        tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(al, M, ks), bd, idl, 1u);
+      }
+      tc::mma_commit(&bar_mma[as]);
+      ++n_mma[as];
+      // results of the previous tile -> HBM
+      if (it > 0) {
+        ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
+        if (!ok) break;
+        DGTD_TC_MARK(6);
+        store(it - 1);
+      }
+      // the slots of tile it-1 are refilled once its stores have read them
+      tc::bulk_wait_read0();
+      DGTD_TC_MARK(7);
+      if (it + 2 < n_my) load_y(it + 2);
+      if (it + 1 < n_my && use_p) load_p(it + 1);
     }
-    DGTD_TC_MARK(6);
+    if (ok && n_my > 0) {
+      ok = tc_wait1(&bar_epi[(n_my - 1) & 1], (uint32_t)(((n_my - 1) >> 1) & 1), abort_flag);
+      if (ok) store(n_my - 1);
+    }
+    tc::bulk_wait0();
+    if (!ok) {
+      *abort_flag = 1;
+      // let every async operation still in flight finish before the CTA exits
+      for (int s = 0; s < 3; ++s)
+        if (n_ld[s]) (void)tc::mbar_wait(&bar_ld[s], (n_ld[s] - 1) & 1u, kTcWaitLimit);
+      for (int s = 0; s < 2; ++s) {
+        if (n_p[s]) (void)tc::mbar_wait(&bar_p[s], (n_p[s] - 1) & 1u, kTcWaitLimit);
+        if (n_mma[s]) (void)tc::mbar_wait(&bar_mma[s], (n_mma[s] - 1) & 1u, kTcWaitLimit);
+      }
+      if (n_vd) (void)tc::mbar_wait(&bar_vdone, (n_vd - 1) & 1u, kTcWaitLimit);
+    }
   }
 
-  // ---- drain: stores complete; on an abort wait (bounded) for loads in flight
-  if (ctl0) tc::bulk_wait0();
-  if (s_abort) {
-    if (tid == 0) atomicExch(err, 1);
-    if (ctl0) {
-      for (int b = 0; b < 2; ++b)
-        if ((pending >> b) & 1u) (void)tc::mbar_wait(&s_bar_ld[b], (ld_phase >> b) & 1u, kTcWaitLimit);
-      if (p_pending) (void)tc::mbar_wait(&s_bar_p, p_phase, kTcWaitLimit);
-      if (mma_out) (void)tc::mbar_wait(&s_bar_mma, mma_phase, kTcWaitLimit);
-    }
-  }
   tc::tc_fence_before();
   __syncthreads();
+  if (tid == 0 && s_abort) atomicExch(err, 1);
 #ifdef DGTD_TC_PHASE_TIMERS
-  if (tid == 0 && P.phase_clk != nullptr)
-    for (int i = 0; i < 7; ++i) atomicAdd(P.phase_clk + i, clk_acc[i]);
+  if (timer_thread && P.phase_clk != nullptr)
+    for (int i = 0; i < 8; ++i) atomicAdd(P.phase_clk + i, clk_acc[i]);
 #endif
   if (warp == 0) tc::tmem_dealloc(tmem, C::TMEM_COLS);
 }

@@ -1,7 +1,9 @@
 // tc_selftest.cuh -- a one-CTA tcgen05 GEMM through the same operand layout,
 // descriptors, TMEM allocation and TMEM loads as the tensor-core RHS kernel:
 // C[128 x N] = A[128 x K] * B[N x K]^T, with the 3xTF32 split products
-// (hi*hi + hi*lo + lo*hi) or a single tf32 product.  Test hook only.
+// (hi*hi + hi*lo + lo*hi) or a single tf32 product, and the A operand in shared
+// memory or in TMEM (written by tcgen05.st, one row per lane).  Test hook only.
+// flags: bit 0 = 3xTF32, bit 1 = A from TMEM.
 #pragma once
 #include <cstdint>
 
@@ -13,7 +15,7 @@ constexpr int kSelftestMaxK = 64;
 constexpr int kSelftestMaxN = 256;
 
 __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A, const float* __restrict__ B,
-                                                     float* __restrict__ C, int N, int K, int split3,
+                                                     float* __restrict__ C, int N, int K, int flags,
                                                      int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tc_sm[];
   const int M = 128;
@@ -41,8 +43,11 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
     put(b_hi, N, r, k, h);
     put(b_lo, N, r, k, tc::to_tf32(v - h));
   }
+  const bool split3 = (flags & 1) != 0, a_tmem = (flags & 2) != 0;
+  const int n32 = (N + 31) & ~31, k32 = (K + 31) & ~31;
+  const int a_hi_col = n32, a_lo_col = n32 + k32;
   uint32_t ncols = 32;
-  while ((int)ncols < N) ncols <<= 1;
+  while ((int)ncols < (a_tmem ? n32 + 2 * k32 : N)) ncols <<= 1;
   if (warp == 0) tc::tmem_alloc(&s_tmem, ncols);
   if (tid == 0) {
     tc::mbar_init(&s_bar, 1);
@@ -53,7 +58,38 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = s_tmem;
-  if (tid == 0) {
+  if (a_tmem) {
+    // row tid of A -> TMEM lane tid (warp w owns lanes 32w..32w+31)
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int k0 = 0; k0 < K; k0 += 8) {
+      float h[8], l[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float v = A[tid * K + k0 + q];
+        h[q] = tc::to_tf32(v);
+        l[q] = tc::to_tf32(v - h[q]);
+      }
+      tc::tmem_st8(lane_addr + (uint32_t)(a_hi_col + k0), h);
+      tc::tmem_st8(lane_addr + (uint32_t)(a_lo_col + k0), l);
+    }
+    tc::tmem_st_wait();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+  }
+  if (tid == 0 && a_tmem) {
+    const uint32_t id = tc::idesc_tf32(M, N);
+    const uint32_t bh = tc::smem_u32(b_hi), bl = tc::smem_u32(b_lo);
+    for (int ks = 0; ks < K / 8; ++ks) {
+      const uint32_t ah = tmem + (uint32_t)(a_hi_col + 8 * ks), al = tmem + (uint32_t)(a_lo_col + 8 * ks);
+      tc::mma_tf32_ta(tmem, ah, tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
+      if (split3) {
+        tc::mma_tf32_ta(tmem, ah, tc::tf32_step_desc(bl, N, ks), id, 1u);
+        tc::mma_tf32_ta(tmem, al, tc::tf32_step_desc(bh, N, ks), id, 1u);
+      }
+    }
+    tc::mma_commit(&s_bar);
+  } else if (tid == 0) {
     const uint32_t id = tc::idesc_tf32(M, N);
     const uint32_t ah = tc::smem_u32(a_hi), al = tc::smem_u32(a_lo);
     const uint32_t bh = tc::smem_u32(b_hi), bl = tc::smem_u32(b_lo);

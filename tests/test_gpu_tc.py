@@ -1,5 +1,6 @@
 """tcgen05 building blocks: a one-CTA GEMM through the tensor-core RHS kernel's
-operand layout, descriptors and TMEM path, against numpy in f64."""
+operand layout, descriptors and TMEM path (A from shared memory or from TMEM),
+against numpy in f64."""
 import numpy as np
 import pytest
 
@@ -11,17 +12,18 @@ from .conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("a_tmem", [0, 2], ids=["a_smem", "a_tmem"])
 @pytest.mark.parametrize("n,k", [(16, 8), (32, 16), (112, 40), (48, 64), (176, 56), (256, 64)])
-def test_tc_gemm_3xtf32(n, k):
+def test_tc_gemm_3xtf32(n, k, a_tmem):
     ctx = G.GpuContext(0)
     rng = np.random.default_rng(n * 100 + k)
     a = rng.normal(size=(128, k)).astype(np.float32)
     b = rng.normal(size=(n, k)).astype(np.float32)
     c = np.zeros((128, n), dtype=np.float32)
-    _native.check(_native.lib.dgtd_debug_tc_gemm(ctx.handle, a.ravel(), b.ravel(), c.ravel(), n, k, 1))
+    _native.check(_native.lib.dgtd_debug_tc_gemm(ctx.handle, a.ravel(), b.ravel(), c.ravel(), n, k, 1 | a_tmem))
     want = a.astype(np.float64) @ b.astype(np.float64).T
     assert rel_l2(c, want) < 2e-6
     c1 = np.zeros((128, n), dtype=np.float32)
-    _native.check(_native.lib.dgtd_debug_tc_gemm(ctx.handle, a.ravel(), b.ravel(), c1.ravel(), n, k, 0))
+    _native.check(_native.lib.dgtd_debug_tc_gemm(ctx.handle, a.ravel(), b.ravel(), c1.ravel(), n, k, a_tmem))
     e1 = rel_l2(c1, want)
     assert 1e-5 < e1 < 5e-3  # one tf32 product: ~2^-11 relative
