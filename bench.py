@@ -46,12 +46,17 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic(kernel, order):
+def _traffic(kernel, order, n_dof):
+    """DRAM bytes per launch of the stage kernel (dram__bytes_read.sum +
+    dram__bytes_write.sum from the ncu capture summarised in profiles/, scaled
+    from bytes per DOF to this workload's n_dof), or None when no capture exists."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    return d.get(f"{kernel}/N{order}")
+    d = json.load(open(p)).get(f"{kernel}/N{order}")
+    if not d:
+        return None
+    return float(d["bytes_per_dof_stage_avg"]) * n_dof
 
 
 class Clocks:
@@ -170,8 +175,7 @@ def run_b200(args):
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     gop = G.GpuOperator(ctx, op)
-    if args.engine:
-        gop.set_engine({"fp32": 0, "tf32x3": 1, "bf16x3": 2}[args.engine])
+    gop.set_engine({"fp32": 0, "tf32x3": 1}[args.engine])
     n = gop.n_dof()
     y0 = wl.y0(op).astype(np.float32)
 
@@ -228,7 +232,7 @@ def run_b200(args):
     alg_bytes = BYTES_PER_DOF_STAGE[order] * n
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
-    traffic = _traffic("rhs_fp32_lserk" if gop.engine == 0 else "rhs_tc_lserk", order)
+    traffic = _traffic("rhs_fp32_lserk" if gop.engine == 0 else "rhs_tc_lserk", order, n)
 
     # end to end through the public API with pinned host buffers
     e2e_steps = args.steps
@@ -296,7 +300,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=48)
-    ap.add_argument("--engine", default=None, choices=[None, "fp32", "tf32x3", "bf16x3"])
+    ap.add_argument("--engine", default="tf32x3", choices=["fp32", "tf32x3"],
+                    help="stage kernel: FP32 CUDA cores, or the tcgen05 tensor-core kernel (3xTF32 products)")
     ap.add_argument("--power-iters", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-cells", type=int, default=24)
