@@ -132,6 +132,54 @@ int dgtd_transient_probes(dgtd_op *op, const float *y0, float dt, int64_t steps,
                           const float *g_samples, const int64_t *probes, int64_t n_probes,
                           float *out, float *y_final);
 
+/* As dgtd_transient, recording per frame n_fun linear functionals of the state
+ * on the device, F_q(y) = sum_{k in [fun_ptr[q], fun_ptr[q+1])} fun_w[k] * y[fun_idx[k]]
+ * (fun_idx: AoS DOF indices), accumulated in f64, into out[(steps+1)*n_fun];
+ * the final state into y_final[n_dof] (may be NULL).  Port modal amplitudes
+ * (rhs.rs:1211-1242 as dgtd_host_port_modal_weights) per step without a host
+ * trajectory; the reference computes them on the host from a recorded
+ * trajectory (session.rs:1041-1054). */
+int dgtd_transient_functionals(dgtd_op *op, const float *y0, float dt, int64_t steps,
+                               int64_t substeps, int drive, int64_t src_dof, const double *src_vec,
+                               const float *g_samples, int64_t n_fun, const int64_t *fun_ptr,
+                               const int64_t *fun_idx, const double *fun_w, double *out,
+                               float *y_final);
+
+/* ---- KCL adaptive transient (gpu/operator.rs:823-893, session.rs:130-187)
+ * The KCL RK4(3)5[2R+]C embedded pair with the PI step-size controller, the
+ * controller running on the device: attempts are queued in batches and the
+ * host reads one status word per batch instead of the error norm of every
+ * substep.  g_frames[steps] holds the waveform per output frame (held across
+ * the frame's substeps); NULL for a free run. */
+typedef struct dgtd_kcl_controller {
+    double atol, rtol, safety, growth_limit, shrink_limit, pi_alpha, pi_beta, min_step_factor;
+} dgtd_kcl_controller;
+typedef struct dgtd_kcl_stats {
+    int64_t accepted, rejected;
+    float h_min, h_max; /* step sizes in operator time, as the reference logs them */
+} dgtd_kcl_stats;
+/* One KCL RK4(3)5[2R+]C step of h from the AoS state y (KclWorkspace::step_into,
+ * explicit_adaptive.rs:84-152; TdSession::step_adaptive, session.rs:499):
+ * y_out = the fourth-order solution, err = the embedded-error vector. */
+int dgtd_kcl_step(dgtd_op *op, const double *y, double h, double *y_out, double *err);
+/* Controller::default (session.rs:145-158, constants.rs:260-292). */
+void dgtd_kcl_controller_default(dgtd_kcl_controller *ctl);
+/* With record != 0, out[(steps+1)*n_dof] receives the trajectory (row 0 = y0);
+ * else out[n_dof] the final state.  DGTD_ERR_COLLAPSE when the step falls
+ * below min_step_factor*dt (the reference's "step size collapsed" error). */
+int dgtd_transient_kcl(dgtd_op *op, const float *y0, float dt, int64_t steps, int drive,
+                       int64_t src_dof, const double *src_vec, const float *g_frames,
+                       const dgtd_kcl_controller *ctl, int record, float *out, dgtd_kcl_stats *stats);
+/* As dgtd_transient_kcl, recording per frame the linear functionals of
+ * dgtd_transient_functionals into out[(steps+1)*n_fun] (f64) and the final
+ * state into y_final (may be NULL). */
+int dgtd_transient_kcl_functionals(dgtd_op *op, const float *y0, float dt, int64_t steps, int drive,
+                                   int64_t src_dof, const double *src_vec, const float *g_frames,
+                                   const dgtd_kcl_controller *ctl, int64_t n_fun,
+                                   const int64_t *fun_ptr, const int64_t *fun_idx,
+                                   const double *fun_w, double *out, float *y_final,
+                                   dgtd_kcl_stats *stats);
+
 /* GpuOperator::expmv (gpu/operator.rs:1175): exp(t*A)*v by Arnoldi, f64 basis
  * and CGS2 on the device, sub-stepped into chunks of <= 12 (KRYLOV_CHUNK).
  * With tol > 0 each chunk also stops on the a-posteriori estimate

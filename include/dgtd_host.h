@@ -68,6 +68,12 @@ int dgtd_host_port_n_faces(const dgtd_host_op *op, int32_t port, int64_t *n_face
  * FaceFrame::fit (waveguide.rs:39-81) of the port nodes with `inward_normal`. */
 int dgtd_host_rect_port_profiles(const dgtd_host_op *op, int32_t port, const double *inward_normal,
                                  int32_t mode_m, int32_t mode_n, double *out);
+/* The modal projections P_e (which = 0) or P_h (which = 1) of a port as linear
+ * functionals of the AoS state (rhs.rs:1211-1242, port_modal_projections):
+ * P = sum_k w[k] * y[idx[k]], with n_faces*nfp*3 terms written to idx / w.
+ * profiles as for dgtd_host_port_source. */
+int dgtd_host_port_modal_weights(const dgtd_host_op *op, int32_t port, const double *profiles,
+                                 int32_t which, int64_t *idx, double *w);
 /* port_source (rhs.rs:1157-1199) from per-node profiles: b[n_dof]. */
 int dgtd_host_port_source(const dgtd_host_op *op, int32_t port, const double *profiles,
                           double *b);

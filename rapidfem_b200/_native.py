@@ -15,6 +15,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("DGTD_LIB_PATH") or os.path.join(_PKG, "_lib", "librapidfem_b200.so")
 
 DGTD_OK = 0
+DGTD_ERR_COLLAPSE = 8
 ERR_NAMES = {
     1: "BAD_ARG", 2: "CUDA", 3: "NONFINITE", 4: "TIMEOUT", 5: "NO_DEVICE", 6: "UNSUPPORTED",
     7: "OOM", 8: "COLLAPSE",
@@ -84,6 +85,25 @@ _sig("dgtd_apply", C.c_int, _vp, _pf, _pf)
 _sig("dgtd_transient", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pf)
 _sig("dgtd_transient_probes", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _vp,
      _i64, _vp, _vp)
+class KclController(C.Structure):
+    """dgtd_kcl_controller (session.rs:130-143)."""
+    _fields_ = [(k, C.c_double) for k in ("atol", "rtol", "safety", "growth_limit", "shrink_limit",
+                                           "pi_alpha", "pi_beta", "min_step_factor")]
+
+
+class KclStats(C.Structure):
+    _fields_ = [("accepted", C.c_int64), ("rejected", C.c_int64), ("h_min", C.c_float), ("h_max", C.c_float)]
+
+
+lib.dgtd_kcl_controller_default.argtypes = [C.POINTER(KclController)]
+lib.dgtd_kcl_controller_default.restype = None
+_sig("dgtd_kcl_step", C.c_int, _vp, _pd, _f64, _pd, _pd)
+_sig("dgtd_transient_kcl", C.c_int, _vp, _pf, _f32, _i64, C.c_int, _i64, _vp, _vp, C.POINTER(KclController),
+     C.c_int, _vp, C.POINTER(KclStats))
+_sig("dgtd_transient_kcl_functionals", C.c_int, _vp, _pf, _f32, _i64, C.c_int, _i64, _vp, _vp,
+     C.POINTER(KclController), _i64, _vp, _vp, _vp, _vp, _vp, C.POINTER(KclStats))
+_sig("dgtd_transient_functionals", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _i64,
+     _vp, _vp, _vp, _vp, _vp)
 _sig("dgtd_expmv", C.c_int, _vp, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32))
 _sig("dgtd_etd_step", C.c_int, _vp, _pd, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32))
 _sig("dgtd_state_upload", C.c_int, _vp, _pf)
@@ -115,6 +135,7 @@ _sig("dgtd_host_nearest_node_dof", C.c_int, _vp, _pd, _i32, _i32, C.POINTER(_i64
 _sig("dgtd_host_port_n_faces", C.c_int, _vp, _i32, C.POINTER(_i64))
 _sig("dgtd_host_rect_port_profiles", C.c_int, _vp, _i32, _pd, _i32, _i32, _pd)
 _sig("dgtd_host_port_source", C.c_int, _vp, _i32, _pd, _pd)
+_sig("dgtd_host_port_modal_weights", C.c_int, _vp, _i32, _pd, _i32, _pl, _pd)
 
 
 def last_error() -> str:

@@ -24,6 +24,7 @@
 #include "rhs_fp32.cuh"
 #include "rhs_tc.cuh"
 #include "tc_selftest.cuh"
+#include "kcl.cuh"
 
 // ------------------------------------------------------------------ errors
 
@@ -176,6 +177,10 @@ struct dgtd_op {
   DevBuf<float> tc_bvol, tc_blift;
   DevBuf<int> err;
   unsigned long long* phase_clk = nullptr;  // instrumented builds: per-phase cycle counters
+  // KCL adaptive stepping: controller, backup, embedded error, stage point, RHS, waveform
+  DevBuf<dgtd::KclCtl> kcl_ctl;
+  DevBuf<float> kcl_bak, kcl_e, kcl_stage, kcl_k, kcl_g;
+  DevBuf<double> kcl_part;
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
@@ -185,6 +190,7 @@ struct dgtd_op {
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
     kst.free(); skip.free(); mass.free(); absdet.free();
     tc_bvol.free(); tc_blift.free(); err.free();
+    kcl_ctl.free(); kcl_bak.free(); kcl_e.free(); kcl_stage.free(); kcl_k.free(); kcl_g.free(); kcl_part.free();
   }
 };
 
@@ -217,6 +223,25 @@ __global__ void k_gather_f32(const float* __restrict__ src, const int64_t* __res
                              int64_t n, float* __restrict__ out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
     out[k] = src[idx[k]];
+}
+
+// One block per functional: sum_k w[k] * y[idx[k]] in f64 (fixed order per
+// thread and a fixed reduction tree, so the result is deterministic).
+__global__ void __launch_bounds__(256) k_functionals(const float* __restrict__ y, const int64_t* __restrict__ ptr,
+                                                     const int64_t* __restrict__ idx, const double* __restrict__ w,
+                                                     double* __restrict__ out) {
+  __shared__ double part[8];
+  const int q = blockIdx.x;
+  double s = 0.0;
+  for (int64_t k = ptr[q] + threadIdx.x; k < ptr[q + 1]; k += blockDim.x) s += w[k] * (double)y[idx[k]];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < 8; ++i) t += part[i];
+    out[q] = t;
+  }
 }
 
 int grid_for(int64_t n, int threads, int num_sms) {
@@ -774,6 +799,79 @@ extern "C" int dgtd_transient_probes(dgtd_op* op, const float* y0, float dt, int
   return DGTD_OK;
 }
 
+extern "C" int dgtd_transient_functionals(dgtd_op* op, const float* y0, float dt, int64_t steps,
+                                          int64_t substeps, int drive, int64_t src_dof,
+                                          const double* src_vec, const float* g, int64_t n_fun,
+                                          const int64_t* fun_ptr, const int64_t* fun_idx,
+                                          const double* fun_w, double* out, float* y_final) {
+  if (!op || !y0 || steps < 0 || n_fun < 0 || (n_fun > 0 && (!fun_ptr || !out)))
+    return set_error(DGTD_ERR_BAD_ARG, "transient_functionals: bad argument");
+  if (n_fun > 65535) return set_error(DGTD_ERR_BAD_ARG, "transient_functionals: at most 65535 functionals");
+  if (!(std::isfinite(dt) && dt > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "dt must be positive");
+  const int64_t n_terms = n_fun > 0 ? fun_ptr[n_fun] : 0;
+  if (n_fun > 0 && fun_ptr[0] != 0) return set_error(DGTD_ERR_BAD_ARG, "fun_ptr[0] must be 0");
+  for (int64_t q = 0; q < n_fun; ++q)
+    if (fun_ptr[q + 1] < fun_ptr[q]) return set_error(DGTD_ERR_BAD_ARG, "fun_ptr must be non-decreasing");
+  if (n_terms > 0 && (!fun_idx || !fun_w)) return set_error(DGTD_ERR_BAD_ARG, "functional terms missing");
+  substeps = std::max<int64_t>(substeps, 1);
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (drive == DGTD_DRIVE_VECTOR) {
+    if (!src_vec) return set_error(DGTD_ERR_BAD_ARG, "vector drive without src_vec");
+    DGTD_TRY(dgtd_set_source_vector(op, src_vec));
+  }
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g, steps * substeps, &src_idx));
+  std::vector<int64_t> sidx((size_t)n_terms);
+  for (int64_t k = 0; k < n_terms; ++k) {
+    if (fun_idx[k] < 0 || fun_idx[k] >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "functional DOF " + std::to_string(fun_idx[k]) + " out of range");
+    sidx[k] = aos_to_soa_index(fun_idx[k], op->np);
+  }
+  DevBuf<int64_t> d_ptr, d_idx;
+  DevBuf<double> d_w, d_out;
+  if (n_fun > 0) {
+    DGTD_TRY(d_ptr.alloc(n_fun + 1));
+    DGTD_TRY(d_idx.alloc(std::max<int64_t>(n_terms, 1)));
+    DGTD_TRY(d_w.alloc(std::max<int64_t>(n_terms, 1)));
+    DGTD_TRY(d_out.alloc((size_t)(steps + 1) * n_fun));
+    CUDA_TRY(cudaMemcpyAsync(d_ptr.p, fun_ptr, (n_fun + 1) * 8, cudaMemcpyHostToDevice, op->stream()));
+    if (n_terms > 0) {
+      CUDA_TRY(cudaMemcpyAsync(d_idx.p, sidx.data(), n_terms * 8, cudaMemcpyHostToDevice, op->stream()));
+      CUDA_TRY(cudaMemcpyAsync(d_w.p, fun_w, n_terms * 8, cudaMemcpyHostToDevice, op->stream()));
+    }
+  }
+  DGTD_TRY(dgtd_state_upload(op, y0));
+  auto record = [&](int64_t row) -> int {
+    if (n_fun == 0) return DGTD_OK;
+    k_functionals<<<(unsigned)n_fun, 256, 0, op->stream()>>>(op->y[op->cur].p, d_ptr.p, d_idx.p, d_w.p,
+                                                             d_out.p + row * n_fun);
+    op->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return DGTD_OK;
+  };
+  int st = record(0);
+  const float h = dt / (float)substeps;
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  for (int64_t k = 0; k < steps && st == DGTD_OK; ++k) {
+    for (int64_t j = 0; j < substeps && st == DGTD_OK; ++j) {
+      const float gk = drive == DGTD_DRIVE_FREE ? 0.f : g[k * substeps + j];
+      st = lserk_step(op, h, src_idx, gk, sv);
+    }
+    if (st == DGTD_OK) st = record(k + 1);
+  }
+  if (st == DGTD_OK && n_fun > 0) {
+    cudaError_t e = cudaMemcpyAsync(out, d_out.p, (size_t)(steps + 1) * n_fun * 8, cudaMemcpyDeviceToHost,
+                                    op->stream());
+    if (e) st = set_error(DGTD_ERR_CUDA, std::string("functional download: ") + cudaGetErrorString(e));
+  }
+  if (st == DGTD_OK && y_final) st = dgtd_state_download(op, y_final);
+  cudaError_t e = cudaStreamSynchronize(op->stream());
+  d_ptr.free(); d_idx.free(); d_w.free(); d_out.free();
+  if (st != DGTD_OK) return st;
+  CUDA_TRY(e);
+  return check_kernel_flag(op);
+}
+
 extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t steps, int64_t substeps,
                               int drive, int64_t src_dof, const double* src_vec, const float* g,
                               int record, float* out) {
@@ -800,6 +898,280 @@ extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t st
   }
   if (!record) DGTD_TRY(dgtd_state_download(op, out));
   return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ KCL adaptive
+
+extern "C" void dgtd_kcl_controller_default(dgtd_kcl_controller* c) {
+  if (!c) return;
+  c->atol = 1e-8;                 // KCL_ATOL
+  c->rtol = 1e-4;                 // KCL_RTOL
+  c->safety = 0.9;                // KCL_SAFETY
+  c->growth_limit = 5.0;          // KCL_GROWTH_LIMIT
+  c->shrink_limit = 0.2;          // KCL_SHRINK_LIMIT
+  c->pi_alpha = 0.7 / 4.0;        // KCL_PI_ALPHA
+  c->pi_beta = 0.4 / 4.0;         // KCL_PI_BETA
+  c->min_step_factor = 1e-10;     // KCL_MIN_STEP_FACTOR
+}
+
+namespace {
+
+constexpr long long kKclAttemptCap = 10000000;  // per output frame
+
+// One adaptive run on the resident state.  Frames are recorded into d_traj
+// (SoA rows, may be null) or as functionals into d_fun (may be null).
+int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, const float* g,
+            const dgtd_kcl_controller* cin, float* d_traj, int64_t n_fun, const int64_t* d_ptr,
+            const int64_t* d_idx, const double* d_w, double* d_fun, dgtd_kcl_stats* stats) {
+  using dgtd::KclCtl;
+  const int64_t n = op->n_dof;
+  cudaStream_t s = op->stream();
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g, steps, &src_idx));
+  const size_t len = state_len(op);
+  DGTD_TRY(op->kcl_ctl.alloc(1));
+  const bool fresh = op->kcl_stage.n < len;
+  DGTD_TRY(op->kcl_bak.alloc(len));
+  DGTD_TRY(op->kcl_e.alloc(len));
+  DGTD_TRY(op->kcl_stage.alloc(len));
+  DGTD_TRY(op->kcl_k.alloc(len));
+  if (fresh) {  // the padding tail of the RHS input must hold finite values
+    CUDA_TRY(cudaMemsetAsync(op->kcl_stage.p, 0, len * 4, s));
+    CUDA_TRY(cudaMemsetAsync(op->kcl_k.p, 0, len * 4, s));
+  }
+  const int nt = 256, ng = grid_for(n, nt, op->ctx->num_sms);
+  DGTD_TRY(op->kcl_part.alloc(ng));
+  const float* gv = nullptr;
+  if (drive != DGTD_DRIVE_FREE && steps > 0) {
+    DGTD_TRY(op->kcl_g.alloc(steps));
+    CUDA_TRY(cudaMemcpyAsync(op->kcl_g.p, g, steps * 4, cudaMemcpyHostToDevice, s));
+    gv = op->kcl_g.p;
+  }
+  KclCtl c;
+  std::memset(&c, 0, sizeof(c));
+  c.atol = cin->atol; c.rtol = cin->rtol; c.safety = cin->safety; c.growth = cin->growth_limit;
+  c.shrink = cin->shrink_limit; c.alpha = cin->pi_alpha; c.beta = cin->pi_beta;
+  c.min_step_factor = cin->min_step_factor;
+  c.dt = dt; c.h = dt; c.prev_err = 0.f; c.t_rel = 0.f;
+  c.h_min_log = INFINITY; c.h_max_log = 0.f;
+  c.steps = steps; c.attempt_cap = kKclAttemptCap;
+  c.status = steps > 0 ? dgtd::kKclRunning : dgtd::kKclDone;
+  c.record = -1;
+  KclCtl* dc = op->kcl_ctl.p;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  const int* d_skip = &dc->skip;
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  float* y = op->y[op->cur].p;
+  auto attempt = [&]() -> int {
+    dgtd::k_kcl_begin<<<ng, nt, 0, s>>>(dc, y, op->kcl_bak.p, n);
+    for (int st = 0; st < 5; ++st) {
+      RhsParams P = base_params(op);
+      P.y_in = st == 0 ? y : op->kcl_stage.p;
+      P.out = op->kcl_k.p;
+      P.skip = d_skip;
+      DGTD_TRY(launch_rhs<kModeApply>(op, P));
+      const float b = (float)dgtd::kKclB[st], ew = (float)(dgtd::kKclBhat[st] - dgtd::kKclB[st]);
+      const float amb = st < 4 ? (float)(dgtd::kKclA[st] - dgtd::kKclB[st]) : 0.f;
+      dgtd::k_kcl_stage<<<ng, nt, 0, s>>>(dc, st, b, ew, amb, y, op->kcl_e.p, op->kcl_k.p, op->kcl_stage.p,
+                                          src_idx, sv, gv, n);
+    }
+    dgtd::k_kcl_err<<<ng, 256, 0, s>>>(dc, op->kcl_bak.p, y, op->kcl_e.p, op->kcl_part.p, n);
+    dgtd::k_kcl_control<<<1, 256, 0, s>>>(dc, op->kcl_part.p, ng, n);
+    dgtd::k_kcl_restore<<<ng, nt, 0, s>>>(dc, y, op->kcl_bak.p, n);
+    if (d_traj) dgtd::k_kcl_record_state<<<ng, nt, 0, s>>>(dc, y, d_traj, n);
+    if (n_fun > 0)
+      dgtd::k_kcl_record_fun<<<(unsigned)n_fun, 256, 0, s>>>(dc, y, d_ptr, d_idx, d_w, d_fun, n_fun);
+    op->launches += 10;
+    CUDA_TRY(cudaGetLastError());
+    return DGTD_OK;
+  };
+  // Batches of attempts; one status read per batch.  The batch is sized from
+  // the attempts per frame seen so far; surplus attempts at the end of the
+  // run do nothing.
+  int64_t batch = 4, attempts = 0;
+  while (c.status == dgtd::kKclRunning) {
+    for (int64_t b = 0; b < batch; ++b) DGTD_TRY(attempt());
+    attempts += batch;
+    CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    DGTD_TRY(check_kernel_flag(op));
+    if (c.frame > 0) {
+      const double per_frame = (double)(c.n_acc + c.n_rej) / (double)c.frame;
+      batch = (int64_t)std::ceil(per_frame * (double)(steps - c.frame)) + 1;
+    } else {
+      batch *= 2;
+    }
+    batch = std::max<int64_t>(1, std::min<int64_t>(batch, 256));
+  }
+  (void)attempts;
+  if (stats) {
+    stats->accepted = c.n_acc;
+    stats->rejected = c.n_rej;
+    stats->h_min = c.n_acc ? c.h_min_log : 0.f;
+    stats->h_max = c.h_max_log;
+  }
+  if (c.status == dgtd::kKclCollapsed) {
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  "GPU KCL: step size collapsed below %g*dt after %lld accepted, %lld rejected substeps",
+                  cin->min_step_factor, (long long)c.n_acc, (long long)c.n_rej);
+    return set_error(DGTD_ERR_COLLAPSE, msg);
+  }
+  if (c.status == dgtd::kKclCapped)
+    return set_error(DGTD_ERR_TIMEOUT, "GPU KCL: more than 1e7 attempts in one output frame");
+  return DGTD_OK;
+}
+
+int kcl_args(dgtd_op* op, const float* y0, float dt, int64_t steps, int drive, const double* src_vec,
+             const dgtd_kcl_controller* ctl, const char* what) {
+  if (!op || !y0 || !ctl || steps < 0) return set_error(DGTD_ERR_BAD_ARG, std::string(what) + ": bad argument");
+  if (!(std::isfinite(dt) && dt > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "dt must be positive");
+  if (!(ctl->atol >= 0.0 && ctl->rtol >= 0.0 && ctl->atol + ctl->rtol > 0.0 && ctl->safety > 0.0 &&
+        ctl->shrink_limit > 0.0 && ctl->growth_limit >= ctl->shrink_limit && ctl->min_step_factor >= 0.0))
+    return set_error(DGTD_ERR_BAD_ARG, std::string(what) + ": invalid controller settings");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (drive == DGTD_DRIVE_VECTOR) {
+    if (!src_vec) return set_error(DGTD_ERR_BAD_ARG, "vector drive without src_vec");
+    DGTD_TRY(dgtd_set_source_vector(op, src_vec));
+  }
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_kcl_step(dgtd_op* op, const double* y, double h, double* y_out, double* err) {
+  if (!op || !y || !y_out || !err) return set_error(DGTD_ERR_BAD_ARG, "kcl_step: null argument");
+  if (!(std::isfinite(h) && h > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "kcl_step: step must be positive");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  cudaStream_t s = op->stream();
+  const int64_t n = op->n_dof;
+  DGTD_TRY(op->tmp64.alloc(n));
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, y, n * 8, cudaMemcpyHostToDevice, s));
+  DGTD_TRY((to_soa<double, float>(op, op->tmp64.p, op->y[op->cur].p)));
+  const size_t len = state_len(op);
+  const bool fresh = op->kcl_stage.n < len;
+  DGTD_TRY(op->kcl_ctl.alloc(1));
+  DGTD_TRY(op->kcl_bak.alloc(len));
+  DGTD_TRY(op->kcl_e.alloc(len));
+  DGTD_TRY(op->kcl_stage.alloc(len));
+  DGTD_TRY(op->kcl_k.alloc(len));
+  if (fresh) {
+    CUDA_TRY(cudaMemsetAsync(op->kcl_stage.p, 0, len * 4, s));
+    CUDA_TRY(cudaMemsetAsync(op->kcl_k.p, 0, len * 4, s));
+  }
+  dgtd::KclCtl c;
+  std::memset(&c, 0, sizeof(c));
+  c.h_try = (float)h;
+  c.record = -1;
+  dgtd::KclCtl* dc = op->kcl_ctl.p;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  const int nt = 256, ng = grid_for(n, nt, op->ctx->num_sms);
+  float* yd = op->y[op->cur].p;
+  for (int st = 0; st < 5; ++st) {
+    RhsParams P = base_params(op);
+    P.y_in = st == 0 ? yd : op->kcl_stage.p;
+    P.out = op->kcl_k.p;
+    DGTD_TRY(launch_rhs<kModeApply>(op, P));
+    const float b = (float)dgtd::kKclB[st], ew = (float)(dgtd::kKclBhat[st] - dgtd::kKclB[st]);
+    const float amb = st < 4 ? (float)(dgtd::kKclA[st] - dgtd::kKclB[st]) : 0.f;
+    dgtd::k_kcl_stage<<<ng, nt, 0, s>>>(dc, st, b, ew, amb, yd, op->kcl_e.p, op->kcl_k.p, op->kcl_stage.p, -1,
+                                        nullptr, nullptr, n);
+    op->launches++;
+    CUDA_TRY(cudaGetLastError());
+  }
+  DGTD_TRY((to_aos<float, double>(op, yd, op->tmp64.p)));
+  CUDA_TRY(cudaMemcpyAsync(y_out, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  DGTD_TRY((to_aos<float, double>(op, op->kcl_e.p, op->tmp64.p)));
+  CUDA_TRY(cudaMemcpyAsync(err, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return check_kernel_flag(op);
+}
+
+extern "C" int dgtd_transient_kcl(dgtd_op* op, const float* y0, float dt, int64_t steps, int drive,
+                                  int64_t src_dof, const double* src_vec, const float* g,
+                                  const dgtd_kcl_controller* ctl, int record, float* out,
+                                  dgtd_kcl_stats* stats) {
+  if (!out) return set_error(DGTD_ERR_BAD_ARG, "transient_kcl: null output");
+  DGTD_TRY(kcl_args(op, y0, dt, steps, drive, src_vec, ctl, "transient_kcl"));
+  DGTD_TRY(dgtd_state_upload(op, y0));
+  DevBuf<float> traj;
+  if (record) {
+    DGTD_TRY(traj.alloc((size_t)(steps + 1) * op->n_dof));
+    CUDA_TRY(cudaMemcpyAsync(traj.p, op->y[op->cur].p, op->n_dof * 4, cudaMemcpyDeviceToDevice, op->stream()));
+  }
+  int st = kcl_run(op, dt, steps, drive, src_dof, g, ctl, record ? traj.p : nullptr, 0, nullptr, nullptr,
+                   nullptr, nullptr, stats);
+  if (st == DGTD_OK) {
+    if (record) {
+      std::memcpy(out, y0, op->n_dof * 4);
+      DGTD_TRY(op->aos32.alloc(op->n_dof + 4));
+      for (int64_t r = 1; r <= steps && st == DGTD_OK; ++r) {
+        st = to_aos<float, float>(op, traj.p + r * op->n_dof, op->aos32.p);
+        if (st == DGTD_OK) {
+          cudaError_t e = cudaMemcpyAsync(out + r * op->n_dof, op->aos32.p, op->n_dof * 4,
+                                          cudaMemcpyDeviceToHost, op->stream());
+          if (!e) e = cudaStreamSynchronize(op->stream());
+          if (e) st = set_error(DGTD_ERR_CUDA, std::string("trajectory download: ") + cudaGetErrorString(e));
+        }
+      }
+    } else {
+      st = dgtd_state_download(op, out);
+    }
+  }
+  cudaStreamSynchronize(op->stream());
+  traj.free();
+  return st;
+}
+
+extern "C" int dgtd_transient_kcl_functionals(dgtd_op* op, const float* y0, float dt, int64_t steps, int drive,
+                                              int64_t src_dof, const double* src_vec, const float* g,
+                                              const dgtd_kcl_controller* ctl, int64_t n_fun,
+                                              const int64_t* fun_ptr, const int64_t* fun_idx,
+                                              const double* fun_w, double* out, float* y_final,
+                                              dgtd_kcl_stats* stats) {
+  if (n_fun < 0 || n_fun > 65535 || (n_fun > 0 && (!fun_ptr || !out)))
+    return set_error(DGTD_ERR_BAD_ARG, "transient_kcl_functionals: bad functionals");
+  DGTD_TRY(kcl_args(op, y0, dt, steps, drive, src_vec, ctl, "transient_kcl_functionals"));
+  const int64_t n_terms = n_fun > 0 ? fun_ptr[n_fun] : 0;
+  if (n_fun > 0 && fun_ptr[0] != 0) return set_error(DGTD_ERR_BAD_ARG, "fun_ptr[0] must be 0");
+  for (int64_t q = 0; q < n_fun; ++q)
+    if (fun_ptr[q + 1] < fun_ptr[q]) return set_error(DGTD_ERR_BAD_ARG, "fun_ptr must be non-decreasing");
+  if (n_terms > 0 && (!fun_idx || !fun_w)) return set_error(DGTD_ERR_BAD_ARG, "functional terms missing");
+  std::vector<int64_t> sidx((size_t)n_terms);
+  for (int64_t k = 0; k < n_terms; ++k) {
+    if (fun_idx[k] < 0 || fun_idx[k] >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "functional DOF " + std::to_string(fun_idx[k]) + " out of range");
+    sidx[k] = aos_to_soa_index(fun_idx[k], op->np);
+  }
+  DevBuf<int64_t> d_ptr, d_idx;
+  DevBuf<double> d_w, d_out;
+  cudaStream_t s = op->stream();
+  if (n_fun > 0) {
+    DGTD_TRY(d_ptr.alloc(n_fun + 1));
+    DGTD_TRY(d_idx.alloc(std::max<int64_t>(n_terms, 1)));
+    DGTD_TRY(d_w.alloc(std::max<int64_t>(n_terms, 1)));
+    DGTD_TRY(d_out.alloc((size_t)(steps + 1) * n_fun));
+    CUDA_TRY(cudaMemcpyAsync(d_ptr.p, fun_ptr, (n_fun + 1) * 8, cudaMemcpyHostToDevice, s));
+    if (n_terms > 0) {
+      CUDA_TRY(cudaMemcpyAsync(d_idx.p, sidx.data(), n_terms * 8, cudaMemcpyHostToDevice, s));
+      CUDA_TRY(cudaMemcpyAsync(d_w.p, fun_w, n_terms * 8, cudaMemcpyHostToDevice, s));
+    }
+  }
+  DGTD_TRY(dgtd_state_upload(op, y0));
+  if (n_fun > 0) {
+    k_functionals<<<(unsigned)n_fun, 256, 0, s>>>(op->y[op->cur].p, d_ptr.p, d_idx.p, d_w.p, d_out.p);
+    CUDA_TRY(cudaGetLastError());
+  }
+  int st = kcl_run(op, dt, steps, drive, src_dof, g, ctl, nullptr, n_fun, d_ptr.p, d_idx.p, d_w.p, d_out.p, stats);
+  if (st == DGTD_OK && n_fun > 0) {
+    cudaError_t e = cudaMemcpyAsync(out, d_out.p, (size_t)(steps + 1) * n_fun * 8, cudaMemcpyDeviceToHost, s);
+    if (e) st = set_error(DGTD_ERR_CUDA, std::string("functional download: ") + cudaGetErrorString(e));
+  }
+  if (st == DGTD_OK && y_final) st = dgtd_state_download(op, y_final);
+  cudaStreamSynchronize(s);
+  d_ptr.free(); d_idx.free(); d_w.free(); d_out.free();
+  return st;
 }
 
 // ------------------------------------------------------------------ Krylov

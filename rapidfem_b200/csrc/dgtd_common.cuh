@@ -57,7 +57,8 @@ struct RhsParams {
   const float* src_vec;    // Lserk DRIVE_VECTOR pattern (SoA f32) or null
   const double* src64;     // Arnoldi augmented column b (SoA f64) or null
   const double* aug_s;     // Arnoldi: device scalar s_j (augmented component), or null
-  const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop)
+  const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop,
+                           // adaptive attempts past the end of a run)
   int64_t n_elem;
   int64_t src_idx;         // Lserk DRIVE_POINT: SoA index, or -1
   float src_g;             // held waveform value of the step

@@ -657,6 +657,43 @@ extern "C" int dgtd_host_rect_port_profiles(const dgtd_host_op* h, int32_t port,
   return DGTD_OK;
 }
 
+// The modal projections of port_modal_projections (rhs.rs:1211-1242) as linear
+// functionals of the AoS state: P_e = sum_k w[k] y[idx[k]] over the E components
+// of the port face nodes (which = 0), P_h over the H components (which = 1).
+// n_faces * nfp * 3 terms, in port-face order.  A zero-norm profile gives zero
+// weights (the reference returns 0 then).
+extern "C" int dgtd_host_port_modal_weights(const dgtd_host_op* h, int32_t port, const double* profiles,
+                                            int32_t which, int64_t* idx, double* w) {
+  if (!h || !profiles || !idx || !w || (which != 0 && which != 1))
+    return set_error(DGTD_ERR_BAD_ARG, "port_modal_weights: bad arguments");
+  const auto& o = h->op;
+  const int np = o.re.np, nfp = o.re.nfp;
+  double norm = 0.0;
+  size_t fi = 0, k = 0;
+  for (int64_t e = 0; e < o.K; ++e)
+    for (int f = 0; f < 4; ++f) {
+      const int64_t ef = 4 * e + f;
+      if (o.port[ef] != port) continue;
+      const double area = o.fscale[ef] * std::fabs(o.det[e]) / 2.0;
+      for (int m = 0; m < nfp; ++m) {
+        const double* pr = profiles + 6 * (fi * nfp + m) + 3 * which;
+        const double wn = 2.0 * area * o.re.face_w[size_t(f) * nfp + m];
+        const int vi = o.re.face_nodes[size_t(f) * nfp + m];
+        const int64_t base = (e * np + vi) * 6 + 3 * which;
+        norm += wn * (pr[0] * pr[0] + pr[1] * pr[1] + pr[2] * pr[2]);
+        for (int c = 0; c < 3; ++c) {
+          idx[k] = base + c;
+          w[k] = wn * pr[c];
+          ++k;
+        }
+      }
+      ++fi;
+    }
+  const double inv = norm > 0.0 ? 1.0 / norm : 0.0;
+  for (size_t q = 0; q < k; ++q) w[q] *= inv;
+  return DGTD_OK;
+}
+
 extern "C" int dgtd_host_port_source(const dgtd_host_op* h, int32_t port, const double* profiles,
                                      double* b) {
   if (!h || !profiles || !b) return set_error(DGTD_ERR_BAD_ARG, "port_source: null argument");

@@ -67,7 +67,7 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
   uint8_t* sG = sFn + 4 * NFP;
   const int tid = threadIdx.x;
 
-  if (MODE == kModeArnoldi && P.skip != nullptr && *P.skip) return;
+  if (P.skip != nullptr && *P.skip) return;  // uniform: nothing to do for this launch
 
   for (int i = tid; i < 3 * NP * NP; i += blockDim.x) sD[i] = T.dT[i];
   for (int i = tid; i < NF * NP; i += blockDim.x) sL[i] = T.liftT[i];

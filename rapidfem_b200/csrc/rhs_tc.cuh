@@ -193,6 +193,10 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   const int64_t n_my =
       n_tiles > (int64_t)blockIdx.x ? (n_tiles - (int64_t)blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
+  // a launch flagged off (adaptive stepping past its last attempt) does
+  // nothing; the flag is read before any barrier or TMEM allocation
+  if (P.skip != nullptr && *P.skip) return;
+
   // ---- set-up: TMEM, barriers, constant operands, tables
   if (warp == 0) tc::tmem_alloc(&s_tmem, C::TMEM_COLS);
   if (tid == 0) {

@@ -171,6 +171,106 @@ class GpuOperator:
                                         series.ctypes.data, yf.ctypes.data))
         return series[: (steps + 1) * pr.size].reshape(steps + 1, pr.size), yf
 
+    def transient_functionals(self, y0, dt, steps, substeps=1, drive=None, g=None, functionals=()):
+        """As transient, recording per frame the linear functionals
+        `functionals = [(idx, w), ...]` (F(y) = sum w[k] y[idx[k]], AoS DOF
+        indices) on the device in f64; returns (series[steps+1, F], y_final)."""
+        y0 = _f32(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        substeps = max(int(substeps), 1)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g)
+            if gs.size != steps * substeps:
+                raise ValueError("wrong number of waveform samples")
+        idx = [np.ascontiguousarray(i, dtype=np.int64).ravel() for i, _ in functionals]
+        wts = [np.ascontiguousarray(w, dtype=np.float64).ravel() for _, w in functionals]
+        for i, w in zip(idx, wts):
+            if i.size != w.size:
+                raise ValueError("functional index and weight arrays differ in length")
+        nf = len(idx)
+        ptr = np.zeros(nf + 1, dtype=np.int64)
+        ptr[1:] = np.cumsum([i.size for i in idx]) if nf else []
+        all_i = np.concatenate(idx) if nf else np.zeros(0, dtype=np.int64)
+        all_w = np.concatenate(wts) if nf else np.zeros(0, dtype=np.float64)
+        series = np.empty((steps + 1) * max(nf, 1), dtype=np.float64)
+        yf = np.empty(self._n, dtype=np.float32)
+        check(lib.dgtd_transient_functionals(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
+                                             nat.ptr(gs), nf, nat.ptr(ptr) if nf else None,
+                                             nat.ptr(all_i) if all_i.size else None,
+                                             nat.ptr(all_w) if all_w.size else None,
+                                             series.ctypes.data, yf.ctypes.data))
+        return series[: (steps + 1) * nf].reshape(steps + 1, nf), yf
+
+    def kcl_step(self, y, h):
+        """One KCL RK4(3)5 step (explicit_adaptive.rs:84-152): (y_new, err)."""
+        y = _f64(y)
+        self._check_len("state", y)
+        out = np.empty_like(y)
+        err = np.empty_like(y)
+        check(lib.dgtd_kcl_step(self._h, y, float(h), out, err))
+        return out, err
+
+    @staticmethod
+    def kcl_controller(**overrides):
+        """Controller::default (session.rs:145-158) with keyword overrides."""
+        c = nat.KclController()
+        lib.dgtd_kcl_controller_default(C.byref(c))
+        for k, v in overrides.items():
+            if not hasattr(c, k):
+                raise ValueError(f"unknown controller setting {k!r}")
+            setattr(c, k, float(v))
+        return c
+
+    def _kcl_common(self, y0, steps, drive, g, controller):
+        y0 = _f32(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self._check_len("source", vec)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g)
+            if gs.size != steps:
+                raise ValueError("a KCL run takes one waveform sample per output frame")
+        ctl = controller if controller is not None else self.kcl_controller()
+        return y0, kind, dof, vec, gs, ctl
+
+    def transient_kcl(self, y0, dt, steps, drive=None, g=None, controller=None, record=True):
+        """KCL RK4(3)5 adaptive transient (gpu/operator.rs:823) with the PI
+        controller on the device.  Returns (trajectory[steps+1, n] or final
+        state, stats dict with accepted, rejected, h_min, h_max)."""
+        y0, kind, dof, vec, gs, ctl = self._kcl_common(y0, steps, drive, g, controller)
+        out = np.empty(((steps + 1) if record else 1) * self._n, dtype=np.float32)
+        st = nat.KclStats()
+        check(lib.dgtd_transient_kcl(self._h, y0, float(dt), int(steps), kind, dof, nat.ptr(vec), nat.ptr(gs),
+                                     C.byref(ctl), 1 if record else 0, out.ctypes.data, C.byref(st)))
+        stats = {"accepted": st.accepted, "rejected": st.rejected, "h_min": st.h_min, "h_max": st.h_max}
+        return (out.reshape(steps + 1, self._n) if record else out), stats
+
+    def transient_kcl_functionals(self, y0, dt, steps, drive=None, g=None, controller=None, functionals=()):
+        """As transient_kcl, recording per frame the linear functionals
+        [(idx, w), ...] on the device; returns (series[steps+1, F], y_final, stats)."""
+        y0, kind, dof, vec, gs, ctl = self._kcl_common(y0, steps, drive, g, controller)
+        idx = [np.ascontiguousarray(i, dtype=np.int64).ravel() for i, _ in functionals]
+        wts = [np.ascontiguousarray(w, dtype=np.float64).ravel() for _, w in functionals]
+        nf = len(idx)
+        ptr = np.zeros(nf + 1, dtype=np.int64)
+        ptr[1:] = np.cumsum([i.size for i in idx]) if nf else []
+        all_i = np.concatenate(idx) if nf else np.zeros(0, dtype=np.int64)
+        all_w = np.concatenate(wts) if nf else np.zeros(0, dtype=np.float64)
+        series = np.empty((steps + 1) * max(nf, 1), dtype=np.float64)
+        yf = np.empty(self._n, dtype=np.float32)
+        st = nat.KclStats()
+        check(lib.dgtd_transient_kcl_functionals(self._h, y0, float(dt), int(steps), kind, dof, nat.ptr(vec),
+                                                 nat.ptr(gs), C.byref(ctl), nf, nat.ptr(ptr) if nf else None,
+                                                 nat.ptr(all_i) if all_i.size else None,
+                                                 nat.ptr(all_w) if all_w.size else None,
+                                                 series.ctypes.data, yf.ctypes.data, C.byref(st)))
+        stats = {"accepted": st.accepted, "rejected": st.rejected, "h_min": st.h_min, "h_max": st.h_max}
+        return series[: (steps + 1) * nf].reshape(steps + 1, nf), yf, stats
+
     def expmv(self, v, t, m, tol=0.0):
         """exp(t*A)*v (gpu/operator.rs:1175); returns (out, dim_used)."""
         v = _f64(v)

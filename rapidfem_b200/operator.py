@@ -161,6 +161,18 @@ class MaxwellOperator:
                                                int(mode[0]), int(mode[1]), out.ravel()))
         return out
 
+    def port_modal_weights(self, port: int, profiles, which: str = "E"):
+        """P_e (which="E") or P_h ("H") of `port` as a linear functional of the
+        AoS state (rhs.rs:1211-1242): returns (idx, w) with P = w @ y[idx]."""
+        if which not in ("E", "H"):
+            raise ValueError("which must be 'E' or 'H'")
+        nt = self.port_n_faces(port) * self.nfp * 3
+        idx = np.empty(nt, dtype=np.int64)
+        w = np.empty(nt, dtype=np.float64)
+        check(lib.dgtd_host_port_modal_weights(self._h, port, np.ascontiguousarray(profiles, dtype=np.float64).ravel(),
+                                               0 if which == "E" else 1, idx, w))
+        return idx, w
+
     def port_source(self, port: int, profiles) -> np.ndarray:
         b = np.zeros(self.n_dof)
         check(lib.dgtd_host_port_source(self._h, port, np.ascontiguousarray(profiles, dtype=np.float64).ravel(), b))

@@ -142,6 +142,11 @@ class TdSession:
         """One LSERK4 step of h (td.rs:242-244)."""
         return self.gop.transient(self._check("y", y), self.c * float(h), 1, 1).astype(np.float64)
 
+    def step_adaptive(self, y, h):
+        """One KCL RK4(3)5 step of h (session.rs:499): (y_new, embedded error)."""
+        out, err = self.gop.kcl_step(self._check("y", y), self.c * float(h))
+        return out, err
+
     def cfl_dt(self, recompute=False) -> float:
         """The largest stable LSERK4 step in physical time (session.rs:514-569)."""
         if self._cfl_h is None or recompute:
@@ -168,16 +173,46 @@ class TdSession:
         prof = self.op.rect_port_profiles(k, spec["inward_normal"], spec["mode"])
         return self.op.port_source(k, prof)
 
+    def port_functional(self, name, which="E"):
+        """P_e (or P_h) of a modal port as (idx, w) over the AoS state
+        (rhs.rs:1211-1242)."""
+        if name not in self._ports:
+            raise ValueError(f"no port named {name!r}")
+        k, spec = self._ports[name]
+        if spec.get("mode") is None:
+            raise ValueError(f"port {name!r} is an absorbing boundary, not a modal port")
+        prof = self.op.rect_port_profiles(k, spec["inward_normal"], spec["mode"])
+        return self.op.port_modal_weights(k, prof, which)
+
+    def port_signals(self, states, ports):
+        """The modal amplitude P_e of each port over a row-major trajectory,
+        [ports, rows] (session.rs:1041-1054)."""
+        n = self.n_dofs()
+        states = np.asarray(states, dtype=np.float64)
+        if states.size == 0 or states.size % n:
+            raise ValueError(f"the trajectory length {states.size} is not a multiple of n_dof = {n}")
+        rows = states.reshape(-1, n)
+        out = np.empty((len(ports), rows.shape[0]))
+        for q, name in enumerate(ports):
+            idx, w = self.port_functional(name)
+            out[q] = rows[:, idx] @ w
+        return out
+
     # ---- runs
     def transient(self, y0=None, *, dt, steps, source_dof=None, port=None, waveform=None, probes=None,
-                  method=None, device="gpu", krylov_dim=40, warmup=0, verbose=True):
+                  port_probes=None, method=None, device="gpu", krylov_dim=40, warmup=0, verbose=True):
         """A run of `steps` frames of `dt` (td.rs:281-324, session.rs:620-777).
-        Returns (frames [steps+1, n_dof or len(probes)], None)."""
+        Returns (frames [steps+1, n_dof, or len(probes) + len(port_probes)], None).
+        `port_probes` names modal ports whose amplitude P_e is recorded per frame
+        (on the device in the explicit path) after the point probes."""
         if device not in ("gpu", "cuda"):
             raise ValueError("rapidfem_b200 runs the DGTD path on the GPU only (device='gpu')")
         method = method or "explicit"
-        if method not in ("exponential", "explicit"):
-            raise ValueError("method must be 'exponential' or 'explicit'")
+        if method not in ("exponential", "explicit", "adaptive"):
+            raise ValueError("method must be 'exponential', 'explicit', or 'adaptive'")
+        if method == "adaptive" and warmup > 0:
+            raise ValueError("warmup is not supported with method='adaptive' (the controller "
+                             "stabilises itself in the first few frames)")
         if not (math.isfinite(dt) and dt > 0.0):
             raise ValueError(f"dt must be positive, got {dt}")
         if source_dof is not None and port is not None:
@@ -197,12 +232,39 @@ class TdSession:
             bad = [p for p in probes if not 0 <= p < n]
             if bad:
                 raise ValueError(f"probe DOF {bad[0]} out of range (n_dof = {n})")
+        funcs = [self.port_functional(p) for p in (port_probes or [])]
+        if funcs and probes is None:
+            probes = []
         warmup = min(int(warmup), steps)
         y = np.zeros(n) if y0 is None else self._check("y0", y0)
-        rows = [y[probes] if probes is not None else y.copy()]
+
+        def sample(v):
+            v = np.asarray(v, dtype=np.float64)
+            if probes is None:
+                return v.copy()
+            return np.concatenate([v[probes], [v[i] @ w for i, w in funcs]])
+
+        rows = [sample(y)]
 
         def push(v):
-            rows.append(v[probes] if probes is not None else np.asarray(v, dtype=np.float64).copy())
+            rows.append(sample(v))
+
+        if method == "adaptive":
+            # KCL RK4(3)5 with the PI controller on the device (session.rs:940-970)
+            _log(verbose, "transient: KCL adaptive on the GPU (atol=1e-08, rtol=1e-04)")
+            g = None
+            if drive is not None:
+                g = _sample(waveform, np.arange(steps) * dt)
+            if probes is not None:
+                fun = [(np.array([p], dtype=np.int64), np.ones(1)) for p in probes] + funcs
+                series, _, st = self.gop.transient_kcl_functionals(y, self.c * dt, steps, drive=drive, g=g,
+                                                                   functionals=fun)
+                rows.extend(list(series[1:]))
+            else:
+                traj, st = self.gop.transient_kcl(y, self.c * dt, steps, drive=drive, g=g, record=True)
+                rows.extend(list(traj[1:].astype(np.float64)))
+            stats = (st["accepted"], st["rejected"], st["h_min"] / self.c, st["h_max"] / self.c)
+            return np.array(rows), stats
 
         exp_frames = steps if method == "exponential" else warmup
         for k in range(exp_frames):
@@ -226,7 +288,13 @@ class TdSession:
             if drive is not None:
                 t = (warmup * nsub + np.arange(kk * nsub)) * h_sub
                 g = _sample(waveform, t)
-            if probes is not None:
+            if funcs:
+                fun = [(np.array([p], dtype=np.int64), np.ones(1)) for p in probes] + funcs
+                series, yf = self.gop.transient_functionals(y, self.c * dt, kk, nsub, drive=drive, g=g,
+                                                            functionals=fun)
+                rows.extend(list(series[1:]))
+                y = yf.astype(np.float64)
+            elif probes is not None:
                 series, yf = self.gop.transient_probes(y, self.c * dt, kk, nsub, drive=drive, g=g, probes=probes)
                 rows.extend(list(series[1:].astype(np.float64)))
                 y = yf.astype(np.float64)
@@ -276,6 +344,9 @@ class ProblemTD:
     def step_explicit(self, y, h):
         return self._op.step_explicit(y, float(h))
 
+    def step_adaptive(self, y, h):
+        return self._op.step_adaptive(y, float(h))
+
     def cfl_dt(self, *, recompute=False):
         return self._op.cfl_dt(recompute)
 
@@ -292,9 +363,18 @@ class ProblemTD:
         return np.arange(steps + 1) * dt, frames.T
 
     def transient(self, y0=None, *, dt, steps, source=None, waveform=None, port=None, krylov_dim=40,
-                  method="exponential", warmup=0, device="gpu", verbose=True):
+                  method="exponential", warmup=0, device="gpu", verbose=True, port_probes=None):
         src = None if source is None else self.probe_dof(source[0], field=source[1], component=source[2])
         frames, _ = self._op.transient(y0, dt=float(dt), steps=int(steps), source_dof=src, port=port,
                                        waveform=waveform, method=method, device=device,
-                                       krylov_dim=int(krylov_dim), warmup=int(warmup), verbose=verbose)
+                                       krylov_dim=int(krylov_dim), warmup=int(warmup), verbose=verbose,
+                                       port_probes=port_probes)
         return frames
+
+    def port_signals(self, traj, ports, *, dt=None):
+        """Modal amplitude P_e(t) of each port over a trajectory (problem/td.py:612):
+        returns (t, rows [ports, n_snapshot])."""
+        traj = np.ascontiguousarray(traj, dtype=np.float64)
+        rows = self._op.port_signals(traj, list(ports))
+        n_rows = rows.shape[1]
+        return np.arange(n_rows) * (1.0 if dt is None else float(dt)), rows

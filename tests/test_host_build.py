@@ -106,3 +106,26 @@ def test_port_source_matches_oracle():
     b = prod.port_source(0, prof)
     assert np.array_equal(b, orc.port_source(0, prof))
     assert np.linalg.norm(b) > 0
+
+
+def test_port_modal_weights_match_oracle_projections():
+    """P_e, P_h as sparse functionals equal port_modal_projections (rhs.rs:1211-1242)."""
+    nodes, tets = R.box_mesh_jittered(3, 2, 4, 1.0, 0.6, 1.2, 0.1, 11)
+    m = O.Mesh(nodes, tets)
+    port = np.where(O.boundary_faces_on_plane(m, 2, 0.0), 0, -1)
+    port[O.boundary_faces_on_plane(m, 2, 1.2)] = 1
+    prod = O.MaxwellOperator(m, 3, face_port=port)
+    orc = R.Operator(nodes, tets, 3, face_port=port)
+    rng = np.random.default_rng(5)
+    y = rng.normal(size=prod.n_dof)
+    for p in (0, 1):
+        prof = prod.rect_port_profiles(p, [0, 0, 1.0 if p == 0 else -1.0], (1, 0))
+        ie, we = prod.port_modal_weights(p, prof, "E")
+        ih, wh = prod.port_modal_weights(p, prof, "H")
+        assert ie.size == prod.port_n_faces(p) * prod.nfp * 3
+        assert np.all(ie % 6 < 3) and np.all(ih % 6 >= 3)
+        pe, ph = orc.port_projections(p, prof, y)
+        assert abs(y[ie] @ we - pe) <= 1e-12 * max(1.0, abs(pe))
+        assert abs(y[ih] @ wh - ph) <= 1e-12 * max(1.0, abs(ph))
+    with pytest.raises(ValueError):
+        prod.port_modal_weights(0, prof, "X")
