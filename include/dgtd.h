@@ -145,6 +145,18 @@ int dgtd_transient_functionals(dgtd_op *op, const float *y0, float dt, int64_t s
                                const int64_t *fun_idx, const double *fun_w, double *out,
                                float *y_final);
 
+/* ---- stage-level stepping for drivers that act between stages
+ * (a partitioned run's halo exchange).  One fused LSERK4 stage (0..4) of h on
+ * the resident state (explicit.rs:122-133); stage 0 restarts the residual
+ * register (a_0 = 0), stage 4 does not write it.  No reference counterpart:
+ * the reference steps whole LSERK4 steps only (gpu/operator.rs:906). */
+int dgtd_lserk_stage(dgtd_op *op, float h, int32_t stage, int drive, int64_t src_dof, float g);
+/* Copy element blocks (6*Np f32 each, element-major SoA) of the resident
+ * state to / from a device buffer: buf[j*6*Np + r] <-> element d_elems[j].
+ * d_elems and d_buf are device pointers. */
+int dgtd_state_gather_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, float *d_buf);
+int dgtd_state_scatter_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, const float *d_buf);
+
 /* ---- KCL adaptive transient (gpu/operator.rs:823-893, session.rs:130-187)
  * The KCL RK4(3)5[2R+]C embedded pair with the PI step-size controller, the
  * controller running on the device: attempts are queued in batches and the

@@ -97,6 +97,9 @@ class KclStats(C.Structure):
 
 lib.dgtd_kcl_controller_default.argtypes = [C.POINTER(KclController)]
 lib.dgtd_kcl_controller_default.restype = None
+_sig("dgtd_lserk_stage", C.c_int, _vp, _f32, _i32, C.c_int, _i64, _f32)
+_sig("dgtd_state_gather_elements", C.c_int, _vp, _vp, _i64, _vp)
+_sig("dgtd_state_scatter_elements", C.c_int, _vp, _vp, _i64, _vp)
 _sig("dgtd_kcl_step", C.c_int, _vp, _pd, _f64, _pd, _pd)
 _sig("dgtd_transient_kcl", C.c_int, _vp, _pf, _f32, _i64, C.c_int, _i64, _vp, _vp, C.POINTER(KclController),
      C.c_int, _vp, C.POINTER(KclStats))

@@ -711,6 +711,73 @@ extern "C" int dgtd_run_lserk(dgtd_op* op, float h, int64_t steps, int drive, in
   return DGTD_OK;
 }
 
+// Element blocks (6*Np f32, contiguous in the element-major SoA state).
+__global__ void k_gather_blocks(const float* __restrict__ y, const int64_t* __restrict__ elems, int64_t n,
+                                int bs, float* __restrict__ buf) {
+  const int64_t total = n * bs;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = t / bs;
+    buf[t] = y[elems[j] * bs + (t - j * bs)];
+  }
+}
+__global__ void k_scatter_blocks(float* __restrict__ y, const int64_t* __restrict__ elems, int64_t n, int bs,
+                                 const float* __restrict__ buf) {
+  const int64_t total = n * bs;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = t / bs;
+    y[elems[j] * bs + (t - j * bs)] = buf[t];
+  }
+}
+
+extern "C" int dgtd_state_gather_elements(dgtd_op* op, const int64_t* d_elems, int64_t n, float* d_buf) {
+  if (!op || n < 0 || (n > 0 && (!d_elems || !d_buf)))
+    return set_error(DGTD_ERR_BAD_ARG, "state_gather_elements: bad argument");
+  if (n == 0) return DGTD_OK;
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  const int bs = 6 * op->np;
+  k_gather_blocks<<<grid_for(n * bs, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(op->y[op->cur].p, d_elems, n,
+                                                                                      bs, d_buf);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_state_scatter_elements(dgtd_op* op, const int64_t* d_elems, int64_t n, const float* d_buf) {
+  if (!op || n < 0 || (n > 0 && (!d_elems || !d_buf)))
+    return set_error(DGTD_ERR_BAD_ARG, "state_scatter_elements: bad argument");
+  if (n == 0) return DGTD_OK;
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  const int bs = 6 * op->np;
+  k_scatter_blocks<<<grid_for(n * bs, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(op->y[op->cur].p, d_elems, n,
+                                                                                       bs, d_buf);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_lserk_stage(dgtd_op* op, float h, int32_t stage, int drive, int64_t src_dof, float g) {
+  if (!op || stage < 0 || stage > 4) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: stage must be 0..4");
+  if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: step must be positive");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, &g, 1, &src_idx));
+  RhsParams P = base_params(op);
+  P.y_in = op->y[op->cur].p;
+  P.out = op->y[op->cur ^ 1].p;
+  P.p = op->p.p;
+  P.a = (float)kLserkA[stage];
+  P.b = (float)kLserkB[stage];
+  P.dt = h;
+  P.read_p = stage > 0;
+  P.write_p = stage < 4;
+  P.src_idx = src_idx;
+  P.src_vec = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  P.src_g = drive == DGTD_DRIVE_FREE ? 0.f : g;
+  DGTD_TRY(launch_rhs<kModeLserk>(op, P));
+  op->cur ^= 1;
+  return DGTD_OK;
+}
+
 extern "C" int dgtd_apply_device(dgtd_op* op, const float* d_y, float* d_dy) {
   if (!op || !d_y || !d_dy) return set_error(DGTD_ERR_BAD_ARG, "apply_device: null argument");
   CUDA_TRY(cudaSetDevice(op->ctx->device));

@@ -130,7 +130,7 @@ class GpuOperator:
         if kind == "point":
             return nat.DRIVE_POINT, int(arg), None
         if kind == "vector":
-            return nat.DRIVE_VECTOR, 0, _f64(arg)
+            return nat.DRIVE_VECTOR, 0, None if arg is None else _f64(arg)
         raise ValueError(f"unknown drive {kind!r}")
 
     def transient(self, y0, dt, steps, substeps=1, drive=None, g=None, record=False) -> np.ndarray:
@@ -202,6 +202,22 @@ class GpuOperator:
                                              nat.ptr(all_w) if all_w.size else None,
                                              series.ctypes.data, yf.ctypes.data))
         return series[: (steps + 1) * nf].reshape(steps + 1, nf), yf
+
+    def lserk_stage(self, h, stage, drive=None, g=0.0):
+        """One fused LSERK4 stage on the resident state (drivers that act between
+        stages, e.g. a partitioned run's halo exchange)."""
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            raise ValueError("set a vector drive with set_source_vector first and pass ('vector', None)")
+        check(lib.dgtd_lserk_stage(self._h, float(h), int(stage), kind, dof, float(g)))
+
+    def gather_elements(self, d_elems: int, n: int, d_buf: int) -> None:
+        """Element blocks (6*Np f32) of the resident state into a device buffer."""
+        check(lib.dgtd_state_gather_elements(self._h, d_elems, int(n), d_buf))
+
+    def scatter_elements(self, d_elems: int, n: int, d_buf: int) -> None:
+        """A device buffer of element blocks into the resident state."""
+        check(lib.dgtd_state_scatter_elements(self._h, d_elems, int(n), d_buf))
 
     def kcl_step(self, y, h):
         """One KCL RK4(3)5 step (explicit_adaptive.rs:84-152): (y_new, err)."""

@@ -1,0 +1,133 @@
+"""Element partition with one halo exchange per stage (the multi-GPU path):
+partition invariants, an in-process run of all parts, and a world_size-2 gloo
+run on CPU, each against the single-domain oracle.  The oracle stands in for
+the device engine of each rank here; tests/test_gpu_partition.py runs the
+device engine."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from oracle import oracle as R
+from rapidfem_b200 import operator as O
+from rapidfem_b200 import partition as PT
+
+
+class OracleEngine:
+    """The per-part compute of a partitioned run on the f64 oracle."""
+
+    def __init__(self, part: PT.Part, order: int):
+        self.orc = R.Operator(part.mesh.nodes, part.mesh.tets, order, 1.0, face_port=part.face_port,
+                              materials=part.materials)
+        self.bs = 6 * self.orc.np
+        self.a, self.b = R.lserk_coeffs()
+        self.y = None
+        self.p = None
+
+    def new_buffer(self, n_elem):
+        return torch.empty(n_elem * self.bs, dtype=torch.float64)
+
+    def gather(self, ids, buf):
+        buf.copy_(torch.from_numpy(self.y.reshape(-1, self.bs)[ids].ravel()))
+
+    def scatter(self, ids, buf):
+        self.y.reshape(-1, self.bs)[ids] = buf.numpy().reshape(-1, self.bs)
+
+    def stage(self, h, s):
+        k = self.orc.apply(self.y)
+        self.p = h * k if s == 0 else self.a[s] * self.p + h * k
+        self.y = self.y + self.b[s] * self.p
+
+    def sync(self):
+        pass
+
+    def load(self, y):
+        self.y = np.array(y, dtype=np.float64)
+
+    def state(self):
+        return self.y
+
+
+def _problem():
+    mesh = O.structured_box_jittered(4, 3, 3, 1.0, 0.8, 0.9, 0.1, 7)
+    port = np.where(O.boundary_faces_on_plane(mesh, 2, 0.0), 0, -1)
+    eps = np.where(mesh.nodes[mesh.tets].mean(axis=1)[:, 0] > 0.5, 4.0, 1.0)
+    mat = O.isotropic_materials(eps)
+    return mesh, port, mat
+
+
+def test_parts_are_consistent():
+    mesh, port, mat = _problem()
+    part = PT.morton_partition(mesh, 3)
+    counts = np.bincount(part, minlength=3)
+    assert counts.size == 3 and counts.max() - counts.min() <= 1  # equal shares
+    parts = PT.build_parts(mesh, part, face_port=port, materials=mat)
+    nbr = PT.face_neighbours(mesh.tets)
+    assert np.array_equal(np.sort(np.concatenate([p.owned for p in parts])), np.arange(mesh.n_tets))
+    for p in parts:
+        need = nbr[p.owned].ravel()
+        need = np.unique(need[need >= 0])
+        assert np.array_equal(np.setdiff1d(need, p.owned), p.halo)
+        for q, ids in p.send.items():
+            r_ids = parts[q].recv[p.rank]
+            assert np.array_equal(p.owned[ids], parts[q].elements[r_ids])
+        assert set(p.recv) == {q for q in range(3) if p.rank in parts[q].send}
+
+
+def _global_run(mesh, port, mat, order, y0, h, steps):
+    orc = R.Operator(mesh.nodes, mesh.tets, order, 1.0, face_port=port, materials=mat)
+    return orc.lserk(y0, h, steps), orc
+
+
+def test_loopback_partition_matches_single_domain():
+    mesh, port, mat = _problem()
+    order = 2
+    orc = R.Operator(mesh.nodes, mesh.tets, order, 1.0, face_port=port, materials=mat)
+    y0 = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    h = 0.5 / orc.power_rho(30)[0]
+    want = orc.lserk(y0, h, 4)
+    parts = PT.build_parts(mesh, PT.morton_partition(mesh, 3), face_port=port, materials=mat)
+    engines = [OracleEngine(p, order) for p in parts]
+    for e, yl in zip(engines, PT.split_state(parts, y0, orc.np)):
+        e.load(yl)
+    PT.LoopbackLserk(parts, engines).step(h, 4)
+    got = PT.join_state(parts, [e.state() for e in engines], orc.np)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+def _rank_main(rank, world, port_no, tmp):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port_no}", rank=rank, world_size=world)
+    try:
+        mesh, port, mat = _problem()
+        order = 2
+        parts = PT.build_parts(mesh, PT.morton_partition(mesh, world), face_port=port, materials=mat)
+        me = parts[rank]
+        eng = OracleEngine(me, order)
+        n = 6 * eng.orc.np * mesh.n_tets
+        y0 = np.sin(0.3 + 0.017 * np.arange(n))
+        eng.load(PT.split_state(parts, y0, eng.orc.np)[rank])
+        h = float(np.load(os.path.join(tmp, "h.npy")))
+        PT.ShardedLserk(me, eng, PT.TorchTransport()).step(h, 3)
+        np.save(os.path.join(tmp, f"y{rank}.npy"), eng.state())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_matches_single_domain():
+    mesh, port, mat = _problem()
+    order = 2
+    orc = R.Operator(mesh.nodes, mesh.tets, order, 1.0, face_port=port, materials=mat)
+    y0 = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    h = 0.5 / orc.power_rho(30)[0]
+    want = orc.lserk(y0, h, 3)
+    with tempfile.TemporaryDirectory() as tmp:
+        np.save(os.path.join(tmp, "h.npy"), np.array(h))
+        port_no = 29500 + (os.getpid() % 2000)
+        mp.spawn(_rank_main, args=(2, port_no, tmp), nprocs=2, join=True)
+        parts = PT.build_parts(mesh, PT.morton_partition(mesh, 2), face_port=port, materials=mat)
+        got = PT.join_state(parts, [np.load(os.path.join(tmp, f"y{r}.npy")) for r in range(2)], orc.np)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
