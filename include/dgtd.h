@@ -88,6 +88,9 @@ typedef struct {
     const int32_t *face_perm;      /* 4K*Nfp neighbour face-node match, rhs.rs:546-566 */
     const double *mass;            /* Np*Np reference mass matrix (dg_basis.rs:95), or NULL;
                                       needed only by the energy entry points */
+    const double *dt_scale;        /* K per-element multiplier of the LSERK4 step, or NULL (= 1):
+                                      a batch of independent instances in one operator, each
+                                      stepping with its own dt (no reference counterpart) */
 } dgtd_op_desc;
 
 /* Contraction engine of the RHS kernels. */

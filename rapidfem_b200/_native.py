@@ -58,7 +58,7 @@ class OpDesc(C.Structure):
         ("diff_r", _vp), ("diff_s", _vp), ("diff_t", _vp), ("lift", _vp), ("face_nodes", _vp),
         ("jinv", _vp), ("inv_eps", _vp), ("inv_mu", _vp), ("sigma_eps", _vp), ("sigma_mu", _vp),
         ("face_normal", _vp), ("face_fscale", _vp), ("face_neighbor", _vp),
-        ("face_nbr_local", _vp), ("face_port", _vp), ("face_perm", _vp), ("mass", _vp),
+        ("face_nbr_local", _vp), ("face_port", _vp), ("face_perm", _vp), ("mass", _vp), ("dt_scale", _vp),
     ]
 
 

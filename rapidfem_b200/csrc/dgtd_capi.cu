@@ -460,6 +460,12 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
     const uint32_t w0 = codes[0] | (codes[1] << 16), w1 = codes[2] | (codes[3] << 16);
     std::memcpy(&M[41], &w0, 4);
     std::memcpy(&M[42], &w1, 4);
+    M[43] = 1.0f;
+    if (d->dt_scale) {
+      const double sc = d->dt_scale[e];
+      if (!(std::isfinite(sc) && sc > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "op_create: dt_scale must be positive");
+      M[43] = (float)sc;
+    }
   }
   std::vector<float> dT((size_t)3 * np * np), liftT((size_t)4 * nfp * np);
   const double* D[3] = {d->diff_r, d->diff_s, d->diff_t};

@@ -12,7 +12,8 @@
 //                       [41..43) 4 face codes, 16 bits each (faces 0,1 in word 41):
 //                                bits 0..7 gather-table id, bits 8..9 kind
 //                                (0 interior, 1 PEC wall, 2 port)
-//                       [43]     padding
+//                       [43]     LSERK step multiplier of the element (1, or an
+//                                instance's own step in a batched operator)
 //   gather tables (per operator, uint8): gtab[id][m] = volume node of the
 //                       neighbour that matches this face's node m
 //                       (face_nodes[nbr_lf][perm[m]], rhs.rs:1404-1406).

@@ -495,6 +495,7 @@ extern "C" int dgtd_host_op_destroy(dgtd_host_op* op) {
 extern "C" int dgtd_host_op_desc(const dgtd_host_op* h, dgtd_op_desc* d) {
   if (!h || !d) return set_error(DGTD_ERR_BAD_ARG, "host_op_desc: null argument");
   const auto& o = h->op;
+  *d = dgtd_op_desc{};  // optional arrays (dt_scale) start unset
   d->order = o.re.order;
   d->n_elem = int32_t(o.K);
   d->flux_alpha = o.alpha;

@@ -247,7 +247,7 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
           float k = dy[c];
           if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g), k);
           if (g == P.src_idx) k += P.src_g;
-          float pv = P.dt * k;
+          float pv = (P.dt * M[43]) * k;
           if (P.read_p) pv = fmaf(P.a, P.p[g], pv);
           if (P.write_p) P.p[g] = pv;
           P.out[g] = fmaf(P.b, pv, Y[c * NP + i_me]);

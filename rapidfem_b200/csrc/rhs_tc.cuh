@@ -426,6 +426,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const float inv_w = Me[25 + 3 * e_fld + e_t];
       const float w_curl = e_sign * inv_w;
       const float sig_w = Me[31 + 3 * e_fld + e_t];
+      const float dt_e = P.dt * Me[43];  // the element's own step (batched instances)
       float* const yrow = sY0 + ys * kYStride + e_row_off;
       float* const prow = sP0 + ps * kYStride + e_row_off;  // p in, p out (LSERK) / dy out (Apply)
       const int64_t t0 = tile * C::TILE_F;
@@ -464,7 +465,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
                   if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g_row + i), k);
                   if (P.src_idx == g_row + i) k += P.src_g;
                 }
-                float pv = P.dt * k;
+                float pv = dt_e * k;
                 if (P.read_p) pv = fmaf(P.a, prow[i], pv);
                 prow[i] = pv;
                 yrow[i] = fmaf(P.b, pv, yv);

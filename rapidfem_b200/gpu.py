@@ -33,7 +33,7 @@ class GpuContext:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:  # lib is None at interpreter shutdown
             lib.dgtd_ctx_destroy(h)
             self._h = C.c_void_p()
 
@@ -67,10 +67,17 @@ def _f64(a):
 class GpuOperator:
     """GpuOperator::new (gpu/operator.rs:207): the operator resident on the device."""
 
-    def __init__(self, ctx: GpuContext, op: MaxwellOperator):
+    def __init__(self, ctx: GpuContext, op: MaxwellOperator, dt_scale=None):
+        """`dt_scale[K]` (optional): a per-element multiplier of the LSERK4 step,
+        for a batch of independent instances that step with their own dt."""
         self.ctx = ctx
         self.host_op = op
         d = op.desc()
+        if dt_scale is not None:
+            ds = np.ascontiguousarray(dt_scale, dtype=np.float64).ravel()
+            if ds.size != op.n_elem:
+                raise ValueError("dt_scale needs one entry per element")
+            d.dt_scale = ds.ctypes.data
         h = C.c_void_p()
         check(lib.dgtd_op_create(ctx.handle, C.byref(d), C.byref(h)))
         self._h = h
@@ -81,7 +88,7 @@ class GpuOperator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:  # lib is None at interpreter shutdown
             lib.dgtd_op_destroy(h)
             self._h = C.c_void_p()
 
