@@ -208,6 +208,14 @@ int dgtd_expmv(dgtd_op *op, const double *v, double t, int32_t m, double tol, do
  * augmented Arnoldi, the augmented scalar kept on the device. */
 int dgtd_etd_step(dgtd_op *op, const double *y, const double *b, double h, int32_t m,
                   double tol, double *out, int32_t *dim_used);
+/* As dgtd_etd_step with tol > 0, also returning the a-posteriori Krylov error
+ * estimate h_{d+1,d}*|exp(tH)_{d-1,0}| (propagator.rs:278-294, relative to |y|)
+ * summed over the KRYLOV_CHUNK sub-steps, each of the k sub-steps stopping at
+ * tol/k; the estimate is formed at the final dimension too, so `est` > tol
+ * reports a step whose space was too small.  The accept/reject test of an
+ * adaptive or learned step controller. */
+int dgtd_etd_step_est(dgtd_op *op, const double *y, const double *b, double h, int32_t m, double tol,
+                      double *out, int32_t *dim_used, double *est);
 
 /* ---- device-resident state (no host copies) ---------------------------
  * The op owns a resident f32 state (the reference's `y` buffer). */
@@ -258,6 +266,30 @@ int dgtd_state_energy(dgtd_op *op, double *energy);
 /* Kernel launches issued by this op since creation / the last reset. */
 int dgtd_op_launch_count(const dgtd_op *op, int64_t *count);
 int dgtd_op_reset_launch_count(dgtd_op *op);
+
+/* ---- the MLP of the learned ETD step controller (no reference counterpart)
+ * n_in -> n_hidden -> n_hidden -> n_out, tanh hidden layers, linear output,
+ * mean-squared-error loss, Adam; forward, backward and Adam run as device
+ * kernels.  Parameters (f32) in the order W1[H][n_in], b1[H], W2[H][H], b2[H],
+ * W3[n_out][H], b3[n_out]; weights start Glorot-uniform from `seed`. */
+typedef struct dgtd_mlp dgtd_mlp;
+int dgtd_mlp_create(dgtd_ctx *ctx, int32_t n_in, int32_t n_hidden, int32_t n_out, uint64_t seed,
+                    dgtd_mlp **out);
+void dgtd_mlp_destroy(dgtd_mlp *mlp);
+int dgtd_mlp_n_params(const dgtd_mlp *mlp, int64_t *n_params);
+int dgtd_mlp_get_params(dgtd_mlp *mlp, float *params);
+/* Also resets the Adam moments. */
+int dgtd_mlp_set_params(dgtd_mlp *mlp, const float *params);
+/* y[batch*n_out] = f(x[batch*n_in]); batch 1..65535, host arrays. */
+int dgtd_mlp_forward(dgtd_mlp *mlp, const float *x, int64_t batch, float *y);
+/* The gradient of L = mean_b sum_o (f(x_b)_o - t_bo)^2 w.r.t. the parameters
+ * (grad[n_params]) and L, without updating. */
+int dgtd_mlp_gradient(dgtd_mlp *mlp, const float *x, const float *t, int64_t batch, float *grad,
+                      float *loss);
+/* `epochs` full-batch Adam steps (beta1 0.9, beta2 0.999, eps 1e-8) at rate lr;
+ * losses[epochs] (may be NULL) receives L before each step. */
+int dgtd_mlp_train(dgtd_mlp *mlp, const float *x, const float *t, int64_t batch, int32_t epochs, float lr,
+                   float *losses);
 
 /* ---- test hooks --------------------------------------------------------
  * Dense exp(A) of a d x d row-major matrix (d <= 64) by the device kernel the

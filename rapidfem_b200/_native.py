@@ -97,6 +97,16 @@ class KclStats(C.Structure):
 
 lib.dgtd_kcl_controller_default.argtypes = [C.POINTER(KclController)]
 lib.dgtd_kcl_controller_default.restype = None
+_sig("dgtd_mlp_create", C.c_int, _vp, _i32, _i32, _i32, C.c_uint64, C.POINTER(_vp))
+lib.dgtd_mlp_destroy.argtypes = [_vp]
+lib.dgtd_mlp_destroy.restype = None
+_sig("dgtd_mlp_n_params", C.c_int, _vp, C.POINTER(_i64))
+_sig("dgtd_mlp_get_params", C.c_int, _vp, _pf)
+_sig("dgtd_mlp_set_params", C.c_int, _vp, _pf)
+_sig("dgtd_mlp_forward", C.c_int, _vp, _pf, _i64, _pf)
+_sig("dgtd_mlp_gradient", C.c_int, _vp, _pf, _pf, _i64, _pf, C.POINTER(_f32))
+_sig("dgtd_mlp_train", C.c_int, _vp, _pf, _pf, _i64, _i32, _f32, _pf)
+_sig("dgtd_etd_step_est", C.c_int, _vp, _pd, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32), C.POINTER(_f64))
 _sig("dgtd_lserk_stage", C.c_int, _vp, _f32, _i32, C.c_int, _i64, _f32)
 _sig("dgtd_state_gather_elements", C.c_int, _vp, _vp, _i64, _vp)
 _sig("dgtd_state_scatter_elements", C.c_int, _vp, _vp, _i64, _vp)

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -25,6 +26,7 @@
 #include "rhs_tc.cuh"
 #include "tc_selftest.cuh"
 #include "kcl.cuh"
+#include "mlp.cuh"
 
 // ------------------------------------------------------------------ errors
 
@@ -973,6 +975,180 @@ extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t st
   return DGTD_OK;
 }
 
+// ------------------------------------------------------------------ MLP (learned ETD controller)
+
+struct dgtd_mlp {
+  dgtd_ctx* ctx = nullptr;
+  dgtd::MlpShape S{};
+  int step = 0;
+  DevBuf<float> p, m, v, grad, loss;
+  DevBuf<float> x, y, tg, a1, a2, G, lb;
+  ~dgtd_mlp() {
+    cudaSetDevice(ctx->device);
+    p.free(); m.free(); v.free(); grad.free(); loss.free();
+    x.free(); y.free(); tg.free(); a1.free(); a2.free(); G.free(); lb.free();
+  }
+};
+
+namespace {
+
+// splitmix64 (Steele, Lea & Flood 2014): the seeded initial weights.
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+int mlp_stage(dgtd_mlp* n, const float* x, const float* t, int64_t batch, bool keep) {
+  cudaStream_t s = n->ctx->stream;
+  DGTD_TRY(n->x.alloc((size_t)batch * n->S.n_in));
+  DGTD_TRY(n->y.alloc((size_t)batch * n->S.n_out));
+  CUDA_TRY(cudaMemcpyAsync(n->x.p, x, (size_t)batch * n->S.n_in * 4, cudaMemcpyHostToDevice, s));
+  if (t) {
+    DGTD_TRY(n->tg.alloc((size_t)batch * n->S.n_out));
+    CUDA_TRY(cudaMemcpyAsync(n->tg.p, t, (size_t)batch * n->S.n_out * 4, cudaMemcpyHostToDevice, s));
+  }
+  if (keep) {
+    DGTD_TRY(n->a1.alloc((size_t)batch * n->S.n_hidden));
+    DGTD_TRY(n->a2.alloc((size_t)batch * n->S.n_hidden));
+    DGTD_TRY(n->G.alloc((size_t)batch * n->S.n_params()));
+    DGTD_TRY(n->lb.alloc((size_t)batch));
+  }
+  return DGTD_OK;
+}
+
+int mlp_grad_launch(dgtd_mlp* n, int64_t batch) {
+  cudaStream_t s = n->ctx->stream;
+  const int th = std::max(32, (n->S.n_hidden + 31) / 32 * 32);
+  const int np = n->S.n_params();
+  dgtd::k_mlp_forward<<<(unsigned)batch, th, 0, s>>>(n->S, n->p.p, n->x.p, batch, n->y.p, n->a1.p, n->a2.p);
+  dgtd::k_mlp_backward<<<(unsigned)batch, th, 0, s>>>(n->S, n->p.p, n->x.p, n->tg.p, n->y.p, n->a1.p, n->a2.p,
+                                                      batch, n->G.p, n->lb.p);
+  dgtd::k_mlp_reduce<<<(np + 255) / 256, 256, 0, s>>>(n->G.p, batch, np, n->grad.p, n->lb.p, n->loss.p);
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+int mlp_check(dgtd_mlp* n, int64_t batch, const char* what) {
+  if (!n || batch < 1 || batch > 65535) return set_error(DGTD_ERR_BAD_ARG, std::string(what) + ": batch must be 1..65535");
+  CUDA_TRY(cudaSetDevice(n->ctx->device));
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_mlp_create(dgtd_ctx* ctx, int32_t n_in, int32_t n_hidden, int32_t n_out, uint64_t seed,
+                               dgtd_mlp** out) {
+  if (!ctx || !out || n_in < 1 || n_in > dgtd::kMlpMaxIn || n_hidden < 1 || n_hidden > dgtd::kMlpMaxHidden ||
+      n_out < 1 || n_out > dgtd::kMlpMaxOut || n_out > n_hidden)
+    return set_error(DGTD_ERR_BAD_ARG, "mlp_create: sizes must be 1..64 in, 1..128 hidden, 1..8 (<= hidden) out");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  auto n = std::make_unique<dgtd_mlp>();
+  n->ctx = ctx;
+  n->S = dgtd::MlpShape{n_in, n_hidden, n_out};
+  const int np = n->S.n_params();
+  // Glorot-uniform weights, zero biases
+  std::vector<float> h(np, 0.f);
+  uint64_t st = seed;
+  auto fill = [&](int off, int rows, int cols) {
+    const double a = std::sqrt(6.0 / (double)(rows + cols));
+    for (int q = 0; q < rows * cols; ++q) {
+      const double u = (double)(splitmix64(st) >> 11) * (1.0 / 9007199254740992.0);
+      h[off + q] = (float)((2.0 * u - 1.0) * a);
+    }
+  };
+  fill(n->S.o_w1(), n_hidden, n_in);
+  fill(n->S.o_w2(), n_hidden, n_hidden);
+  fill(n->S.o_w3(), n_out, n_hidden);
+  DGTD_TRY(n->p.alloc(np));
+  DGTD_TRY(n->m.alloc(np));
+  DGTD_TRY(n->v.alloc(np));
+  DGTD_TRY(n->grad.alloc(np));
+  DGTD_TRY(n->loss.alloc(1));
+  CUDA_TRY(cudaMemcpyAsync(n->p.p, h.data(), np * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(n->m.p, 0, np * 4, ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(n->v.p, 0, np * 4, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  *out = n.release();
+  return DGTD_OK;
+}
+
+extern "C" void dgtd_mlp_destroy(dgtd_mlp* n) { delete n; }
+
+extern "C" int dgtd_mlp_n_params(const dgtd_mlp* n, int64_t* np) {
+  if (!n || !np) return set_error(DGTD_ERR_BAD_ARG, "mlp_n_params: null argument");
+  *np = n->S.n_params();
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_mlp_get_params(dgtd_mlp* n, float* out) {
+  if (!n || !out) return set_error(DGTD_ERR_BAD_ARG, "mlp_get_params: null argument");
+  CUDA_TRY(cudaSetDevice(n->ctx->device));
+  CUDA_TRY(cudaMemcpyAsync(out, n->p.p, n->S.n_params() * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(n->ctx->stream));
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_mlp_set_params(dgtd_mlp* n, const float* in) {
+  if (!n || !in) return set_error(DGTD_ERR_BAD_ARG, "mlp_set_params: null argument");
+  CUDA_TRY(cudaSetDevice(n->ctx->device));
+  CUDA_TRY(cudaMemcpyAsync(n->p.p, in, n->S.n_params() * 4, cudaMemcpyHostToDevice, n->ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(n->m.p, 0, n->S.n_params() * 4, n->ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(n->v.p, 0, n->S.n_params() * 4, n->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(n->ctx->stream));
+  n->step = 0;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_mlp_forward(dgtd_mlp* n, const float* x, int64_t batch, float* y) {
+  DGTD_TRY(mlp_check(n, batch, "mlp_forward"));
+  if (!x || !y) return set_error(DGTD_ERR_BAD_ARG, "mlp_forward: null argument");
+  DGTD_TRY(mlp_stage(n, x, nullptr, batch, false));
+  const int th = std::max(32, (n->S.n_hidden + 31) / 32 * 32);
+  dgtd::k_mlp_forward<<<(unsigned)batch, th, 0, n->ctx->stream>>>(n->S, n->p.p, n->x.p, batch, n->y.p, nullptr,
+                                                                  nullptr);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(y, n->y.p, (size_t)batch * n->S.n_out * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(n->ctx->stream));
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_mlp_gradient(dgtd_mlp* n, const float* x, const float* t, int64_t batch, float* grad,
+                                 float* loss) {
+  DGTD_TRY(mlp_check(n, batch, "mlp_gradient"));
+  if (!x || !t || !grad) return set_error(DGTD_ERR_BAD_ARG, "mlp_gradient: null argument");
+  DGTD_TRY(mlp_stage(n, x, t, batch, true));
+  DGTD_TRY(mlp_grad_launch(n, batch));
+  CUDA_TRY(cudaMemcpyAsync(grad, n->grad.p, n->S.n_params() * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+  if (loss) CUDA_TRY(cudaMemcpyAsync(loss, n->loss.p, 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(n->ctx->stream));
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_mlp_train(dgtd_mlp* n, const float* x, const float* t, int64_t batch, int32_t epochs, float lr,
+                              float* losses) {
+  DGTD_TRY(mlp_check(n, batch, "mlp_train"));
+  if (!x || !t || epochs < 0 || !(lr > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "mlp_train: bad argument");
+  DGTD_TRY(mlp_stage(n, x, t, batch, true));
+  DevBuf<float> hist;
+  DGTD_TRY(hist.alloc(std::max(epochs, 1)));
+  cudaStream_t s = n->ctx->stream;
+  const int np = n->S.n_params();
+  for (int e = 0; e < epochs; ++e) {
+    DGTD_TRY(mlp_grad_launch(n, batch));
+    ++n->step;
+    dgtd::k_mlp_adam<<<(np + 255) / 256, 256, 0, s>>>(n->p.p, n->m.p, n->v.p, n->grad.p, np, lr, 0.9f, 0.999f,
+                                                      1e-8f, n->step);
+    CUDA_TRY(cudaMemcpyAsync(hist.p + e, n->loss.p, 4, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (losses && epochs > 0) CUDA_TRY(cudaMemcpyAsync(losses, hist.p, epochs * 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  hist.free();
+  return DGTD_OK;
+}
+
 // ------------------------------------------------------------------ KCL adaptive
 
 extern "C" void dgtd_kcl_controller_default(dgtd_kcl_controller* c) {
@@ -1276,7 +1452,7 @@ int ensure_krylov(dgtd_op* op, int m) {
 // One Arnoldi chunk: out = first n components of exp(t*Aug)[v; 1] (aug) or
 // exp(t*A) v, from the SoA f64 vector `v` (device).  dim_out gets the dimension.
 int krylov_chunk(dgtd_op* op, const double* v, double t, int m, double tol, bool aug, double* out,
-                 int* dim_out) {
+                 int* dim_out, double* est_out) {
   using namespace dgtd;
   cudaStream_t s = op->stream();
   const int64_t n = op->n_dof;
@@ -1315,16 +1491,21 @@ int krylov_chunk(dgtd_op* op, const double* v, double t, int m, double tol, bool
   op->launches += 2;
   CUDA_TRY(cudaGetLastError());
   int dim = 0;
+  double est = -1.0;
   CUDA_TRY(cudaMemcpyAsync(&dim, &st->dim, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   *dim_out = dim;
+  if (est_out) *est_out = est;
   return DGTD_OK;
 }
 
 // exp(t*A)v or the ETD step, sub-stepped into ceil(m/12) chunks
 // (gpu/operator.rs:1175-1197, :1267-1291).
+// With split_tol each of the k sub-steps runs to tol/k, so that the summed
+// estimate of a step whose sub-steps all converged stays within tol.
 int krylov_run(dgtd_op* op, const double* v_host, const double* b_host, double t, int m, double tol,
-               double* out_host, int* dim_used) {
+               double* out_host, int* dim_used, double* est_sum = nullptr, bool split_tol = false) {
   if (m < 1) return set_error(DGTD_ERR_BAD_ARG, "Krylov dimension must be >= 1");
   if (!std::isfinite(t)) return set_error(DGTD_ERR_BAD_ARG, "Krylov time must be finite");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
@@ -1344,16 +1525,20 @@ int krylov_run(dgtd_op* op, const double* v_host, const double* b_host, double t
   }
   const double tau = t / (double)k;
   int total = 0;
+  double esum = 0.0;
   for (int q = 0; q < k; ++q) {
     int d = 0;
-    DGTD_TRY(krylov_chunk(op, op->vin64.p, tau, chunk, tol, aug, op->w.p, &d));
+    double e = -1.0;
+    DGTD_TRY(krylov_chunk(op, op->vin64.p, tau, chunk, split_tol ? tol / (double)k : tol, aug, op->w.p, &d, &e));
     total += d;
+    esum = (e < 0.0 || esum < 0.0) ? -1.0 : esum + e;
     CUDA_TRY(cudaMemcpyAsync(op->vin64.p, op->w.p, n * 8, cudaMemcpyDeviceToDevice, s));
   }
   DGTD_TRY((to_aos<double, double>(op, op->vin64.p, op->tmp64.p)));
   CUDA_TRY(cudaMemcpyAsync(out_host, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   if (dim_used) *dim_used = total;
+  if (est_sum) *est_sum = esum;
   return DGTD_OK;
 }
 
@@ -1373,6 +1558,16 @@ extern "C" int dgtd_etd_step(dgtd_op* op, const double* y, const double* b, doub
   if (!op || !y || !b || !out) return set_error(DGTD_ERR_BAD_ARG, "etd_step: null argument");
   int d = 0;
   DGTD_TRY(krylov_run(op, y, b, h, m, tol, out, &d));
+  if (dim_used) *dim_used = d;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_etd_step_est(dgtd_op* op, const double* y, const double* b, double h, int32_t m,
+                                 double tol, double* out, int32_t* dim_used, double* est) {
+  if (!op || !y || !b || !out || !est) return set_error(DGTD_ERR_BAD_ARG, "etd_step_est: null argument");
+  if (!(tol > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "etd_step_est: the estimate needs tol > 0");
+  int d = 0;
+  DGTD_TRY(krylov_run(op, y, b, h, m, tol, out, &d, est, true));
   if (dim_used) *dim_used = d;
   return DGTD_OK;
 }

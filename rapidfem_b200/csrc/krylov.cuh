@@ -29,6 +29,7 @@ struct KrylovDev {
   double coef[kKrylovMaxDim];               // final combination coefficients
   double w_s;                               // augmented component of the working vector
   double beta, inv_beta, inv_h, t, tol;
+  double est;                               // last a-posteriori estimate (tol > 0), 0 on breakdown
   int dim;                                  // dimension decided so far (the final one when done)
   int done;                                 // 1: stop growing the space
   int aug;                                  // 1: ETD augmented system
@@ -230,6 +231,7 @@ __global__ void k_finish_start(KrylovDev* st, const double* partials, int nblock
     st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
     st->t = t;
     st->tol = tol;
+    st->est = beta == 0.0 ? 0.0 : -1.0;  // -1: no estimate formed (tol = 0)
     st->aug = aug;
     st->max_dim = max_dim;
     st->dim = max_dim;
@@ -279,17 +281,21 @@ __global__ void k_finish_norm(KrylovDev* st, const double* partials, int nblocks
   extern __shared__ double sm[];
   __shared__ double s_hnext;
   __shared__ int s_stop;
+  __shared__ int s_break;
   const int d = j + 1;
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKrylovMaxDim];
     if (st->aug) s += st->w_s * st->w_s;
     s_hnext = sqrt(s);
-    s_stop = (s_hnext < 1e-12 || d == st->max_dim) ? 1 : 0;
+    s_break = s_hnext < 1e-12 ? 1 : 0;
+    s_stop = (s_break || d == st->max_dim) ? 1 : 0;
+    if (s_break) st->est = 0.0;
   }
   __syncthreads();
   const double hnext = s_hnext;
-  if (!s_stop && st->tol > 0.0) {
+  // the estimate is also formed at the last dimension, where it only reports
+  if (!s_break && st->tol > 0.0) {
     double* a = sm;
     double* out = a + kKrylovMaxDim * kKrylovMaxDim;
     double* b = out + kKrylovMaxDim * kKrylovMaxDim;
@@ -302,7 +308,11 @@ __global__ void k_finish_norm(KrylovDev* st, const double* partials, int nblocks
     }
     __syncthreads();
     block_expm(a, d, out, b, t1, t2);
-    if (threadIdx.x == 0 && hnext * fabs(out[(d - 1) * d]) < st->tol) s_stop = 1;
+    if (threadIdx.x == 0) {
+      const double est = hnext * fabs(out[(d - 1) * d]);
+      st->est = est;
+      if (est < st->tol) s_stop = 1;
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {

@@ -1,0 +1,241 @@
+"""Adaptive exponential (ETD) time stepping on the device with an a-posteriori
+Krylov error check, and a learned step proposer.
+
+A step of dy/dt = A y + b g(t) is the augmented exponential
+exp(h [[A, b g_n],[0, 0]]) [y; 1] (propagator.rs:338-373, g held at the step
+start); the device Arnoldi reports its a-posteriori estimate
+h_{d+1,d}|exp(tH)_{d-1,0}| (propagator.rs:278-294), and a step is accepted when
+the estimate is at most `tol`.
+
+PlainEtd is the adaptive controller: after a step it scales h by
+0.9 (tol/est)^(1/(d+1)) (d the Krylov dimension per sub-step), clipped to
+[1/2, 2] after an accepted step and to [1/4, 1/2] after a rejected one, with
+the Krylov dimension capped at m_max.
+
+LearnedEtd asks a small MLP (16 -> 64 -> 64 -> 2, trained on traces the plain
+controller logged) for the next step size and Krylov cap from the history of
+the last four accepted steps; the proposal is tried and kept only if its
+estimate passes, otherwise the plain controller decides the step (and remains
+the judge of its error).  The training target of a logged step is what its
+run says in hindsight: the largest step the plain controller itself took
+within the next LOOKAHEAD accepted steps (a step size it reached and passed
+from a similar state), relative to the previous step, and that step's Krylov
+dimension relative to m_max.  The network so learns to skip the plain
+controller's slow growth.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+from ._native import check, lib
+
+N_FEATURES = 16
+N_HIDDEN = 64
+N_OUT = 2
+HISTORY = 4
+LOOKAHEAD = 5
+
+
+class Mlp:
+    """The device MLP (dgtd_mlp_*): forward, gradient and Adam training run as
+    the library's own kernels."""
+
+    def __init__(self, ctx, n_in=N_FEATURES, n_hidden=N_HIDDEN, n_out=N_OUT, seed=0):
+        self.ctx = ctx
+        self.n_in, self.n_hidden, self.n_out = n_in, n_hidden, n_out
+        h = C.c_void_p()
+        check(lib.dgtd_mlp_create(ctx.handle, n_in, n_hidden, n_out, C.c_uint64(seed), C.byref(h)))
+        self._h = h
+        n = C.c_int64()
+        check(lib.dgtd_mlp_n_params(h, C.byref(n)))
+        self.n_params = n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and lib is not None:
+            lib.dgtd_mlp_destroy(h)
+            self._h = C.c_void_p()
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        check(lib.dgtd_mlp_get_params(self._h, out))
+        return out
+
+    @params.setter
+    def params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters")
+        check(lib.dgtd_mlp_set_params(self._h, p))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float32)
+        y = np.empty((x.shape[0], self.n_out), dtype=np.float32)
+        check(lib.dgtd_mlp_forward(self._h, x, x.shape[0], y))
+        return y
+
+    def gradient(self, x, t):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float32)
+        t = np.ascontiguousarray(np.atleast_2d(t), dtype=np.float32)
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_float()
+        check(lib.dgtd_mlp_gradient(self._h, x, t, x.shape[0], g, C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, t, epochs=2000, lr=3e-3) -> np.ndarray:
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float32)
+        t = np.ascontiguousarray(np.atleast_2d(t), dtype=np.float32)
+        losses = np.empty(max(int(epochs), 1), dtype=np.float32)
+        check(lib.dgtd_mlp_train(self._h, x, t, x.shape[0], int(epochs), float(lr), losses))
+        return losses[: int(epochs)]
+
+
+@dataclass
+class StepRecord:
+    h: float
+    dim: int
+    est: float
+    rejected_before: int
+
+
+@dataclass
+class EtdStats:
+    accepted: int = 0
+    rejected: int = 0
+    proposals_kept: int = 0
+    proposals_failed: int = 0
+    matvecs: int = 0
+    seconds: float = 0.0
+    history: list = field(default_factory=list)
+
+
+def features(hist: list, tol: float, m_max: int, h_ref: float) -> np.ndarray:
+    """16 features from the last four accepted steps (most recent first; zero
+    padding before there are four): log10(est/tol)/8, log(h_k/h_{k-1})/2,
+    d_k/m_max, rejections before step k / 4."""
+    f = np.zeros(N_FEATURES, dtype=np.float32)
+    for q in range(HISTORY):
+        k = len(hist) - 1 - q
+        if k < 0:
+            break
+        r = hist[k]
+        prev_h = hist[k - 1].h if k > 0 else h_ref
+        est = max(r.est, 1e-30)
+        f[4 * q + 0] = math.log10(est / tol) / 8.0
+        f[4 * q + 1] = math.log(r.h / prev_h) / 2.0
+        f[4 * q + 2] = r.dim / m_max
+        f[4 * q + 3] = r.rejected_before / 4.0
+    return f
+
+
+class PlainEtd:
+    """The adaptive controller (see the module docstring)."""
+
+    def __init__(self, tol=1e-7, m_max=48, safety=0.9):
+        self.tol, self.m_max, self.safety = float(tol), int(m_max), float(safety)
+
+    def _factor(self, est, dim, m, accepted):
+        chunks = max(1, math.ceil(m / 12))
+        d = max(1.0, dim / chunks)
+        est = max(est, 1e-300)
+        f = self.safety * (self.tol / est) ** (1.0 / (d + 1.0))
+        return min(max(f, 0.5), 2.0) if accepted else min(max(f, 0.25), 0.5)
+
+    def next_after(self, h, est, dim, m, accepted):
+        return h * self._factor(est, dim, m, accepted), self.m_max
+
+
+class LearnedEtd:
+    """MLP proposals, kept only when their estimate passes (else PlainEtd)."""
+
+    def __init__(self, mlp: Mlp, plain: PlainEtd, m_min=10):
+        self.mlp, self.plain, self.m_min = mlp, plain, int(m_min)
+
+    def propose(self, hist, h_ref):
+        x = features(hist, self.plain.tol, self.plain.m_max, h_ref)
+        out = self.mlp.forward(x[None, :])[0]
+        h_prev = hist[-1].h if hist else h_ref
+        h = h_prev * math.exp(float(np.clip(out[0], -1.4, 1.4)))
+        # The Krylov cap sets the number of <= 12-dimensional sub-steps, so a
+        # cap below the predicted dimension starves every sub-step: the
+        # predicted dimension is rounded up to whole sub-steps with a margin.
+        d = float(np.clip(out[1], 0.0, 1.0)) * self.plain.m_max
+        m = int(min(self.plain.m_max, max(self.m_min, 12 * math.ceil((1.25 * d + 1) / 12))))
+        return h, m
+
+
+def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEtd | None = None,
+            log: list | None = None, max_attempts=100000):
+    """ETD from t = 0 to t_end; returns (y, EtdStats).  `log`, if given, gets a
+    (features, target) pair per accepted step of the plain controller for
+    training (the look-ahead target of the module docstring)."""
+    y = np.asarray(y0, dtype=np.float64).copy()
+    b = np.zeros_like(y) if b is None else np.asarray(b, dtype=np.float64)
+    st = EtdStats()
+    pending = []  # (features, index of the accepted step, previous step) awaiting look-ahead targets
+    hist: list[StepRecord] = []
+    t, h, m = 0.0, float(h0), plain.m_max
+    rejects = 0
+    w0 = time.perf_counter()
+    attempts = 0
+    while t < t_end * (1 - 1e-12):
+        attempts += 1
+        if attempts > max_attempts:
+            raise RuntimeError("ETD run exceeded the attempt limit")
+        g = 0.0 if waveform is None else float(waveform(t))
+        feat = features(hist, plain.tol, plain.m_max, h0)
+        tried_learned = False
+        if learned is not None:
+            hp, mp = learned.propose(hist, h0)
+            hp = min(hp, t_end - t)
+            y_new, dim, est = gop.etd_step_est(y, b * g, hp, mp, plain.tol)
+            st.matvecs += dim
+            tried_learned = True
+            if est <= plain.tol:
+                st.proposals_kept += 1
+                st.accepted += 1
+                t += hp
+                y = y_new
+                hist.append(StepRecord(hp, dim, est, rejects))
+                rejects = 0
+                h, m = plain.next_after(hp, est, dim, mp, True)
+                continue
+            st.proposals_failed += 1
+        h_try = min(h, t_end - t)
+        y_new, dim, est = gop.etd_step_est(y, b * g, h_try, m, plain.tol)
+        st.matvecs += dim
+        if est <= plain.tol:
+            st.accepted += 1
+            if log is not None and not tried_learned:
+                pending.append((feat, len(hist), hist[-1].h if hist else h0))
+            t += h_try
+            y = y_new
+            hist.append(StepRecord(h_try, dim, est, rejects))
+            rejects = 0
+            h, m = plain.next_after(h_try, est, dim, m, True)
+        else:
+            st.rejected += 1
+            rejects += 1
+            h, m = plain.next_after(h_try, est, dim, m, False)
+    st.seconds = time.perf_counter() - w0
+    st.history = [(r.h, r.dim, r.est) for r in hist]
+    if log is not None:
+        for feat, k, prev in pending:
+            window = hist[k:k + LOOKAHEAD]
+            best = max(window, key=lambda r: r.h)
+            log.append((feat, np.array([math.log(best.h / prev), best.dim / plain.m_max], dtype=np.float32)))
+    return y, st
+
+
+def train_controller(mlp: Mlp, logs: list, epochs=3000, lr=3e-3) -> np.ndarray:
+    """Fit the MLP to logged (features, target) pairs with the device Adam."""
+    x = np.stack([f for f, _ in logs]).astype(np.float32)
+    t = np.stack([g for _, g in logs]).astype(np.float32)
+    return mlp.train(x, t, epochs=epochs, lr=lr)

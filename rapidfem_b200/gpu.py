@@ -210,6 +210,18 @@ class GpuOperator:
                                              series.ctypes.data, yf.ctypes.data))
         return series[: (steps + 1) * nf].reshape(steps + 1, nf), yf
 
+    def etd_step_est(self, y, b, h, m, tol):
+        """ETD step with its a-posteriori Krylov estimate: (out, dim_used, est)."""
+        y = _f64(y)
+        b = _f64(b)
+        self._check_len("state", y)
+        self._check_len("source", b)
+        out = np.empty_like(y)
+        dim = C.c_int32()
+        est = C.c_double()
+        check(lib.dgtd_etd_step_est(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim), C.byref(est)))
+        return out, dim.value, est.value
+
     def lserk_stage(self, h, stage, drive=None, g=0.0):
         """One fused LSERK4 stage on the resident state (drivers that act between
         stages, e.g. a partitioned run's halo exchange)."""
