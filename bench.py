@@ -412,6 +412,110 @@ def run_c4(args):
     return 0
 
 
+def run_time_to_t(args):
+    """Time to reach T at <= 1e-4 relative L2 against the FP64 oracle: plain FP32
+    LSERK4 on the GPU vs the tensor-core LSERK4 and the adaptive / learned ETD
+    integrators, on the stiff graded-slab case (the grid graded 20:1 toward
+    z = 0, N = 3, a lossy slab z < 0.2 with eps_r 2.2 and sigma 5), free
+    evolution of a Gaussian E_z pulse.  The headline value is the learned ETD
+    time; the ratio to the plain FP32 LSERK4 time is in `config.methods`."""
+    import ctypes as C
+
+    import torch
+
+    from oracle import oracle as R
+    from rapidfem_b200 import _native as nat
+    from rapidfem_b200 import etd as E
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    n_cells, order, T = args.ttt_cells, 3, args.ttt_time
+    wl = W.graded_slab(n_cells, order)
+    op = wl.build()
+    x = op.node_coords()
+
+    def pulse(c, s=0.08):
+        y = np.zeros((x.shape[0], 6))
+        y[:, 2] = np.exp(-((x - np.array(c)) ** 2).sum(axis=1) / (2 * s * s))
+        return y.ravel()
+
+    y0 = pulse([0.5, 0.5, 0.3])
+    ctx = G.GpuContext(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    gop = G.GpuOperator(ctx, op)
+    rho = C.c_double()
+    nat.check(nat.lib.dgtd_power_rho(gop.handle, 40, C.byref(rho)))
+    rho = rho.value
+    dt_cfl = 2.8 / rho
+    steps = int(np.ceil(T / (0.5 * dt_cfl)))
+    dt = T / steps
+
+    # the FP64 oracle at half the step
+    R.build()
+    cores = os.cpu_count() or 1
+    R.set_threads(cores)
+    orc = R.Operator(wl.mesh.nodes, wl.mesh.tets, order, 1.0, materials=wl.materials)
+    w = time.perf_counter()
+    ref = orc.lserk(y0.astype(np.float32).astype(np.float64), dt / 2, 2 * steps)
+    oracle_s = time.perf_counter() - w
+
+    def rel(a):
+        return float(np.linalg.norm(np.asarray(a, dtype=np.float64) - ref) / np.linalg.norm(ref))
+
+    methods = {}
+    for name, eng in (("lserk4_fp32", nat.ENGINE_FP32), ("lserk4_tf32x3", nat.ENGINE_TF32X3)):
+        gop.set_engine(eng)
+        gop.upload(y0)
+        gop.run_lserk(dt, 2)  # warm
+        gop.upload(y0)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gop.run_lserk(dt, steps)
+        e1.record(stream)
+        stream.synchronize()
+        methods[name] = {"seconds": e0.elapsed_time(e1) * 1e-3, "rel_l2": rel(gop.download()), "steps": steps,
+                         "matvecs": 5 * steps, "dt": dt}
+    gop.set_engine(nat.ENGINE_FP32)
+    plain = E.PlainEtd(tol=1e-7, m_max=48)
+    logs = []
+    for c in ([0.3, 0.4, 0.5], [0.6, 0.5, 0.4], [0.5, 0.3, 0.6], [0.4, 0.6, 0.2], [0.7, 0.3, 0.4]):
+        E.run_etd(gop, pulse(c), None, None, T, 4 * dt_cfl, plain, log=logs)
+    mlp = E.Mlp(ctx, seed=1)
+    w = time.perf_counter()
+    losses = E.train_controller(mlp, logs, epochs=3000, lr=3e-3)
+    train_s = time.perf_counter() - w
+    for name, learned in (("etd_plain", None), ("etd_learned", E.LearnedEtd(mlp, plain))):
+        yf, st = E.run_etd(gop, y0, None, None, T, 4 * dt_cfl, plain, learned=learned)
+        methods[name] = {"seconds": st.seconds, "rel_l2": rel(yf), "steps": st.accepted, "rejected": st.rejected,
+                         "matvecs": st.matvecs, "proposals_kept": st.proposals_kept,
+                         "proposals_failed": st.proposals_failed}
+    base = methods["lserk4_fp32"]["seconds"]
+    for m in methods.values():
+        m["speedup_vs_lserk4_fp32"] = base / m["seconds"]
+        m["within_1e-4"] = m["rel_l2"] <= 1e-4
+    line = {
+        "metric": "time-to-T at <= 1e-4 relative L2 vs the FP64 oracle", "value": methods["etd_learned"]["seconds"],
+        "unit": "s", "n_gpus": 1, "steps": methods["etd_learned"]["steps"], "warmup": 0,
+        "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"graded slab {n_cells}^3 x 6 tets (20:1 toward z=0), N={order}, lossy slab z<0.2 "
+                               f"eps_r 2.2 sigma 5, free Gaussian E_z pulse at (0.5,0.5,0.3), T={T}",
+                   "n_dof": op.n_dof, "rho": rho, "dt_cfl": dt_cfl, "methods": methods,
+                   "controller_training": {"traces": len(logs), "epochs": 3000, "seconds": train_s,
+                                           "loss_first": float(losses[0]), "loss_last": float(losses[-1])},
+                   "oracle": {"kind": "port", "step": dt / 2, "seconds": oracle_s, "cores": cores}},
+        "e2e": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def cpu_batch_rate(inst, groups, n_inst=4, steps=2):
     """The oracle (f64, OpenMP) on the first instances of the batch."""
     from oracle import oracle as R
@@ -448,8 +552,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-cells", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4"],
-                    help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities")
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "time-to-t"],
+                    help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
+                         "time-to-t: LSERK4 vs adaptive / learned ETD to a final time against the oracle")
+    ap.add_argument("--ttt-cells", type=int, default=12)
+    ap.add_argument("--ttt-time", type=float, default=0.5)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--graph-steps", type=int, default=10)
     args = ap.parse_args()
@@ -458,6 +565,8 @@ def main():
         return run_reference(args)
     if args.workload == "c4":
         return run_c4(args)
+    if args.workload == "time-to-t":
+        return run_time_to_t(args)
     return run_b200(args)
 
 

@@ -14,9 +14,10 @@ the Krylov dimension capped at m_max.
 
 LearnedEtd asks a small MLP (16 -> 64 -> 64 -> 2, trained on traces the plain
 controller logged) for the next step size and Krylov cap from the history of
-the last four accepted steps; the proposal is tried and kept only if its
-estimate passes, otherwise the plain controller decides the step (and remains
-the judge of its error).  The training target of a logged step is what its
+the last four accepted steps; the proposed step is never below the plain
+controller's own next step, it is tried and kept only if its estimate passes,
+otherwise the plain controller decides the step (and remains the judge of its
+error).  The training target of a logged step is what its
 run says in hindsight: the largest step the plain controller itself took
 within the next LOOKAHEAD accepted steps (a step size it reached and passed
 from a similar state), relative to the previous step, and that step's Krylov
@@ -194,7 +195,9 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
         tried_learned = False
         if learned is not None:
             hp, mp = learned.propose(hist, h0)
-            hp = min(hp, t_end - t)
+            # never below the plain controller's own next step: the network
+            # can only skip ahead of it
+            hp = min(max(hp, h), t_end - t)
             y_new, dim, est = gop.etd_step_est(y, b * g, hp, mp, plain.tol)
             st.matvecs += dim
             tried_learned = True
