@@ -53,6 +53,8 @@ const char *dgtd_version(void);
  * Replaces GpuContext::new (crates/rapidfem-td/src/gpu/mod.rs:49): picks the
  * CUDA device, creates the stream the ops run on. */
 int dgtd_ctx_create(int device, dgtd_ctx **out);
+/* Ops and MLPs made on a context may be destroyed after it (their destructors
+ * do not touch the context); any other call on them needs the context alive. */
 int dgtd_ctx_destroy(dgtd_ctx *ctx);
 /* Device name (GpuContext::device_name, gpu/mod.rs:35). */
 int dgtd_ctx_device_name(dgtd_ctx *ctx, char *buf, size_t len);

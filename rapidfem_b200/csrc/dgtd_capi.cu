@@ -153,6 +153,7 @@ struct DevBuf {
 
 struct dgtd_op {
   dgtd_ctx* ctx = nullptr;
+  int device = 0;  // the destructor must not read ctx: a host may free the context first
   int order = 0, np = 0, nfp = 0;
   int64_t n_elem = 0, n_dof = 0;
   float alpha = 1.f;
@@ -186,7 +187,7 @@ struct dgtd_op {
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
-    cudaSetDevice(ctx->device);
+    cudaSetDevice(device);
     meta.free(); dT.free(); liftT.free(); fnodes.free(); gtab.free();
     y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
@@ -482,6 +483,7 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
 
   auto* op = new dgtd_op;
   op->ctx = ctx;
+  op->device = ctx->device;
   op->order = N;
   op->np = np;
   op->nfp = nfp;
@@ -979,12 +981,13 @@ extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t st
 
 struct dgtd_mlp {
   dgtd_ctx* ctx = nullptr;
+  int device = 0;  // as dgtd_op: the destructor does not read ctx
   dgtd::MlpShape S{};
   int step = 0;
   DevBuf<float> p, m, v, grad, loss;
   DevBuf<float> x, y, tg, a1, a2, G, lb;
   ~dgtd_mlp() {
-    cudaSetDevice(ctx->device);
+    cudaSetDevice(device);
     p.free(); m.free(); v.free(); grad.free(); loss.free();
     x.free(); y.free(); tg.free(); a1.free(); a2.free(); G.free(); lb.free();
   }
@@ -1046,6 +1049,7 @@ extern "C" int dgtd_mlp_create(dgtd_ctx* ctx, int32_t n_in, int32_t n_hidden, in
   CUDA_TRY(cudaSetDevice(ctx->device));
   auto n = std::make_unique<dgtd_mlp>();
   n->ctx = ctx;
+  n->device = ctx->device;
   n->S = dgtd::MlpShape{n_in, n_hidden, n_out};
   const int np = n->S.n_params();
   // Glorot-uniform weights, zero biases
