@@ -516,6 +516,98 @@ def run_time_to_t(args):
     return 0
 
 
+def run_c5(args):
+    """The waveguide study: a 22.86 x 10.16 x 60 mm guide (39 x 17 x 101 hex x 6
+    tets), N = 3, a centred dielectric post (r = 1.5 mm) with eps_r spread over
+    2-10 in `--c5-variants` variants, a TE10 Gaussian-modulated pulse (10 GHz,
+    4 GHz FWHM bandwidth) injected by incident-field flux at z = 0, an absorbing
+    port at z = 60 mm, PEC walls; LSERK4 on the tensor-core stage kernel with
+    the modal amplitudes P_e of both ports recorded per step on the device, and
+    the first and last variants' series checked against the FP32 stage kernel."""
+    import ctypes as C
+
+    import torch
+
+    from rapidfem_b200 import _native as nat
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import td as T
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    c_light = 299792458.0
+    a, b_w, L = 22.86e-3, 10.16e-3, 60e-3
+    cells = tuple(args.c5_cells)
+    wl = W.waveguide_post(6.0, order=3, cells=cells)
+    op = wl.build()
+    cen = wl.mesh.nodes[wl.mesh.tets].mean(axis=1)
+    post = np.hypot(cen[:, 0] - a / 2, cen[:, 2] - L / 2) < 1.5e-3
+    prof_in = op.rect_port_profiles(0, [0, 0, 1.0], (1, 0))
+    prof_out = op.rect_port_profiles(1, [0, 0, -1.0], (1, 0))
+    src = op.port_source(0, prof_in)
+    funcs = [op.port_modal_weights(1, prof_out, "E"), op.port_modal_weights(0, prof_in, "E")]
+    ctx = G.GpuContext(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    vac = G.GpuOperator(ctx, op, inv_eps=np.ones(3 * op.n_elem))
+    rho = C.c_double()
+    nat.check(nat.lib.dgtd_power_rho(vac.handle, 40, C.byref(rho)))
+    del vac
+    dt = 0.5 * 2.8 / rho.value  # operator time c*t; eps_r >= 1 only slows waves
+    tau = 2.0 * np.sqrt(np.log(2.0)) / (np.pi * 4e9) * c_light
+    t0 = 3.0 * tau
+    t_end = t0 + 3.0 * tau + L / 0.7
+    steps = int(np.ceil(t_end / dt)) if args.c5_steps <= 0 else args.c5_steps
+    g = T.GaussianPulse(t0, tau, 10e9 / c_light)(np.arange(steps) * dt).astype(np.float32)
+    V = args.c5_variants
+    eps_list = [2.0 + 8.0 * k / max(V - 1, 1) for k in range(V)]
+
+    def run(eps, engine):
+        ie = np.repeat(np.where(post, 1.0 / eps, 1.0), 3)
+        gop = G.GpuOperator(ctx, op, inv_eps=ie)
+        gop.set_engine(engine)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        series, _ = gop.transient_functionals(np.zeros(op.n_dof), dt, steps, 1, drive=("vector", src), g=g,
+                                              functionals=funcs)
+        e1.record(stream)
+        stream.synchronize()
+        return series, e0.elapsed_time(e1) * 1e-3
+
+    series, secs = [], []
+    for eps in eps_list:
+        s_, t_ = run(eps, nat.ENGINE_TF32X3)
+        series.append(s_)
+        secs.append(t_)
+    checks = []
+    for k in sorted({0, V - 1}):
+        ref, _ = run(eps_list[k], nat.ENGINE_FP32)
+        checks.append({"eps_r": eps_list[k],
+                       "rel_l2_out": float(np.linalg.norm(series[k][:, 0] - ref[:, 0]) / np.linalg.norm(ref[:, 0])),
+                       "rel_l2_in": float(np.linalg.norm(series[k][:, 1] - ref[:, 1]) / np.linalg.norm(ref[:, 1]))})
+    total = sum(secs)
+    value = V * op.n_dof * 5 * steps / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "ms_per_step": total / (V * steps) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"WR-90 section 22.86x10.16x60 mm, {cells[0]}x{cells[1]}x{cells[2]} hex x 6 = "
+                               f"{op.n_elem} tets, N=3, dielectric post r=1.5 mm eps_r in 2..10 ({V} variants), "
+                               "TE10 pulse 10 GHz / 4 GHz FWHM injected at z=0, absorbing port at z=60 mm, PEC "
+                               "walls; LSERK4 (tensor-core stage kernel), port modal amplitudes per step on the device",
+                   "n_dof_per_variant": op.n_dof, "dt_operator": dt, "variants": V,
+                   "series_vs_fp32_engine": checks,
+                   "peak_transmitted_Pe": [float(np.max(np.abs(s_[:, 0]))) for s_ in series],
+                   "seconds_per_variant": secs},
+        "gpu_launches": V * 5 * steps + V * (steps + 1),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def cpu_batch_rate(inst, groups, n_inst=4, steps=2):
     """The oracle (f64, OpenMP) on the first instances of the batch."""
     from oracle import oracle as R
@@ -552,9 +644,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-cells", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "time-to-t"],
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
+                         "c5: the waveguide post variants with port probes; "
                          "time-to-t: LSERK4 vs adaptive / learned ETD to a final time against the oracle")
+    ap.add_argument("--c5-variants", type=int, default=32)
+    ap.add_argument("--c5-cells", type=int, nargs=3, default=[39, 17, 101])
+    ap.add_argument("--c5-steps", type=int, default=0, help="0: long enough for the pulse to cross the guide")
     ap.add_argument("--ttt-cells", type=int, default=12)
     ap.add_argument("--ttt-time", type=float, default=0.5)
     ap.add_argument("--instances", type=int, default=256)
@@ -567,6 +663,8 @@ def main():
         return run_c4(args)
     if args.workload == "time-to-t":
         return run_time_to_t(args)
+    if args.workload == "c5":
+        return run_c5(args)
     return run_b200(args)
 
 

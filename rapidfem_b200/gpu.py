@@ -67,9 +67,12 @@ def _f64(a):
 class GpuOperator:
     """GpuOperator::new (gpu/operator.rs:207): the operator resident on the device."""
 
-    def __init__(self, ctx: GpuContext, op: MaxwellOperator, dt_scale=None):
+    def __init__(self, ctx: GpuContext, op: MaxwellOperator, dt_scale=None, inv_eps=None):
         """`dt_scale[K]` (optional): a per-element multiplier of the LSERK4 step,
-        for a batch of independent instances that step with their own dt."""
+        for a batch of independent instances that step with their own dt.
+        `inv_eps[K,3]` (optional): replaces the host operator's 1/eps, for
+        lossless material variants of one mesh (the host operator's sigma/eps
+        is kept as it is)."""
         self.ctx = ctx
         self.host_op = op
         d = op.desc()
@@ -78,6 +81,11 @@ class GpuOperator:
             if ds.size != op.n_elem:
                 raise ValueError("dt_scale needs one entry per element")
             d.dt_scale = ds.ctypes.data
+        if inv_eps is not None:
+            ie = np.ascontiguousarray(inv_eps, dtype=np.float64).ravel()
+            if ie.size != 3 * op.n_elem:
+                raise ValueError("inv_eps needs three entries per element")
+            d.inv_eps = ie.ctypes.data
         h = C.c_void_p()
         check(lib.dgtd_op_create(ctx.handle, C.byref(d), C.byref(h)))
         self._h = h
