@@ -23,6 +23,9 @@
 //                   tiles deep, residual register two deep), the MMAs of both
 //                   contractions into one of two TMEM accumulator sets, and the
 //                   bulk async stores.
+// The LIFT operand is formed and multiplied in two halves (faces 0-1, 2-3),
+// each released by its own MMA completion, so the LIFT MMAs of one half run
+// while the flux warps form the other half (or the next tile's volume operand).
 // All hand-offs are mbarriers; every wait is bounded and an expired wait stops
 // the CTA cleanly with an error flag.  The element count is padded on the
 // device to a multiple of E with inert records (PEC faces, zero metric), so
@@ -92,7 +95,9 @@ struct TcCfg {
   static constexpr int META_B = E * kMetaWords * 4;
   // per-thread work
   static constexpr int SLOTS = E * KL;                                         // flux slots, all faces
-  static constexpr int ITEMS_F = (SLOTS + kTcFluxThreads - 1) / kTcFluxThreads;
+  static constexpr int HSLOTS = SLOTS / 2;                                     // faces 0-1 | faces 2-3
+  static constexpr int ITEMS_H = (HSLOTS + kTcFluxThreads - 1) / kTcFluxThreads;
+  static constexpr int KS_H = KL / 16;                                         // LIFT k-steps per half
   static constexpr int VCH = KV / 8;                                           // volume-operand column chunks
   static constexpr int VCH_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
   static constexpr int ECH = (NP + 3) / 4;                                     // epilogue node chunks of 4
@@ -119,7 +124,8 @@ struct TcCfg {
   static_assert(T_ALO + KV <= TMEM_COLS, "TMEM columns");
   static_assert((TILE_B % 16) == 0 && (META_B % 16) == 0, "bulk copies need 16-byte sizes");
   static_assert(NV <= 256 && NL2 <= 256 && (NV % 16) == 0 && (NL2 % 16) == 0, "MMA N limits");
-  static_assert(ITEMS_F <= 4 && VCH_PER <= 4 && ECH_PER <= 8, "per-thread work tables");
+  static_assert(ITEMS_H <= 2 && VCH_PER <= 4 && ECH_PER <= 8, "per-thread work tables");
+  static_assert((KL % 16) == 0, "LIFT halves are whole k-steps");
 };
 
 // Constant operands prepared by the host: tf32 hi/lo of D (volume B) and LIFT,
@@ -170,7 +176,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   __shared__ __align__(8) uint64_t bar_ld[3];   // state + records of a slot landed
   __shared__ __align__(8) uint64_t bar_p[2];    // residual register of a slot landed
   __shared__ __align__(8) uint64_t bar_avol;    // flux warps: volume operand in TMEM
-  __shared__ __align__(8) uint64_t bar_alift;   // flux warps: LIFT operand in shared memory
+  __shared__ __align__(8) uint64_t bar_alift[2];  // flux warps: LIFT operand half (faces 0-1 | 2-3) written
+  __shared__ __align__(8) uint64_t bar_l0done;    // the MMAs of LIFT half 0 done (half 0 free)
   __shared__ __align__(8) uint64_t bar_vdone;   // volume MMAs done (TMEM operand free)
   __shared__ __align__(8) uint64_t bar_mma[2];  // all MMAs of an accumulator set done
   __shared__ __align__(8) uint64_t bar_epi[2];  // epilogue of a tile done (results staged)
@@ -207,7 +214,9 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       tc::mbar_init(&bar_epi[i], kTcEpiWarps);
     }
     tc::mbar_init(&bar_avol, kTcFluxWarps);
-    tc::mbar_init(&bar_alift, kTcFluxWarps);
+    tc::mbar_init(&bar_alift[0], kTcFluxWarps);
+    tc::mbar_init(&bar_alift[1], kTcFluxWarps);
+    tc::mbar_init(&bar_l0done, 1);
     tc::mbar_init(&bar_vdone, 1);
     tc::mbar_fence_init();
     s_abort = 0;
@@ -247,18 +256,22 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     const bool lane_real = lane < 30;
     const int v_src = lane_real ? ((q4 * 5 + lane / 6) * 6 + lane % 6) * NP : 0;
     const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
-    // flux slots q = (le, face, node-group, node-in-group); packed le | f<<8 | m<<16, -1 idle
-    int f_item[C::ITEMS_F];
+    // flux slots q = (le, face, node-group, node-in-group) of each half (faces
+    // 0-1, then 2-3); packed le | f<<8 | m<<16, -1 idle
+    int f_item[2][C::ITEMS_H];
 #pragma unroll
-    for (int u = 0; u < C::ITEMS_F; ++u) {
-      const int q = tid + u * kTcFluxThreads;
-      f_item[u] = -1;
-      if (q < C::SLOTS) {
-        const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = f * (KLF/4) + mg
-        const int f = rest / (KLF / 4), m = (rest % (KLF / 4)) * 4 + s4;
-        if (m < NFP) f_item[u] = le | (f << 8) | (m << 16);
+    for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+      for (int u = 0; u < C::ITEMS_H; ++u) {
+        const int qh = tid + u * kTcFluxThreads;
+        f_item[hh][u] = -1;
+        if (qh < C::HSLOTS) {
+          const int q = hh * C::HSLOTS + qh;
+          const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = f * (KLF/4) + mg
+          const int f = rest / (KLF / 4), m = (rest % (KLF / 4)) * 4 + s4;
+          if (m < NFP) f_item[hh][u] = le | (f << 8) | (m << 16);
+        }
       }
-    }
     int ys = 0;
     uint32_t ld_par = 0u;  // bit s: parity of the next wait on bar_ld[s]
     for (int64_t it = 0; it < n_my; ++it) {
@@ -297,97 +310,110 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&bar_avol);
       DGTD_TC_MARK(1);
-      // ---- the LIFT operand is free once the previous tile's MMAs are done
-      if (it > 0 && !tc_waitw(&bar_mma[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag)) {
+      // ---- numerical flux (rhs.rs:1370-1441) by halves of the LIFT operand:
+      // faces 0-1, then 2-3.  A half is free once the previous tile's MMAs of
+      // that half are done; its own MMAs then run while the next half is formed.
+      bool half_ok = true;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        if (it > 0) {
+          const bool free_ok = hh == 0 ? tc_waitw(&bar_l0done, (uint32_t)((it - 1) & 1), abort_flag)
+                                       : tc_waitw(&bar_mma[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
+          if (!free_ok) {
+            half_ok = false;
+            break;
+          }
+        }
+        DGTD_TC_MARK(2);
+        {
+          const int u0 = 0;
+          float nb[2][6];
+          // out-of-tile neighbour traces first: independent L2 requests in flight together
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) nb[v][c] = 0.f;
+            const int u = u0 + v;
+            if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
+            const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
+            const float* Me = sM + le * kMetaWords;
+            const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
+            const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
+            const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
+            if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
+              const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
+#pragma unroll
+              for (int c = 0; c < 6; ++c) nb[v][c] = __ldg(Z + c * NP);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+            const int u = u0 + v;
+            if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
+            const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
+            const float* Me = sM + le * kMetaWords;
+            const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
+            const float coef = 0.5f * Me[21 + f];
+            const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
+            const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
+            const int kind = (code >> 8) & 3;
+            const float* Y = sY + le * 6 * NP + sFn[f * NFP + m];
+            const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
+            const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
+            float jex, jey, jez, jhx, jhy, jhz;
+            float a = P.alpha;
+            if (kind == kPort) {
+              // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
+              jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
+              a = 1.0f;
+            } else if (kind == kPec) {
+              // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
+              const float edn = nx * ex + ny * ey + nz * ez;
+              const float hdn = nx * hx + ny * hy + nz * hz;
+              jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
+              jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
+            } else {
+              float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
+              float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
+              const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
+              if (lo >= 0 && lo < E) {
+                const float* Z = sY + lo * 6 * NP + sG[(code & 0xff) * NFP + m];
+                px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
+                qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
+              }
+              jex = ex - px; jey = ey - py; jez = ez - pz;
+              jhx = hx - qx; jhy = hy - qy; jhz = hz - qz;
+            }
+            // fe = coef (-n x [H] + a n x (n x [E])), fh = coef (n x [E] + a n x (n x [H]))
+            // (rhs.rs:1420-1432), with n x (n x v) = n (n.v) - v for the unit normal.
+            const float ca = coef * a;
+            const float de = ca * (nx * jex + ny * jey + nz * jez);
+            const float dh = ca * (nx * jhx + ny * jhy + nz * jhz);
+            float fl[6];
+            fl[0] = fmaf(de, nx, fmaf(-ca, jex, -coef * (ny * jhz - nz * jhy)));
+            fl[1] = fmaf(de, ny, fmaf(-ca, jey, -coef * (nz * jhx - nx * jhz)));
+            fl[2] = fmaf(de, nz, fmaf(-ca, jez, -coef * (nx * jhy - ny * jhx)));
+            fl[3] = fmaf(dh, nx, fmaf(-ca, jhx, coef * (ny * jez - nz * jey)));
+            fl[4] = fmaf(dh, ny, fmaf(-ca, jhy, coef * (nz * jex - nx * jez)));
+            fl[5] = fmaf(dh, nz, fmaf(-ca, jhz, coef * (nx * jey - ny * jex)));
+            const int s = f * KLF + m;
+            const uint32_t off = (uint32_t)((s >> 2) * (M / 8) * 128 + (s & 3) * 4 + tc_row(le, 0) * 16);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+              const float h = tc::tf32_round(fl[c]);
+              *reinterpret_cast<float*>(alh + off + c * 16) = h;
+              *reinterpret_cast<float*>(all + off + c * 16) = tc::tf32_round(fl[c] - h);
+            }
+          }
+        }
+        tc::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&bar_alift[hh]);
+      }
+      if (!half_ok) {
         *abort_flag = 1;
         break;
       }
-      DGTD_TC_MARK(2);
-      // ---- numerical flux of all four faces (rhs.rs:1370-1441), two slots at a time
-#pragma unroll
-      for (int u0 = 0; u0 < C::ITEMS_F; u0 += 2) {
-        float nb[2][6];
-        // out-of-tile neighbour traces first: independent L2 requests in flight together
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-#pragma unroll
-          for (int c = 0; c < 6; ++c) nb[v][c] = 0.f;
-          const int u = u0 + v;
-          if (u >= C::ITEMS_F || f_item[u] < 0) continue;
-          const int le = f_item[u] & 0xff, f = (f_item[u] >> 8) & 0xff, m = f_item[u] >> 16;
-          const float* Me = sM + le * kMetaWords;
-          const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
-          const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
-          const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
-          if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
-            const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) nb[v][c] = __ldg(Z + c * NP);
-          }
-        }
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-          const int u = u0 + v;
-          if (u >= C::ITEMS_F || f_item[u] < 0) continue;
-          const int le = f_item[u] & 0xff, f = (f_item[u] >> 8) & 0xff, m = f_item[u] >> 16;
-          const float* Me = sM + le * kMetaWords;
-          const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
-          const float coef = 0.5f * Me[21 + f];
-          const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
-          const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
-          const int kind = (code >> 8) & 3;
-          const float* Y = sY + le * 6 * NP + sFn[f * NFP + m];
-          const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
-          const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
-          float jex, jey, jez, jhx, jhy, jhz;
-          float a = P.alpha;
-          if (kind == kPort) {
-            // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
-            jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
-            a = 1.0f;
-          } else if (kind == kPec) {
-            // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
-            const float edn = nx * ex + ny * ey + nz * ez;
-            const float hdn = nx * hx + ny * hy + nz * hz;
-            jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
-            jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
-          } else {
-            float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
-            float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
-            const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
-            if (lo >= 0 && lo < E) {
-              const float* Z = sY + lo * 6 * NP + sG[(code & 0xff) * NFP + m];
-              px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
-              qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
-            }
-            jex = ex - px; jey = ey - py; jez = ez - pz;
-            jhx = hx - qx; jhy = hy - qy; jhz = hz - qz;
-          }
-          // fe = coef (-n x [H] + a n x (n x [E])), fh = coef (n x [E] + a n x (n x [H]))
-          // (rhs.rs:1420-1432), with n x (n x v) = n (n.v) - v for the unit normal.
-          const float ca = coef * a;
-          const float de = ca * (nx * jex + ny * jey + nz * jez);
-          const float dh = ca * (nx * jhx + ny * jhy + nz * jhz);
-          float fl[6];
-          fl[0] = fmaf(de, nx, fmaf(-ca, jex, -coef * (ny * jhz - nz * jhy)));
-          fl[1] = fmaf(de, ny, fmaf(-ca, jey, -coef * (nz * jhx - nx * jhz)));
-          fl[2] = fmaf(de, nz, fmaf(-ca, jez, -coef * (nx * jhy - ny * jhx)));
-          fl[3] = fmaf(dh, nx, fmaf(-ca, jhx, coef * (ny * jez - nz * jey)));
-          fl[4] = fmaf(dh, ny, fmaf(-ca, jhy, coef * (nz * jex - nx * jez)));
-          fl[5] = fmaf(dh, nz, fmaf(-ca, jhz, coef * (nx * jey - ny * jex)));
-          const int s = f * KLF + m;
-          const uint32_t off = (uint32_t)((s >> 2) * (M / 8) * 128 + (s & 3) * 4 + tc_row(le, 0) * 16);
-#pragma unroll
-          for (int c = 0; c < 6; ++c) {
-            const float h = tc::tf32_round(fl[c]);
-            *reinterpret_cast<float*>(alh + off + c * 16) = h;
-            *reinterpret_cast<float*>(all + off + c * 16) = tc::tf32_round(fl[c] - h);
-          }
-        }
-      }
-      tc::fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&bar_alift);
       DGTD_TC_MARK(3);
       ys = ys == 2 ? 0 : ys + 1;
     }
@@ -485,7 +511,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     }
   } else if (ctl0) {
     // ================= control lane: loads, MMAs, stores
-    uint32_t n_ld[3] = {0u, 0u, 0u}, n_p[2] = {0u, 0u}, n_mma[2] = {0u, 0u}, n_vd = 0u;
+    uint32_t n_ld[3] = {0u, 0u, 0u}, n_p[2] = {0u, 0u}, n_mma[2] = {0u, 0u}, n_vd = 0u, n_l0 = 0u;
     const uint32_t idv = tc::idesc_tf32(M, NV), idl = tc::idesc_tf32(M, C::NL2);
     const uint32_t bvh = tc::smem_u32(tsm + C::O_BVH), bvl = tc::smem_u32(tsm + C::O_BVL);
     const uint32_t bl = tc::smem_u32(tsm + C::O_BL);
@@ -538,20 +564,30 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       }
       tc::mma_commit(&bar_vdone);
       ++n_vd;
-      // LIFT MMAs: A = flux hi/lo (shared), B = stacked LIFT hi/lo (shared):
-      // columns [NV, NV+NL) collect hi*hi + lo*hi, [NV+NL, NV+2NL) hi*lo + lo*lo
-      ok = tc_wait1(&bar_alift, (uint32_t)(it & 1), abort_flag);
-      if (!ok) break;
-      tc::tc_fence_after();
-      DGTD_TC_MARK(6);
+      // LIFT MMAs by halves: A = flux hi/lo (shared), B = stacked LIFT hi/lo
+      // (shared): columns [NV, NV+NL) collect hi*hi + lo*hi, [NV+NL, NV+2NL)
+      // hi*lo + lo*lo.  Half 0's commit frees it for the next tile's flux.
 #pragma unroll 1
-      for (int ks = 0; ks < C::KL / 8; ++ks) {
-        const uint64_t bd = tc::tf32_step_desc(bl, C::NL2, ks);
-        tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(ah, M, ks), bd, idl, ks > 0 ? 1u : 0u);
-        tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(al, M, ks), bd, idl, 1u);
+      for (int hh = 0; hh < 2 && ok; ++hh) {
+        ok = tc_wait1(&bar_alift[hh], (uint32_t)(it & 1), abort_flag);
+        if (!ok) break;
+        tc::tc_fence_after();
+        DGTD_TC_MARK(6);
+#pragma unroll 1
+        for (int ks = hh * C::KS_H; ks < (hh + 1) * C::KS_H; ++ks) {
+          const uint64_t bd = tc::tf32_step_desc(bl, C::NL2, ks);
+          tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(ah, M, ks), bd, idl, ks > 0 ? 1u : 0u);
+          tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(al, M, ks), bd, idl, 1u);
+        }
+        if (hh == 0) {
+          tc::mma_commit(&bar_l0done);
+          ++n_l0;
+        } else {
+          tc::mma_commit(&bar_mma[as]);
+          ++n_mma[as];
+        }
       }
-      tc::mma_commit(&bar_mma[as]);
-      ++n_mma[as];
+      if (!ok) break;
       // results of the previous tile -> HBM
       if (it > 0) {
         ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
@@ -580,6 +616,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
         if (n_mma[s]) (void)tc::mbar_wait(&bar_mma[s], (n_mma[s] - 1) & 1u, kTcWaitLimit);
       }
       if (n_vd) (void)tc::mbar_wait(&bar_vdone, (n_vd - 1) & 1u, kTcWaitLimit);
+      if (n_l0) (void)tc::mbar_wait(&bar_l0done, (n_l0 - 1) & 1u, kTcWaitLimit);
     }
   }
 
