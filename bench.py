@@ -263,7 +263,7 @@ def run_b200(args):
         "config": {"workload": "sphere_pulse: jittered 48^3x6 box (663,552 tets), N=4, eps_r=4 sphere r=0.25, "
                                "Gaussian Ez pulse sigma=0.05 at (0.3,0.4,0.5), upwind, PEC, LSERK4",
                    "cells": f"{args.cells}^3", "order": order, "n_dof": n, "dt": dt,
-                   "engine": ["fp32", "tf32x3", "bf16x3"][gop.engine],
+                   "engine": ["fp32", "tf32x3"][gop.engine],
                    "l2": "state 4*n_dof bytes per buffer >> 126 MB L2; no flush",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
         "gpu_launches": launches,

@@ -484,6 +484,7 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   auto* op = new dgtd_op;
   op->ctx = ctx;
   op->device = ctx->device;
+  op->engine = N <= 4 ? DGTD_ENGINE_TF32X3 : DGTD_ENGINE_FP32;
   op->order = N;
   op->np = np;
   op->nfp = nfp;

@@ -49,6 +49,7 @@ def test_waveguide_variants_port_series():
         built = O.MaxwellOperator(wl.mesh, 2, 1.0, face_port=wl.face_port,
                                   materials=O.isotropic_materials(np.where(post, eps, 1.0)))
         ref_op = G.GpuOperator(ctx, built)
+        ref_op.set_engine(nat.ENGINE_FP32)
         ref, _ = ref_op.transient_functionals(np.zeros(op.n_dof), dt, steps, 1, drive=("vector", src), g=g,
                                               functionals=funcs)
         assert np.array_equal(got[nat.ENGINE_FP32], ref)

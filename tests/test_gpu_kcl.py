@@ -13,7 +13,7 @@ from oracle import oracle as R
 from rapidfem_b200 import gpu as G
 from rapidfem_b200 import operator as O
 from rapidfem_b200 import td as T
-from rapidfem_b200._native import DGTD_ERR_COLLAPSE, DgtdError
+from rapidfem_b200._native import DGTD_ERR_COLLAPSE, ENGINE_FP32, ENGINE_TF32X3, DgtdError
 
 from .conftest import rel_l2
 
@@ -93,9 +93,14 @@ def test_kcl_step_matches_oracle(ctx):
     assert rel_l2(e_gpu, e_ref) < 2e-2
 
 
-def test_kcl_run_matches_host_controller(ctx):
+@pytest.mark.parametrize("engine,slack", [(ENGINE_FP32, 2), (ENGINE_TF32X3, 6)], ids=["fp32", "tf32x3"])
+def test_kcl_run_matches_host_controller(ctx, engine, slack):
+    """The replayed reference loop decides on f64 oracle states; the device on
+    f32 states (FP32 kernel: the reference's own f32 path), so decisions near
+    the err_norm = 1 threshold may differ by a few."""
     prod, orc, y0 = _cavity()
     gop = G.GpuOperator(ctx, prod)
+    gop.set_engine(engine)
     rho, _ = orc.power_rho(30)
     dt = 4.0 / rho  # frames longer than the stability limit: the controller must cut the step
     steps = 6
@@ -103,7 +108,7 @@ def test_kcl_run_matches_host_controller(ctx):
     traj, st = gop.transient_kcl(y0, dt, steps, controller=ctl, record=True)
     y_host, acc, rej = _host_kcl(orc, y0.astype(np.float32).astype(np.float64), dt, steps, ctl)
     assert st["accepted"] + st["rejected"] > steps
-    assert abs(st["accepted"] - acc) <= 2 and abs(st["rejected"] - rej) <= 2
+    assert abs(st["accepted"] - acc) <= slack and abs(st["rejected"] - rej) <= slack
     assert rel_l2(traj[-1], y_host) < 1e-3
     assert 0 < st["h_min"] <= st["h_max"]
     assert np.array_equal(traj[0], y0.astype(np.float32))

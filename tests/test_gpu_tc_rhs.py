@@ -55,6 +55,7 @@ def test_tc_matches_fp32_engine(ctx):
     m = O.structured_box_jittered(7, 7, 7, 1.0, 1.0, 1.0, 0.1, 3)
     prod = O.MaxwellOperator(m, 4, 1.0)
     a = G.GpuOperator(ctx, prod)
+    a.set_engine(_native.ENGINE_FP32)
     b = G.GpuOperator(ctx, prod)
     b.set_engine(TF32X3)
     x = prod.node_coords()
