@@ -56,8 +56,8 @@
 namespace dgtd {
 
 constexpr int kTcTileE = 20;
-constexpr int kTcFluxWarps = 16;                          // warps 0..15
-constexpr int kTcEpiWarps = 8;                            // warps 16..23
+constexpr int kTcFluxWarps = 12;                          // warps 0..11
+constexpr int kTcEpiWarps = 12;                           // warps 12..23
 constexpr int kTcCtlWarp = kTcFluxWarps + kTcEpiWarps;    // warp 24, lane 0
 constexpr int kTcThreadsAll = (kTcCtlWarp + 1) * 32;
 constexpr int kTcFluxThreads = kTcFluxWarps * 32;
@@ -272,6 +272,28 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           if (m < NFP) f_item[hh][u] = le | (f << 8) | (m << 16);
         }
       }
+    // Out-of-tile neighbour traces of this thread's slots in half hh (global
+    // loads, zero where the neighbour is in the tile or absent).  They are
+    // issued a phase ahead of their use: half 0's before the volume operand is
+    // formed, half 1's before half 0's fluxes, so their latency is hidden.
+    const auto nb_fetch = [&](const float* sM, int64_t e0, int hh, float (&nb)[2][6]) {
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) nb[u][c] = 0.f;
+        if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
+        const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
+        const float* Me = sM + le * kMetaWords;
+        const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
+        const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
+        const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
+        if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
+          const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) nb[u][c] = __ldg(Z + c * NP);
+        }
+      }
+    };
     int ys = 0;
     uint32_t ld_par = 0u;  // bit s: parity of the next wait on bar_ld[s]
     for (int64_t it = 0; it < n_my; ++it) {
@@ -281,6 +303,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const float* const sM = sM0 + ys * kMStride;
       bool ok = tc_waitw(&bar_ld[ys], (ld_par >> ys) & 1u, abort_flag);
       ld_par ^= 1u << ys;
+      float nb_h[2][2][6];
+      if (ok) nb_fetch(sM, e0, 0, nb_h[0]);
       if (ok && it > 0) ok = tc_waitw(&bar_vdone, (uint32_t)((it - 1) & 1), abort_flag);
       if (!ok) {
         *abort_flag = 1;
@@ -325,30 +349,12 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           }
         }
         DGTD_TC_MARK(2);
+        if (hh == 0) nb_fetch(sM, e0, 1, nb_h[1]);
         {
-          const int u0 = 0;
-          float nb[2][6];
-          // out-of-tile neighbour traces first: independent L2 requests in flight together
+          const float (&nb)[2][6] = nb_h[hh];
 #pragma unroll
           for (int v = 0; v < 2; ++v) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) nb[v][c] = 0.f;
-            const int u = u0 + v;
-            if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
-            const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
-            const float* Me = sM + le * kMetaWords;
-            const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
-            const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
-            const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
-            if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
-              const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
-#pragma unroll
-              for (int c = 0; c < 6; ++c) nb[v][c] = __ldg(Z + c * NP);
-            }
-          }
-#pragma unroll
-          for (int v = 0; v < 2; ++v) {
-            const int u = u0 + v;
+            const int u = v;
             if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
             const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
             const float* Me = sM + le * kMetaWords;
@@ -513,9 +519,16 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     // ================= control lane: loads, MMAs, stores
     uint32_t n_ld[3] = {0u, 0u, 0u}, n_p[2] = {0u, 0u}, n_mma[2] = {0u, 0u}, n_vd = 0u, n_l0 = 0u;
     const uint32_t idv = tc::idesc_tf32(M, NV), idl = tc::idesc_tf32(M, C::NL2);
-    const uint32_t bvh = tc::smem_u32(tsm + C::O_BVH), bvl = tc::smem_u32(tsm + C::O_BVL);
-    const uint32_t bl = tc::smem_u32(tsm + C::O_BL);
-    const uint32_t ah = tc::smem_u32(alh), al = tc::smem_u32(all);
+    // Shared-memory descriptors of k-step 0, built once: k-step ks of an R-row
+    // operand adds ks * 2R (16-byte units) to the start-address field, which
+    // cannot carry (shared addresses are below 2^18).  With the k-steps fully
+    // unrolled the issue of an MMA is an add and the instruction itself, so one
+    // thread keeps the tensor pipe fed.
+    const uint64_t dvh = tc::tf32_step_desc(tc::smem_u32(tsm + C::O_BVH), NV, 0);
+    const uint64_t dvl = tc::tf32_step_desc(tc::smem_u32(tsm + C::O_BVL), NV, 0);
+    const uint64_t dbl = tc::tf32_step_desc(tc::smem_u32(tsm + C::O_BL), C::NL2, 0);
+    const uint64_t dah = tc::tf32_step_desc(tc::smem_u32(alh), M, 0);
+    const uint64_t dal = tc::tf32_step_desc(tc::smem_u32(all), M, 0);
     auto load_y = [&](int64_t j) {  // tile j of this CTA -> slot j % 3
       const int s = (int)(j % 3);
       const int64_t tile = blockIdx.x + j * gridDim.x;
@@ -555,29 +568,41 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       if (!ok) break;
       tc::tc_fence_after();
       DGTD_TC_MARK(6);
-#pragma unroll 1
+#pragma unroll
       for (int ks = 0; ks < KV / 8; ++ks) {
         const uint32_t a_h = tmem + (uint32_t)(C::T_AHI + 8 * ks), a_l = tmem + (uint32_t)(C::T_ALO + 8 * ks);
-        tc::mma_tf32_ta(acc, a_h, tc::tf32_step_desc(bvh, NV, ks), idv, ks > 0 ? 1u : 0u);
-        tc::mma_tf32_ta(acc, a_h, tc::tf32_step_desc(bvl, NV, ks), idv, 1u);
-        tc::mma_tf32_ta(acc, a_l, tc::tf32_step_desc(bvh, NV, ks), idv, 1u);
+        const uint64_t bh = dvh + (uint64_t)(2 * NV * ks), bo = dvl + (uint64_t)(2 * NV * ks);
+        tc::mma_tf32_ta(acc, a_h, bh, idv, ks > 0 ? 1u : 0u);
+        tc::mma_tf32_ta(acc, a_h, bo, idv, 1u);
+        tc::mma_tf32_ta(acc, a_l, bh, idv, 1u);
       }
       tc::mma_commit(&bar_vdone);
       ++n_vd;
+      // Refills: the newest store group is tile it-2's (issued in the previous
+      // iteration); once it has read its slots, they take tile it+1's state
+      // (slot (it+1) % 3) and tile it's residual (slot it & 1).  Waiting after
+      // the volume MMAs are issued keeps the wait off the tensor pipe's path.
+      if (it > 0) {
+        tc::bulk_wait_read0();
+        DGTD_TC_MARK(7);
+        if (it + 1 < n_my) load_y(it + 1);
+        if (use_p) load_p(it);
+      }
       // LIFT MMAs by halves: A = flux hi/lo (shared), B = stacked LIFT hi/lo
       // (shared): columns [NV, NV+NL) collect hi*hi + lo*hi, [NV+NL, NV+2NL)
       // hi*lo + lo*lo.  Half 0's commit frees it for the next tile's flux.
-#pragma unroll 1
-      for (int hh = 0; hh < 2 && ok; ++hh) {
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
         ok = tc_wait1(&bar_alift[hh], (uint32_t)(it & 1), abort_flag);
         if (!ok) break;
         tc::tc_fence_after();
         DGTD_TC_MARK(6);
-#pragma unroll 1
-        for (int ks = hh * C::KS_H; ks < (hh + 1) * C::KS_H; ++ks) {
-          const uint64_t bd = tc::tf32_step_desc(bl, C::NL2, ks);
-          tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(ah, M, ks), bd, idl, ks > 0 ? 1u : 0u);
-          tc::mma_tf32(acc + (uint32_t)NV, tc::tf32_step_desc(al, M, ks), bd, idl, 1u);
+#pragma unroll
+        for (int j = 0; j < C::KS_H; ++j) {
+          const int ks = hh * C::KS_H + j;
+          const uint64_t bd = dbl + (uint64_t)(2 * C::NL2 * ks);
+          tc::mma_tf32(acc + (uint32_t)NV, dah + (uint64_t)(2 * M * ks), bd, idl, ks > 0 ? 1u : 0u);
+          tc::mma_tf32(acc + (uint32_t)NV, dal + (uint64_t)(2 * M * ks), bd, idl, 1u);
         }
         if (hh == 0) {
           tc::mma_commit(&bar_l0done);
@@ -595,11 +620,6 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
         DGTD_TC_MARK(6);
         store(it - 1);
       }
-      // the slots of tile it-1 are refilled once its stores have read them
-      tc::bulk_wait_read0();
-      DGTD_TC_MARK(7);
-      if (it + 2 < n_my) load_y(it + 2);
-      if (it + 1 < n_my && use_p) load_p(it + 1);
     }
     if (ok && n_my > 0) {
       ok = tc_wait1(&bar_epi[(n_my - 1) & 1], (uint32_t)(((n_my - 1) >> 1) & 1), abort_flag);
