@@ -257,19 +257,29 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     const int v_src = lane_real ? ((q4 * 5 + lane / 6) * 6 + lane % 6) * NP : 0;
     const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
     // flux slots q = (le, face, node-group, node-in-group) of each half (faces
-    // 0-1, then 2-3); packed le | f<<8 | m<<16, -1 idle
+    // 0-1, then 2-3).  What does not change from tile to tile is packed once:
+    // f_item = le | f << 5 | m << 7 | (offset of the face node's state in the
+    // tile) << 11, -1 idle; f_off = byte offset of the slot's entry (component 0)
+    // in the LIFT operand.
+    static_assert(E <= 32 && NFP <= 16 && C::TILE_F < (1 << 20), "flux slot packing");
     int f_item[2][C::ITEMS_H];
+    uint32_t f_off[2][C::ITEMS_H];
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh)
 #pragma unroll
       for (int u = 0; u < C::ITEMS_H; ++u) {
         const int qh = tid + u * kTcFluxThreads;
         f_item[hh][u] = -1;
+        f_off[hh][u] = 0u;
         if (qh < C::HSLOTS) {
           const int q = hh * C::HSLOTS + qh;
           const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = f * (KLF/4) + mg
           const int f = rest / (KLF / 4), m = (rest % (KLF / 4)) * 4 + s4;
-          if (m < NFP) f_item[hh][u] = le | (f << 8) | (m << 16);
+          if (m < NFP) {
+            f_item[hh][u] = le | (f << 5) | (m << 7) | ((le * 6 * NP + sFn[f * NFP + m]) << 11);
+            const int sl = f * KLF + m;
+            f_off[hh][u] = (uint32_t)((sl >> 2) * (M / 8) * 128 + (sl & 3) * 4 + tc_row(le, 0) * 16);
+          }
         }
       }
     // Out-of-tile neighbour traces of this thread's slots in half hh (global
@@ -282,13 +292,14 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) nb[u][c] = 0.f;
         if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
-        const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
+        const int x = f_item[hh][u];
+        const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & 15;
         const float* Me = sM + le * kMetaWords;
         const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
         const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
-        const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
-        if (((code >> 8) & 3) == kInterior && !(lo >= 0 && lo < E)) {
-          const float* Z = P.y_in + (e0 + lo) * 6 * NP + sG[(code & 0xff) * NFP + m];
+        const int nbr = __float_as_int(Me[37 + f]);
+        if (((code >> 8) & 3) == kInterior && (uint32_t)(nbr - (int)e0) >= (uint32_t)E) {
+          const float* Z = P.y_in + (int64_t)nbr * (6 * NP) + sG[(code & 0xff) * NFP + m];
 #pragma unroll
           for (int c = 0; c < 6; ++c) nb[u][c] = __ldg(Z + c * NP);
         }
@@ -322,8 +333,9 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           for (int q = 0; q < 8; ++q) {
             const int k = ch * 8 + q;
             const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+            // hi/lo split as for the LIFT operand (flux section below)
             h[q] = tc::tf32_round(v);
-            l[q] = tc::tf32_round(v - h[q]);
+            l[q] = v - h[q];
           }
           tc::tmem_st8(v_taddr + (uint32_t)(C::T_AHI + ch * 8), h);
           tc::tmem_st8(v_taddr + (uint32_t)(C::T_ALO + ch * 8), l);
@@ -356,14 +368,15 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           for (int v = 0; v < 2; ++v) {
             const int u = v;
             if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
-            const int le = f_item[hh][u] & 0xff, f = (f_item[hh][u] >> 8) & 0xff, m = f_item[hh][u] >> 16;
+            const int x = f_item[hh][u];
+            const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & 15;
             const float* Me = sM + le * kMetaWords;
             const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
             const float coef = 0.5f * Me[21 + f];
             const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
             const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
             const int kind = (code >> 8) & 3;
-            const float* Y = sY + le * 6 * NP + sFn[f * NFP + m];
+            const float* Y = sY + (x >> 11);
             const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
             const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
             float jex, jey, jez, jhx, jhy, jhz;
@@ -381,8 +394,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             } else {
               float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
               float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
-              const int64_t lo = (int64_t)__float_as_int(Me[37 + f]) - e0;
-              if (lo >= 0 && lo < E) {
+              const int lo = __float_as_int(Me[37 + f]) - (int)e0;  // element ids fit in int
+              if ((uint32_t)lo < (uint32_t)E) {
                 const float* Z = sY + lo * 6 * NP + sG[(code & 0xff) * NFP + m];
                 px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
                 qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
@@ -402,13 +415,16 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             fl[3] = fmaf(dh, nx, fmaf(-ca, jhx, coef * (ny * jez - nz * jey)));
             fl[4] = fmaf(dh, ny, fmaf(-ca, jhy, coef * (nz * jex - nx * jez)));
             fl[5] = fmaf(dh, nz, fmaf(-ca, jhz, coef * (nx * jey - ny * jex)));
-            const int s = f * KLF + m;
-            const uint32_t off = (uint32_t)((s >> 2) * (M / 8) * 128 + (s & 3) * 4 + tc_row(le, 0) * 16);
+            const uint32_t off = f_off[hh][u];
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
+              // hi = tf32(fl), lo = fl - hi (exact, |lo| <= 2^-11 |fl|).  lo is
+              // stored unrounded: the tf32 MMA reads only its top 19 bits, an
+              // error below 2^-10 |lo| <= 2^-21 |fl|, under the 3xTF32
+              // products' own 2^-22-class terms in the sum of many products.
               const float h = tc::tf32_round(fl[c]);
               *reinterpret_cast<float*>(alh + off + c * 16) = h;
-              *reinterpret_cast<float*>(all + off + c * 16) = tc::tf32_round(fl[c] - h);
+              *reinterpret_cast<float*>(all + off + c * 16) = fl[c] - h;
             }
           }
         }
