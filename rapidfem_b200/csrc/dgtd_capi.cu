@@ -202,24 +202,36 @@ namespace {
 using namespace dgtd;
 
 // ---- layout conversion (AoS y[(e*Np+i)*6+c] <-> SoA y[(e*6+c)*Np+i])
-template <class TI, class TO>
-__global__ void k_aos_to_soa(const TI* __restrict__ aos, TO* __restrict__ soa, int64_t n, int np) {
-  const int64_t per = 6LL * np;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = idx / per;
-    const int r = (int)(idx - e * per);
-    const int c = r / np, i = r - c * np;
-    soa[idx] = (TO)aos[(e * np + i) * 6 + c];
-  }
-}
-template <class TI, class TO>
-__global__ void k_soa_to_aos(const TI* __restrict__ soa, TO* __restrict__ aos, int64_t n, int np) {
-  const int64_t per = 6LL * np;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = idx / per;
-    const int r = (int)(idx - e * per);
-    const int i = r / 6, c = r - i * 6;
-    aos[idx] = (TO)soa[(e * 6 + c) * np + i];
+// Element e occupies the same 6*Np consecutive values in both layouts, so a
+// conversion permutes values inside element blocks: a CTA stages a chunk of
+// kRelayoutElems elements in shared memory with coalesced loads and writes the
+// permuted chunk with coalesced stores (32-bit index arithmetic, Np a
+// compile-time constant).
+constexpr int kRelayoutElems = 8;
+template <class TI, class TO, int NP, bool TO_SOA>
+__global__ void __launch_bounds__(256) k_relayout(const TI* __restrict__ src, TO* __restrict__ dst, int64_t n_elem) {
+  constexpr int PER = 6 * NP, CH = kRelayoutElems * PER;
+  __shared__ TI buf[CH];
+  const int64_t n_chunks = (n_elem + kRelayoutElems - 1) / kRelayoutElems;
+  for (int64_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+    const int64_t base = ch * CH;
+    const int64_t left = (n_elem - ch * kRelayoutElems) * PER;
+    const int len = left < CH ? (int)left : CH;
+    for (int k = threadIdx.x; k < len; k += blockDim.x) buf[k] = src[base + k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+      const int el = k / PER, r = k - el * PER;
+      int from;
+      if (TO_SOA) {
+        const int c = r / NP, i = r - c * NP;  // destination (c, i) <- source (i, c)
+        from = el * PER + i * 6 + c;
+      } else {
+        const int i = r / 6, c = r - i * 6;  // destination (i, c) <- source (c, i)
+        from = el * PER + c * NP + i;
+      }
+      dst[base + k] = (TO)buf[from];
+    }
+    __syncthreads();
   }
 }
 __global__ void k_gather_f32(const float* __restrict__ src, const int64_t* __restrict__ idx,
@@ -263,19 +275,30 @@ int64_t aos_to_soa_index(int64_t dof, int np) {
   return (e * 6 + c) * np + i;
 }
 
-template <class TI, class TO>
-int to_soa(dgtd_op* op, const TI* aos, TO* soa) {
-  k_aos_to_soa<TI, TO><<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(aos, soa, op->n_dof, op->np);
+template <class TI, class TO, bool TO_SOA>
+int relayout(dgtd_op* op, const TI* src, TO* dst) {
+  const int64_t n_elem = op->n_dof / (6 * op->np);
+  const int64_t chunks = (n_elem + kRelayoutElems - 1) / kRelayoutElems;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)op->ctx->num_sms * 16));
+  switch (op->np) {
+    case np_of(1): k_relayout<TI, TO, np_of(1), TO_SOA><<<grid, 256, 0, op->stream()>>>(src, dst, n_elem); break;
+    case np_of(2): k_relayout<TI, TO, np_of(2), TO_SOA><<<grid, 256, 0, op->stream()>>>(src, dst, n_elem); break;
+    case np_of(3): k_relayout<TI, TO, np_of(3), TO_SOA><<<grid, 256, 0, op->stream()>>>(src, dst, n_elem); break;
+    case np_of(4): k_relayout<TI, TO, np_of(4), TO_SOA><<<grid, 256, 0, op->stream()>>>(src, dst, n_elem); break;
+    case np_of(5): k_relayout<TI, TO, np_of(5), TO_SOA><<<grid, 256, 0, op->stream()>>>(src, dst, n_elem); break;
+    default: return set_error(DGTD_ERR_UNSUPPORTED, "layout conversion: unsupported order");
+  }
   op->launches++;
   CUDA_TRY(cudaGetLastError());
   return DGTD_OK;
 }
 template <class TI, class TO>
+int to_soa(dgtd_op* op, const TI* aos, TO* soa) {
+  return relayout<TI, TO, true>(op, aos, soa);
+}
+template <class TI, class TO>
 int to_aos(dgtd_op* op, const TI* soa, TO* aos) {
-  k_soa_to_aos<TI, TO><<<grid_for(op->n_dof, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(soa, aos, op->n_dof, op->np);
-  op->launches++;
-  CUDA_TRY(cudaGetLastError());
-  return DGTD_OK;
+  return relayout<TI, TO, false>(op, soa, aos);
 }
 
 // ---- RHS kernel dispatch

@@ -167,8 +167,11 @@ class GpuOperator:
                                  nat.ptr(gs), 1 if record else 0, out))
         return out.reshape(steps + 1, self._n) if record else out
 
-    def transient_probes(self, y0, dt, steps, substeps=1, drive=None, g=None, probes=()):
-        """As transient, recording `probes` per frame; returns (series[steps+1, P], y_final)."""
+    def transient_probes(self, y0, dt, steps, substeps=1, drive=None, g=None, probes=(), y_final=None):
+        """As transient, recording `probes` per frame; returns (series[steps+1, P], y_final).
+        `y_final`, if given, is a caller-owned contiguous float32 array of n_dof
+        values that receives the final state (page-locked memory makes the
+        download a direct DMA)."""
         y0 = _f32(y0)
         self._check_len("state", y0)
         kind, dof, vec = self._drive(drive)
@@ -180,7 +183,13 @@ class GpuOperator:
                 raise ValueError("wrong number of waveform samples")
         pr = np.ascontiguousarray(probes, dtype=np.int64)
         series = np.empty((steps + 1) * max(pr.size, 1), dtype=np.float32)
-        yf = np.empty(self._n, dtype=np.float32)
+        if y_final is None:
+            yf = np.empty(self._n, dtype=np.float32)
+        else:
+            yf = y_final
+            if not (isinstance(yf, np.ndarray) and yf.dtype == np.float32 and yf.flags.c_contiguous
+                    and yf.size == self._n):
+                raise ValueError(f"y_final must be a contiguous float32 array of {self._n} values")
         check(lib.dgtd_transient_probes(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
                                         nat.ptr(gs), nat.ptr(pr) if pr.size else None, pr.size,
                                         series.ctypes.data, yf.ctypes.data))

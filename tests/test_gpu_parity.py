@@ -161,6 +161,23 @@ def test_transient_probes(ctx):
     traj = gop.transient(y0, dt, 10, 1, record=True)
     assert np.array_equal(series, traj[:, probes])
     assert np.array_equal(yf, traj[-1])
+    # a caller-owned output array receives the same final state
+    out = np.full(gop.n_dof(), np.nan, dtype=np.float32)
+    series2, yf2 = gop.transient_probes(y0, dt, 10, 1, probes=probes, y_final=out)
+    assert yf2 is out and np.array_equal(out, yf) and np.array_equal(series2, series)
+    with pytest.raises(ValueError):
+        gop.transient_probes(y0, dt, 1, 1, probes=probes, y_final=np.empty(3, dtype=np.float32))
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
+def test_state_layout_round_trip(ctx, order):
+    # AoS -> device SoA -> AoS is the identity, including a final chunk of
+    # fewer elements than the conversion kernel stages at once (162 = 8*20 + 2).
+    prod = O.MaxwellOperator(O.structured_box(3, 3, 3), order, 1.0)
+    gop = G.GpuOperator(ctx, prod)
+    y = _y(gop.n_dof()).astype(np.float32)
+    gop.upload(y)
+    assert np.array_equal(gop.download(), y)
 
 
 def test_expmv_matches_oracle(ctx):
