@@ -1940,6 +1940,29 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
   return to_aos<float, float>(op, ya, d_y_out);
 }
 
+// ------------------------------------------------------------------ bounded-wait test hook
+
+extern "C" int dgtd_debug_wait_timeout(dgtd_ctx* ctx, int64_t max_polls, double seconds, double* waited_s) {
+  if (!ctx || max_polls < 1 || max_polls > 0xffffffffLL || !(seconds > 0.0 && seconds <= 10.0))
+    return set_error(DGTD_ERR_BAD_ARG, "debug_wait_timeout: 1 <= max_polls < 2^32 and 0 < seconds <= 10");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  DevBuf<int> d_err;
+  DevBuf<unsigned long long> d_ns;
+  DGTD_TRY(d_err.alloc(1));
+  DGTD_TRY(d_ns.alloc(1));
+  CUDA_TRY(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
+  k_tc_wait_probe<<<1, 32, 0, ctx->stream>>>((uint32_t)max_polls, (uint64_t)(seconds * 1e9), d_err.p, d_ns.p);
+  CUDA_TRY(cudaGetLastError());
+  int h_err = 0;
+  unsigned long long h_ns = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h_err, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(&h_ns, d_ns.p, sizeof(h_ns), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (waited_s) *waited_s = (double)h_ns * 1e-9;
+  if (h_err) return set_error(DGTD_ERR_TIMEOUT, "debug_wait_timeout: the bounded wait gave up (as it should)");
+  return DGTD_OK;
+}
+
 // ------------------------------------------------------------------ tensor-core self test
 
 extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b, float* c, int32_t n, int32_t k,

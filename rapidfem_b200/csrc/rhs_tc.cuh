@@ -141,13 +141,24 @@ struct TcTables {
 // Row of (element le, component c) in the 128-row MMA tile.
 __device__ __forceinline__ int tc_row(int le, int c) { return (le / 5) * 32 + (le % 5) * 6 + c; }
 
-// Bounded waits.  A wait gives up after kTcWaitLimit polls or once another
-// role has raised the abort flag; the warp form is warp-uniform.
+// Bounded waits.  A wait gives up after `limit` polls, after `ns` nanoseconds
+// of the global timer (read only once 256 polls have failed, so waits that
+// complete quickly never touch it: a poll's suspension time is the hardware's
+// choice, so a poll count alone bounds no wall time), or once another role has
+// raised the abort flag; the warp form is warp-uniform.
+constexpr uint64_t kTcWaitNs = 2000000000ull;  // 2 s
+__device__ __forceinline__ uint64_t tc_globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 #ifdef DGTD_TC_PHASE_TIMERS
 __device__ unsigned long long g_tc_polls[3];
 #endif
-__device__ __forceinline__ bool tc_wait1(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t i = 0; i < kTcWaitLimit; ++i) {
+__device__ __forceinline__ bool tc_wait1(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                         uint32_t limit = kTcWaitLimit, uint64_t ns = kTcWaitNs) {
+  uint64_t t0 = 0;
+  for (uint32_t i = 0; i < limit; ++i) {
     if (tc::mbar_try_wait(bar, parity)) {
 #ifdef DGTD_TC_PHASE_TIMERS
       const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -156,13 +167,38 @@ __device__ __forceinline__ bool tc_wait1(uint64_t* bar, uint32_t parity, volatil
 #endif
       return true;
     }
-    if ((i & 255u) == 255u && *abort_flag) return false;
+    if ((i & 255u) == 255u) {
+      if (*abort_flag) return false;
+      const uint64_t now = tc_globaltimer_ns();
+      if (i == 255u)
+        t0 = now;
+      else if (now - t0 > ns)
+        return false;
+    }
   }
   return false;
 }
 __device__ __forceinline__ bool tc_waitw(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
   const bool ok = tc_wait1(bar, parity, abort_flag);
   return __all_sync(0xffffffffu, ok);
+}
+
+// Test hook for the bounded wait: one thread waits, with the kernels' own
+// helper, on an mbarrier that expects one arrival that never comes.  It gives
+// up after `limit` polls or `ns` nanoseconds, records the time it waited and
+// raises `err` as a stage kernel does; nothing faults and the context stays
+// usable.
+__global__ void k_tc_wait_probe(uint32_t limit, uint64_t ns, int* err, unsigned long long* waited_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_abort;
+  if (threadIdx.x != 0) return;
+  tc::mbar_init(&bar, 1);
+  tc::mbar_fence_init();
+  s_abort = 0;
+  const uint64_t t0 = tc_globaltimer_ns();
+  const bool ok = tc_wait1(&bar, 0u, &s_abort, limit, ns);
+  *waited_ns = (unsigned long long)(tc_globaltimer_ns() - t0);
+  if (!ok) atomicExch(err, 1);
 }
 
 template <int N, int MODE>
