@@ -307,12 +307,12 @@ int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
 int dgtd_debug_tc_gemm(dgtd_ctx *ctx, const float *a, const float *b, float *c, int32_t n, int32_t k,
                        int32_t flags);
 /* The bounded wait of the tensor-core kernels, run by one thread on an
- * mbarrier that nothing arrives on: it gives up after max_polls polls or
- * `seconds` (<= 10) of wall time, whichever comes first, and the call returns
+ * mbarrier that nothing arrives on: it gives up after max_polls polls
+ * (1 <= max_polls <= 2^19, the kernels' own limit; a failed poll suspends
+ * about 4 us, so the kernels' limit is about 2 s), and the call returns
  * DGTD_ERR_TIMEOUT through the same device flag a stage kernel raises, with
- * the time waited in *waited_s.  Nothing faults; the context stays usable.
- * The stage kernels' own limit is 2^24 polls or 2 s per wait. */
-int dgtd_debug_wait_timeout(dgtd_ctx *ctx, int64_t max_polls, double seconds, double *waited_s);
+ * the time waited in *waited_s.  Nothing faults; the context stays usable. */
+int dgtd_debug_wait_timeout(dgtd_ctx *ctx, int64_t max_polls, double *waited_s);
 /* Per-phase cycle counters of the tensor-core RHS kernel (8 u64 in device
  * memory, accumulated by thread 0 of every CTA); recorded only by builds
  * compiled with -DDGTD_TC_PHASE_TIMERS, ignored otherwise.  NULL detaches. */

@@ -130,7 +130,7 @@ _sig("dgtd_op_launch_count", C.c_int, _vp, C.POINTER(_i64))
 _sig("dgtd_op_reset_launch_count", C.c_int, _vp)
 _sig("dgtd_debug_expm", C.c_int, _vp, _pd, _i32, _pd)
 _sig("dgtd_debug_tc_gemm", C.c_int, _vp, _pf, _pf, _pf, _i32, _i32, _i32)
-_sig("dgtd_debug_wait_timeout", C.c_int, _vp, _i64, _f64, C.POINTER(_f64))
+_sig("dgtd_debug_wait_timeout", C.c_int, _vp, _i64, C.POINTER(_f64))
 _sig("dgtd_cfl_dt", C.c_int, _vp, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_f64))
 _sig("dgtd_power_rho", C.c_int, _vp, _i32, C.POINTER(_f64))
 _sig("dgtd_field_energy", C.c_int, _vp, _pd, C.POINTER(_f64))

@@ -1942,16 +1942,16 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
 
 // ------------------------------------------------------------------ bounded-wait test hook
 
-extern "C" int dgtd_debug_wait_timeout(dgtd_ctx* ctx, int64_t max_polls, double seconds, double* waited_s) {
-  if (!ctx || max_polls < 1 || max_polls > 0xffffffffLL || !(seconds > 0.0 && seconds <= 10.0))
-    return set_error(DGTD_ERR_BAD_ARG, "debug_wait_timeout: 1 <= max_polls < 2^32 and 0 < seconds <= 10");
+extern "C" int dgtd_debug_wait_timeout(dgtd_ctx* ctx, int64_t max_polls, double* waited_s) {
+  if (!ctx || max_polls < 1 || max_polls > (int64_t)kTcWaitLimit)
+    return set_error(DGTD_ERR_BAD_ARG, "debug_wait_timeout: 1 <= max_polls <= the kernels' own limit (2^19)");
   CUDA_TRY(cudaSetDevice(ctx->device));
   DevBuf<int> d_err;
   DevBuf<unsigned long long> d_ns;
   DGTD_TRY(d_err.alloc(1));
   DGTD_TRY(d_ns.alloc(1));
   CUDA_TRY(cudaMemsetAsync(d_err.p, 0, sizeof(int), ctx->stream));
-  k_tc_wait_probe<<<1, 32, 0, ctx->stream>>>((uint32_t)max_polls, (uint64_t)(seconds * 1e9), d_err.p, d_ns.p);
+  k_tc_wait_probe<<<1, 32, 0, ctx->stream>>>((uint32_t)max_polls, d_err.p, d_ns.p);
   CUDA_TRY(cudaGetLastError());
   int h_err = 0;
   unsigned long long h_ns = 0;

@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
     tc::mma_commit(&s_bar);
   }
   __syncwarp();
-  const bool ok = tc::mbar_wait(&s_bar, 0, 1u << 24);
+  const bool ok = tc::mbar_wait(&s_bar, 0, 1u << 19);  // about 2 s (a failed poll suspends ~4 us)
   if (!ok && lane == 0) atomicExch(err, 1);
   tc::tc_fence_after();
   if (ok) {

@@ -176,6 +176,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait: returns false if the phase did not complete within `limit` polls.
+// A poll that finds the phase incomplete suspends the thread until the phase
+// completes or a hardware time limit passes (about 4 us on B200), so `limit`
+// also bounds the wall time: 2^19 polls is about 2 s.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
   for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;

@@ -55,12 +55,13 @@ class GpuContext:
         check(lib.dgtd_debug_expm(self._h, a.ravel(), a.shape[0], out.ravel()))
         return out
 
-    def wait_timeout_probe(self, max_polls: int, seconds: float) -> float:
+    def wait_timeout_probe(self, max_polls: int) -> float:
         """Run the kernels' bounded wait on a barrier nothing arrives on
         (dgtd_debug_wait_timeout); raises DgtdError (TIMEOUT) once it gives
-        up, with the seconds waited as `waited_s` on the exception."""
+        up after `max_polls` polls, with the seconds waited as `waited_s` on
+        the exception."""
         waited = C.c_double(0.0)
-        st = lib.dgtd_debug_wait_timeout(self._h, int(max_polls), float(seconds), C.byref(waited))
+        st = lib.dgtd_debug_wait_timeout(self._h, int(max_polls), C.byref(waited))
         try:
             check(st)
         except nat.DgtdError as e:
