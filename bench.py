@@ -413,6 +413,71 @@ def run_c4(args):
     return 0
 
 
+def run_c2_accuracy(args):
+    """Accuracy of the f32-class engines over the C2 run length: the
+    sphere_pulse workload, LSERK4 at dt = 0.5 * 2.8 / rho (the bench's rule),
+    `--acc-steps` steps (2000 by default) on the FP32 and the tensor-core
+    engines.  At `--acc-cells`^3 (16 by default) both final states are compared
+    with the f64 oracle run from the same f32 initial state on the host's
+    cores; at the full 48^3 size (139 M DOFs, where the f64 oracle would take
+    hours) the two engines are compared with each other."""
+    import ctypes as C
+
+    import torch
+
+    from oracle import oracle as R
+    from rapidfem_b200 import _native as nat
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    steps = args.acc_steps
+    ctx = G.GpuContext(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    out = {}
+    for cells in (args.acc_cells, args.cells):
+        wl = W.sphere_pulse(cells, 4)
+        op = wl.build()
+        gop = G.GpuOperator(ctx, op)
+        y0 = wl.y0(op).astype(np.float32)
+        rho = C.c_double()
+        nat.check(nat.lib.dgtd_power_rho(gop.handle, 40, C.byref(rho)))
+        dt = 0.5 * 2.8 / rho.value
+        finals, secs = {}, {}
+        for name, eng in (("fp32", 0), ("tf32x3", 1)):
+            gop.set_engine(eng)
+            gop.upload(y0)
+            t0 = time.perf_counter()
+            gop.run_lserk(dt, steps)
+            ctx.synchronize()
+            secs[name] = time.perf_counter() - t0
+            finals[name] = gop.download().astype(np.float64)
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        rec = {"n_dof": int(gop.n_dof()), "dt": dt, "steps": steps, "gpu_seconds": secs,
+               "tf32x3_vs_fp32": rel(finals["tf32x3"], finals["fp32"])}
+        if cells == args.acc_cells:
+            orc = R.Operator(wl.mesh.nodes, wl.mesh.tets, 4, 1.0, materials=wl.materials)
+            t0 = time.perf_counter()
+            ref = orc.lserk(y0.astype(np.float64), dt, steps)
+            rec["oracle_seconds"] = time.perf_counter() - t0
+            rec["oracle_threads"] = R.threads()
+            rec["fp32_vs_f64"] = rel(finals["fp32"], ref)
+            rec["tf32x3_vs_f64"] = rel(finals["tf32x3"], ref)
+        out[f"{cells}^3"] = rec
+        del gop
+    small = out[f"{args.acc_cells}^3"]
+    line = {"metric": "relative L2 error after the C2 run length vs f64", "value": small["tf32x3_vs_f64"],
+            "unit": "relative L2", "n_gpus": 1, "higher_is_better": False, "dtype": "f32 / tf32x3",
+            "data": "synthetic", "config": {"workload": "sphere_pulse (jittered box, N=4, eps_r=4 sphere, "
+                                                        "Gaussian Ez pulse), LSERK4", "runs": out}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_time_to_t(args):
     """Time to reach T at <= 1e-4 relative L2 against the FP64 oracle: plain FP32
     LSERK4 on the GPU vs the tensor-core LSERK4 and the adaptive / learned ETD
@@ -645,7 +710,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-cells", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t"],
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t", "c2-accuracy"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
                          "c5: the waveguide post variants with port probes; "
                          "time-to-t: LSERK4 vs adaptive / learned ETD to a final time against the oracle")
@@ -653,6 +718,8 @@ def main():
     ap.add_argument("--c5-cells", type=int, nargs=3, default=[39, 17, 101])
     ap.add_argument("--c5-steps", type=int, default=0, help="0: long enough for the pulse to cross the guide")
     ap.add_argument("--ttt-cells", type=int, default=12)
+    ap.add_argument("--acc-cells", type=int, default=16)
+    ap.add_argument("--acc-steps", type=int, default=2000)
     ap.add_argument("--ttt-time", type=float, default=0.5)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--graph-steps", type=int, default=10)
@@ -664,6 +731,8 @@ def main():
         return run_c4(args)
     if args.workload == "time-to-t":
         return run_time_to_t(args)
+    if args.workload == "c2-accuracy":
+        return run_c2_accuracy(args)
     if args.workload == "c5":
         return run_c5(args)
     return run_b200(args)
