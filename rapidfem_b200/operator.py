@@ -109,7 +109,7 @@ class MaxwellOperator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:  # lib is None at interpreter shutdown
             lib.dgtd_host_op_destroy(h)
             self._h = C.c_void_p()
 
