@@ -16,8 +16,8 @@ LearnedEtd asks a small MLP (16 -> 64 -> 64 -> 2, trained on traces the plain
 controller logged) for the next step size and Krylov cap from the history of
 the last four accepted steps; the proposed step is never below the plain
 controller's own next step, it is tried and kept only if its estimate passes,
-otherwise the plain controller decides the step (and remains the judge of its
-error).  The training target of a logged step is what its
+otherwise the plain controller decides the step (and its estimate alone decides
+acceptance).  The training target of a logged step is what its
 run says in hindsight: the largest step the plain controller itself took
 within the next LOOKAHEAD accepted steps (a step size it reached and passed
 from a similar state), relative to the previous step, and that step's Krylov
