@@ -310,7 +310,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     // Out-of-tile neighbour traces of this thread's slots in half hh (global
     // loads, zero where the neighbour is in the tile or absent).  They are
     // issued a phase ahead of their use: half 0's before the volume operand is
-    // formed, half 1's before half 0's fluxes, so their latency is hidden.
+    // formed, half 1's right after it (before half 0's fluxes), so their
+    // latency is hidden.
     const auto nb_fetch = [&](const float* sM, int64_t e0, int hh, float (&nb)[2][6]) {
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
@@ -374,6 +375,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       // ---- numerical flux (rhs.rs:1370-1441) by halves of the LIFT operand:
       // faces 0-1, then 2-3.  A half is free once the previous tile's MMAs of
       // that half are done; its own MMAs then run while the next half is formed.
+      // half 1's traces: before the wait for half 0's operand to be free
+      nb_fetch(sM, e0, 1, nb_h[1]);
       bool half_ok = true;
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
@@ -386,7 +389,6 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           }
         }
         DGTD_TC_MARK(2);
-        if (hh == 0) nb_fetch(sM, e0, 1, nb_h[1]);
         {
           const float (&nb)[2][6] = nb_h[hh];
 #pragma unroll
