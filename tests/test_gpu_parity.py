@@ -224,3 +224,63 @@ def test_bad_arguments_raise(ctx):
     with pytest.raises(DgtdError):
         gop.transient(np.zeros(gop.n_dof()), -1.0, 2)
     assert gop.launch_count() >= 0
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+def test_single_cell_mesh_one_padded_tile(ctx, order, engine):
+    # 6 tets: fewer elements than one tile of either kernel, so most of the tile
+    # is inert padding; every face of the cube is a PEC boundary face
+    prod, orc = _pair(O.structured_box(1, 1, 1), order)
+    gop = G.GpuOperator(ctx, prod)
+    gop.set_engine(engine)
+    y32 = _y(gop.n_dof()).astype(np.float32)
+    assert rel_l2(gop.apply(y32), orc.apply(y32.astype(np.float64))) < RHS_TOL
+    dt = 0.5 / _rho(orc)
+    got = gop.transient(y32, dt, 5)
+    want = orc.lserk(y32.astype(np.float64), dt, 5)
+    assert rel_l2(got, want) < RUN_TOL
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+def test_zero_steps_and_empty_probe_list(ctx, engine):
+    prod, orc = _pair(O.structured_box(2, 2, 2), 3)
+    gop = G.GpuOperator(ctx, prod)
+    gop.set_engine(engine)
+    y32 = _y(gop.n_dof()).astype(np.float32)
+    dt = 0.5 / _rho(orc)
+    # no steps: the final state is the initial one, the record is one frame
+    assert np.array_equal(gop.transient(y32, dt, 0), y32)
+    traj = gop.transient(y32, dt, 0, record=True)
+    assert traj.shape == (1, gop.n_dof()) and np.array_equal(traj[0], y32)
+    # no probes: an empty series and the same final state as a plain transient
+    series, yf = gop.transient_probes(y32, dt, 4, 1, probes=())
+    assert series.shape == (5, 0)
+    assert np.array_equal(yf, gop.transient(y32, dt, 4))
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+def test_zero_state_has_zero_rhs(ctx, engine):
+    prod, _ = _pair(O.structured_box(3, 3, 3), 4)
+    gop = G.GpuOperator(ctx, prod)
+    gop.set_engine(engine)
+    assert not np.any(gop.apply(np.zeros(gop.n_dof(), dtype=np.float32)))
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+def test_rhs_linearity_at_size(ctx, engine):
+    # a property that needs no oracle, at a size the oracle would be slow on:
+    # A(a x + b z) = a A x + b A z to f32 rounding (16^3 x 6 tets, 5.2 M DOFs)
+    from rapidfem_b200 import workloads as W
+
+    wl = W.sphere_pulse(16, 4)
+    gop = G.GpuOperator(ctx, wl.build())
+    gop.set_engine(engine)
+    n = gop.n_dof()
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n).astype(np.float32)
+    z = rng.standard_normal(n).astype(np.float32)
+    a, b = np.float32(0.75), np.float32(-1.25)
+    lhs = gop.apply((a * x + b * z).astype(np.float32)).astype(np.float64)
+    rhs = a * gop.apply(x).astype(np.float64) + b * gop.apply(z).astype(np.float64)
+    assert rel_l2(lhs, rhs) < 1e-5
