@@ -1467,12 +1467,12 @@ int ensure_krylov(dgtd_op* op, int m) {
   DGTD_TRY(op->skip.alloc(1));
   DGTD_TRY(op->vin64.alloc(op->n_dof));
   DGTD_TRY(op->tmp64.alloc(op->n_dof));
-  static bool attr = false;
-  if (!attr) {
+  static bool attr[8] = {false};  // kernel attributes are per device
+  if (!attr[op->ctx->device & 7]) {
     CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
     CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
     CUDA_TRY(cudaFuncSetAttribute(dgtd::k_expm_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
-    attr = true;
+    attr[op->ctx->device & 7] = true;
   }
   return DGTD_OK;
 }
@@ -1829,10 +1829,10 @@ static int energy_of(dgtd_op* op, const T* y_soa, double* energy) {
   if (!op->has_mass) return set_error(DGTD_ERR_UNSUPPORTED, "energy: operator created without the mass matrix");
   DGTD_TRY(op->partials.alloc((size_t)dgtd::kKrylovBlocks * dgtd::kKrylovMaxDim));
   const size_t sm = (size_t)op->np * op->np * 8;
-  static bool attr = false;
-  if (!attr) {
+  static bool attr[8] = {false};  // kernel attributes are per device
+  if (!attr[op->ctx->device & 7]) {
     CUDA_TRY(cudaFuncSetAttribute(k_energy<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    attr = true;
+    attr[op->ctx->device & 7] = true;
   }
   k_energy<T><<<kRedBlocks, 256, sm, op->stream()>>>(y_soa, op->mass.p, op->absdet.p, op->meta.p, op->n_elem,
                                                      op->np, op->partials.p);

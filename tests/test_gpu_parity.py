@@ -284,3 +284,38 @@ def test_rhs_linearity_at_size(ctx, engine):
     lhs = gop.apply((a * x + b * z).astype(np.float32)).astype(np.float64)
     rhs = a * gop.apply(x).astype(np.float64) + b * gop.apply(z).astype(np.float64)
     assert rel_l2(lhs, rhs) < 1e-5
+
+
+def test_cfl_dt_matches_oracle(ctx):
+    # session.rs:514-569: 40 power iterations from the same seeded start vector,
+    # then a bisection of the LSERK4 stability point z; h = 0.8 z / rho
+    import ctypes as C
+
+    from rapidfem_b200 import _native as nat
+
+    prod, orc = _pair(O.structured_box(3, 3, 3), 3)
+    gop = G.GpuOperator(ctx, prod)
+    h, rho, z = C.c_double(), C.c_double(), C.c_double()
+    nat.check(nat.lib.dgtd_cfl_dt(gop.handle, C.byref(h), C.byref(rho), C.byref(z)))
+    z_ref, rho_ref = orc.cfl_z()
+    assert abs(rho.value - rho_ref) < 1e-4 * rho_ref
+    assert abs(z.value - z_ref) < 0.25  # within two steps of the bisection's final bracket
+    assert abs(h.value - 0.8 * z.value / rho.value) < 1e-12 * h.value + 1e-15
+
+
+def test_field_energy_matches_oracle(ctx):
+    import ctypes as C
+
+    from rapidfem_b200 import _native as nat
+
+    m = O.structured_box_jittered(3, 3, 3, 1.0, 1.0, 1.0, 0.1, 5)
+    K = m.n_tets
+    rng = np.random.default_rng(2)
+    mat = O.isotropic_materials(rng.uniform(1, 4, K), rng.uniform(1, 2, K))
+    prod, orc = _pair(m, 3, materials=mat)
+    gop = G.GpuOperator(ctx, prod)
+    y = _y(gop.n_dof())
+    e = C.c_double()
+    nat.check(nat.lib.dgtd_field_energy(gop.handle, np.ascontiguousarray(y, dtype=np.float64), C.byref(e)))
+    want = orc.field_energy(y)
+    assert abs(e.value - want) < 1e-6 * abs(want)
