@@ -484,7 +484,8 @@ def run_time_to_t(args):
     integrators, on the stiff graded-slab case (the grid graded 20:1 toward
     z = 0, N = 3, a lossy slab z < 0.2 with eps_r 2.2 and sigma 5), free
     evolution of a Gaussian E_z pulse.  The headline value is the learned ETD
-    time; the ratio to the plain FP32 LSERK4 time is in `config.methods`."""
+    time; the ratio to the plain FP32 LSERK4 time is in `config.methods`, next
+    to the reference's adaptive method (device KCL RK4(3)5, default controller)."""
     import ctypes as C
 
     import torch
@@ -548,6 +549,18 @@ def run_time_to_t(args):
         stream.synchronize()
         methods[name] = {"seconds": e0.elapsed_time(e1) * 1e-3, "rel_l2": rel(gop.download()), "steps": steps,
                          "matvecs": 5 * steps, "dt": dt}
+    # the reference's adaptive method: KCL RK4(3)5 with the default PI controller
+    # (session.rs:130-158) on the device, one output frame of length T
+    for name, eng in (("kcl_fp32", nat.ENGINE_FP32), ("kcl_tf32x3", nat.ENGINE_TF32X3)):
+        gop.set_engine(eng)
+        gop.transient_kcl(y0, T, 1, record=False)  # warm
+        w = time.perf_counter()
+        yk, kst = gop.transient_kcl(y0, T, 1, record=False)
+        secs = time.perf_counter() - w
+        attempts = int(kst["accepted"] + kst["rejected"])
+        methods[name] = {"seconds": secs, "rel_l2": rel(yk), "steps": int(kst["accepted"]),
+                         "rejected": int(kst["rejected"]), "matvecs": 5 * attempts,
+                         "h_min": float(kst["h_min"]), "h_max": float(kst["h_max"])}
     gop.set_engine(nat.ENGINE_FP32)
     plain = E.PlainEtd(tol=1e-7, m_max=48)
     logs = []
