@@ -312,11 +312,15 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     // issued a phase ahead of their use: half 0's before the volume operand is
     // formed, half 1's right after it (before half 0's fluxes), so their
     // latency is hidden.
-    const auto nb_fetch = [&](const float* sM, int64_t e0, int hh, float (&nb)[2][6]) {
+    // It also leaves, per slot, where the flux finds the neighbour trace:
+    // zi >= 0 its offset in the tile's shared state, -1 the fetched registers,
+    // -2 a PEC face, -3 a port face.
+    const auto nb_fetch = [&](const float* sM, int64_t e0, int hh, float (&nb)[2][6], int (&zi)[2]) {
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) nb[u][c] = 0.f;
+        zi[u] = -2;
         if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
         const int x = f_item[hh][u];
         const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & 15;
@@ -324,10 +328,20 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
         const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
         const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
         const int nbr = __float_as_int(Me[37 + f]);
-        if (((code >> 8) & 3) == kInterior && (uint32_t)(nbr - (int)e0) >= (uint32_t)E) {
-          const float* Z = P.y_in + (int64_t)nbr * (6 * NP) + sG[(code & 0xff) * NFP + m];
+        const int kind = (code >> 8) & 3;
+        const int gofs = sG[(code & 0xff) * NFP + m];
+        const int lo = nbr - (int)e0;  // element ids fit in int
+        if (kind == kInterior) {
+          if ((uint32_t)lo < (uint32_t)E) {
+            zi[u] = lo * 6 * NP + gofs;
+          } else {
+            zi[u] = -1;
+            const float* Z = P.y_in + (int64_t)nbr * (6 * NP) + gofs;
 #pragma unroll
-          for (int c = 0; c < 6; ++c) nb[u][c] = __ldg(Z + c * NP);
+            for (int c = 0; c < 6; ++c) nb[u][c] = __ldg(Z + c * NP);
+          }
+        } else {
+          zi[u] = kind == kPort ? -3 : -2;
         }
       }
     };
@@ -341,7 +355,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       bool ok = tc_waitw(&bar_ld[ys], (ld_par >> ys) & 1u, abort_flag);
       ld_par ^= 1u << ys;
       float nb_h[2][2][6];
-      if (ok) nb_fetch(sM, e0, 0, nb_h[0]);
+      int zi_h[2][2];
+      if (ok) nb_fetch(sM, e0, 0, nb_h[0], zi_h[0]);
       if (ok && it > 0) ok = tc_waitw(&bar_vdone, (uint32_t)((it - 1) & 1), abort_flag);
       if (!ok) {
         *abort_flag = 1;
@@ -376,7 +391,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       // faces 0-1, then 2-3.  A half is free once the previous tile's MMAs of
       // that half are done; its own MMAs then run while the next half is formed.
       // half 1's traces: before the wait for half 0's operand to be free
-      nb_fetch(sM, e0, 1, nb_h[1]);
+      nb_fetch(sM, e0, 1, nb_h[1], zi_h[1]);
       bool half_ok = true;
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
@@ -400,19 +415,17 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             const float* Me = sM + le * kMetaWords;
             const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
             const float coef = 0.5f * Me[21 + f];
-            const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
-            const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
-            const int kind = (code >> 8) & 3;
+            const int zi = zi_h[hh][u];
             const float* Y = sY + (x >> 11);
             const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
             const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
             float jex, jey, jez, jhx, jhy, jhz;
             float a = P.alpha;
-            if (kind == kPort) {
+            if (zi == -3) {
               // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
               jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
               a = 1.0f;
-            } else if (kind == kPec) {
+            } else if (zi == -2) {
               // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
               const float edn = nx * ex + ny * ey + nz * ez;
               const float hdn = nx * hx + ny * hy + nz * hz;
@@ -421,9 +434,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             } else {
               float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
               float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
-              const int lo = __float_as_int(Me[37 + f]) - (int)e0;  // element ids fit in int
-              if ((uint32_t)lo < (uint32_t)E) {
-                const float* Z = sY + lo * 6 * NP + sG[(code & 0xff) * NFP + m];
+              if (zi >= 0) {
+                const float* Z = sY + zi;
                 px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
                 qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
               }
