@@ -281,7 +281,7 @@ def run_b200(args):
                 "api": "GpuOperator.transient_probes (dgtd_transient_probes): y0 in, probe series + final state out"},
         "finite": finite,
     }
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline is an N = 1 figure
         rate, info = cpu_reference_rate(args.cpu_steps, 1, n_cells=args.ref_cells)
         line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": info["cores"], "kind": "port",
                                 "sample": info["sample"]}
@@ -400,7 +400,7 @@ def run_c4(args):
                 "api": "GpuOperator.load_device/store_device + BatchRunner.run (graph replays)"},
         "finite": finite,
     }
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline is an N = 1 figure
         rate, info = cpu_batch_rate(inst, groups)
         line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": info["cores"], "kind": "port",
                                 "sample": info["sample"]}
