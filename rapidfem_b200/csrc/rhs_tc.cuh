@@ -68,7 +68,6 @@ static_assert(kTcFluxWarps % 4 == 0 && kTcEpiWarps % 4 == 0, "roles cover whole 
 
 __host__ __device__ constexpr int tc_r8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int tc_r16(int x) { return (x + 15) & ~15; }
-__host__ __device__ constexpr int tc_r32(int x) { return (x + 31) & ~31; }
 __host__ __device__ constexpr int tc_r128(int x) { return (x + 127) & ~127; }
 
 template <int N>
