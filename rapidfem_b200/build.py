@@ -64,11 +64,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
-        cmd = [nvcc, *common, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc, *common, "-Xcompiler", "-fopenmp", "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj]
         _run(cmd, verbose)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], verbose)
+    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lgomp"], verbose)
     os.replace(tmp, LIB)
     return LIB
 

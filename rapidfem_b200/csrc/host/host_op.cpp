@@ -8,13 +8,13 @@
 //   rapidfem-core topology.rs:50-91 + mesh.rs:45-50, rhs.rs:805-1000,
 //   rhs.rs:1030-1066, rhs.rs:1157-1199, waveguide.rs:39-145.
 #include <algorithm>
+#include <parallel/algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <limits>
 #include <string>
-#include <unordered_map>
 #include <vector>
 
 #include "../../../include/dgtd_host.h"
@@ -255,6 +255,10 @@ struct Operator {
     for (int64_t i = 0; i < 4 * K; ++i)
       if (tets[i] < 0 || tets[i] >= n_nodes) return "tet vertex id out of range";
     origin.resize(3 * K); jac.resize(9 * K); jinv.resize(9 * K); det.resize(K);
+    // The element and face loops below write only their own element's entries,
+    // so they run on all host threads with results identical to a serial run.
+    bool degenerate = false;
+#pragma omp parallel for schedule(static) reduction(|| : degenerate)
     for (int64_t e = 0; e < K; ++e) {
       const double* v[4];
       for (int q = 0; q < 4; ++q) v[q] = nodes + 3 * size_t(tets[4 * e + q]);
@@ -263,7 +267,10 @@ struct Operator {
         for (int k = 0; k < 3; ++k) m[i][k] = v[k + 1][i] - v[0][i];
       V3 adj[3] = {cross(m[1], m[2]), cross(m[2], m[0]), cross(m[0], m[1])};
       const double d = dot(m[0], adj[0]);
-      if (d == 0.0 || !std::isfinite(d)) return "degenerate tetrahedron";
+      if (d == 0.0 || !std::isfinite(d)) {
+        degenerate = true;
+        continue;
+      }
       const double id = 1.0 / d;
       for (int i = 0; i < 3; ++i) {
         origin[3 * e + i] = v[0][i];
@@ -274,19 +281,28 @@ struct Operator {
       }
       det[e] = d;
     }
+    if (degenerate) return "degenerate tetrahedron";
     // Face topology (topology.rs:50-91) with neighbours from shared vertex sets.
     normal.resize(12 * K); fscale.resize(4 * K);
     nbr.assign(4 * K, -1); nbr_lf.assign(4 * K, -1); port.assign(4 * K, -1);
     perm.assign(size_t(4) * K * nfp, 0);
     std::vector<double> area(4 * K);
-    struct Key { int64_t a, b, c; bool operator==(const Key& o) const { return a == o.a && b == o.b && c == o.c; } };
-    struct KeyHash { size_t operator()(const Key& k) const {
-      uint64_t h = uint64_t(k.a) * 0x9E3779B97F4A7C15ULL;
-      h ^= uint64_t(k.b) + 0x7F4A7C15ULL + (h << 6) + (h >> 2);
-      h ^= uint64_t(k.c) + 0x94D049BBULL + (h << 6) + (h >> 2);
-      return size_t(h); } };
-    std::unordered_map<Key, std::array<int64_t, 2>, KeyHash> faces;
-    faces.reserve(size_t(2.5 * K) + 16);
+    // Faces are matched by their sorted vertex triples: the 4K records are
+    // sorted (in parallel) by (triple, face id) and equal neighbours paired.
+    // For a triple shared by more than two tets the two lowest face ids, i.e.
+    // the first two tets in element order, are kept.
+    struct FaceRec {
+      int64_t a, b, c, id;
+    };
+    std::vector<FaceRec> fr(size_t(4) * K);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < K; ++e)
+      for (int lf = 0; lf < 4; ++lf) {
+        int64_t t3[3] = {tets[4 * e + kFaceLocal[lf][0]], tets[4 * e + kFaceLocal[lf][1]], tets[4 * e + kFaceLocal[lf][2]]};
+        std::sort(t3, t3 + 3);
+        fr[4 * e + lf] = FaceRec{t3[0], t3[1], t3[2], 4 * e + lf};
+      }
+#pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < K; ++e)
       for (int lf = 0; lf < 4; ++lf) {
         auto P = [&](int loc) { const double* p = nodes + 3 * size_t(tets[4 * e + loc]); return V3{p[0], p[1], p[2]}; };
@@ -299,21 +315,30 @@ struct Operator {
         if (dot({vo[0] - v0[0], vo[1] - v0[1], vo[2] - v0[2]}, n) > 0.0)
           for (int k = 0; k < 3; ++k) n[k] = -n[k];
         for (int k = 0; k < 3; ++k) normal[12 * e + 3 * lf + k] = n[k];
-        int64_t t3[3] = {tets[4 * e + kFaceLocal[lf][0]], tets[4 * e + kFaceLocal[lf][1]], tets[4 * e + kFaceLocal[lf][2]]};
-        std::sort(t3, t3 + 3);
-        auto it = faces.find({t3[0], t3[1], t3[2]});
-        if (it == faces.end()) faces.emplace(Key{t3[0], t3[1], t3[2]}, std::array<int64_t, 2>{4 * e + lf, -1});
-        else if (it->second[1] < 0) it->second[1] = 4 * e + lf;  // the first two tets are kept
       }
-    for (auto& kv : faces) {
-      int64_t a = kv.second[0], b = kv.second[1];
-      if (b < 0) continue;
-      nbr[a] = int32_t(b / 4); nbr_lf[a] = int32_t(b % 4);
-      nbr[b] = int32_t(a / 4); nbr_lf[b] = int32_t(a % 4);
+    const auto rec_less = [](const FaceRec& x, const FaceRec& y) {
+      if (x.a != y.a) return x.a < y.a;
+      if (x.b != y.b) return x.b < y.b;
+      if (x.c != y.c) return x.c < y.c;
+      return x.id < y.id;
+    };
+    __gnu_parallel::sort(fr.begin(), fr.end(), rec_less);
+    for (size_t i = 0; i < fr.size();) {
+      size_t j = i + 1;
+      while (j < fr.size() && fr[j].a == fr[i].a && fr[j].b == fr[i].b && fr[j].c == fr[i].c) ++j;
+      if (j - i >= 2) {
+        const int64_t fa = fr[i].id, fb = fr[i + 1].id;
+        nbr[fa] = int32_t(fb / 4); nbr_lf[fa] = int32_t(fb % 4);
+        nbr[fb] = int32_t(fa / 4); nbr_lf[fb] = int32_t(fa % 4);
+      }
+      i = j;
     }
     // fscale, perm (nearest-node match, tol^2 1e-18 absolute), ports.
-    std::vector<V3> here(nfp), there(nfp);
-    for (int64_t e = 0; e < K; ++e)
+    bool unmatched = false;
+    double worst = 0.0;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < K; ++e) {
+      std::array<V3, 21> here, there;  // Nfp <= 21 (order 5)
       for (int f = 0; f < 4; ++f) {
         const int64_t ef = 4 * e + f;
         fscale[ef] = 2.0 * area[ef] / std::fabs(det[e]);
@@ -333,10 +358,18 @@ struct Operator {
                        powi(here[m][2] - there[m2][2], 2);
             if (d < best) { best = d; bm = m2; }
           }
-          if (!(best < 1e-18)) return "unmatched face node (best distance " + std::to_string(std::sqrt(best)) + ")";
+          if (!(best < 1e-18)) {
+#pragma omp critical(dgtd_unmatched)
+            {
+              unmatched = true;
+              if (!(best <= worst)) worst = best;
+            }
+          }
           perm[size_t(ef) * nfp + m] = bm;
         }
       }
+    }
+    if (unmatched) return "unmatched face node (best distance " + std::to_string(std::sqrt(worst)) + ")";
     inv_eps.resize(3 * K); inv_mu.resize(3 * K); sig_e.resize(3 * K); sig_m.resize(3 * K);
     for (int64_t e = 0; e < K; ++e) {
       double eps[3] = {1, 1, 1}, mu[3] = {1, 1, 1}, sg = 0.0, sm = 0.0;
