@@ -131,3 +131,33 @@ def test_gloo_world2_matches_single_domain():
         parts = PT.build_parts(mesh, PT.morton_partition(mesh, 2), face_port=port, materials=mat)
         got = PT.join_state(parts, [np.load(os.path.join(tmp, f"y{r}.npy")) for r in range(2)], orc.np)
     assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("n_parts", [1, 8])
+def test_loopback_one_and_many_parts(n_parts):
+    # one part: no halo and no exchange at all; eight parts of ~27 tets: most
+    # elements sit on a cut, so every part exchanges with several peers
+    mesh, port, mat = _problem()
+    order = 2
+    orc = R.Operator(mesh.nodes, mesh.tets, order, 1.0, face_port=port, materials=mat)
+    y0 = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    h = 0.5 / orc.power_rho(30)[0]
+    want = orc.lserk(y0, h, 3)
+    parts = PT.build_parts(mesh, PT.morton_partition(mesh, n_parts), face_port=port, materials=mat)
+    assert len(parts) == n_parts
+    if n_parts == 1:
+        assert parts[0].halo.size == 0 and not parts[0].send and not parts[0].recv
+    else:
+        assert all(len(p.send) >= 2 for p in parts)
+    engines = [OracleEngine(p, order) for p in parts]
+    for e, yl in zip(engines, PT.split_state(parts, y0, orc.np)):
+        e.load(yl)
+    PT.LoopbackLserk(parts, engines).step(h, 3)
+    got = PT.join_state(parts, [e.state() for e in engines], orc.np)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+def test_partition_rejects_bad_part_count():
+    mesh, _, _ = _problem()
+    with pytest.raises(ValueError):
+        PT.morton_partition(mesh, 0)
