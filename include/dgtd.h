@@ -43,25 +43,29 @@ typedef enum {
 typedef struct dgtd_ctx dgtd_ctx;
 typedef struct dgtd_op dgtd_op;
 
-/* Copy the calling thread's last error message into buf (NUL-terminated). */
+/* Copy the calling thread's last error message into buf (NUL-terminated): the
+ * String the reference returns in its Result<_, String> errors. */
 int dgtd_last_error(char *buf, size_t len);
 
-/* Library / build identification: "rapidfem_b200 <version> sm_100a". */
+/* Library / build identification: "rapidfem_b200 <version> sm_100a" (no
+ * counterpart in the reference). */
 const char *dgtd_version(void);
 
 /* ---- context ----------------------------------------------------------
  * Replaces GpuContext::new (crates/rapidfem-td/src/gpu/mod.rs:49): picks the
  * CUDA device, creates the stream the ops run on. */
 int dgtd_ctx_create(int device, dgtd_ctx **out);
-/* Ops and MLPs made on a context may be destroyed after it (their destructors
- * do not touch the context); any other call on them needs the context alive. */
+/* Releases the context (GpuContext is dropped in the reference).  Ops and MLPs
+ * made on a context may be destroyed after it (their destructors do not touch
+ * the context); any other call on them needs the context alive. */
 int dgtd_ctx_destroy(dgtd_ctx *ctx);
 /* Device name (GpuContext::device_name, gpu/mod.rs:35). */
 int dgtd_ctx_device_name(dgtd_ctx *ctx, char *buf, size_t len);
 /* Run subsequent work of this context's ops on an external cudaStream_t
- * (NULL restores the context's own stream). */
+ * (NULL restores the context's own stream).  No counterpart in the reference,
+ * whose OpenCL queue is private to GpuContext. */
 int dgtd_ctx_set_stream(dgtd_ctx *ctx, void *cuda_stream);
-/* Block until the context's stream is idle. */
+/* Block until the context's stream is idle (no counterpart in the reference). */
 int dgtd_ctx_synchronize(dgtd_ctx *ctx);
 
 /* ---- operator ---------------------------------------------------------
@@ -106,11 +110,13 @@ typedef enum {
 
 /* GpuOperator::new (gpu/operator.rs:207). Uploads the operator once. */
 int dgtd_op_create(dgtd_ctx *ctx, const dgtd_op_desc *desc, dgtd_op **out);
+/* Releases the op (GpuOperator is dropped in the reference). */
 int dgtd_op_destroy(dgtd_op *op);
 /* GpuOperator::n_dof (gpu/operator.rs:430): 6*Np*K. */
 int dgtd_op_n_dof(const dgtd_op *op, int64_t *n_dof);
 /* Select the contraction engine; fails with DGTD_ERR_UNSUPPORTED if this
- * order has no kernel for it. */
+ * order has no kernel for it.  No counterpart in the reference, which has one
+ * OpenCL kernel. */
 int dgtd_op_set_engine(dgtd_op *op, int engine);
 int dgtd_op_get_engine(const dgtd_op *op, int *engine);
 
@@ -160,7 +166,8 @@ int dgtd_transient_functionals(dgtd_op *op, const float *y0, float dt, int64_t s
 int dgtd_lserk_stage(dgtd_op *op, float h, int32_t stage, int drive, int64_t src_dof, float g);
 /* Copy element blocks (6*Np f32 each, element-major SoA) of the resident
  * state to / from a device buffer: buf[j*6*Np + r] <-> element d_elems[j].
- * d_elems and d_buf are device pointers. */
+ * d_elems and d_buf are device pointers.  No counterpart in the reference: the
+ * halo exchange of a partitioned (multi-GPU) run. */
 int dgtd_state_gather_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, float *d_buf);
 int dgtd_state_scatter_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, const float *d_buf);
 
@@ -222,18 +229,23 @@ int dgtd_etd_step_est(dgtd_op *op, const double *y, const double *b, double h, i
                       double *out, int32_t *dim_used, double *est);
 
 /* ---- device-resident state (no host copies) ---------------------------
- * The op owns a resident f32 state (the reference's `y` buffer). */
+ * The op owns a resident f32 state (the reference's device `y` buffer, which
+ * GpuOperator keeps private: these calls have no counterpart there and serve
+ * callers that keep the state on the device between calls). */
 int dgtd_state_upload(dgtd_op *op, const float *y);        /* host AoS -> device state */
 int dgtd_state_download(dgtd_op *op, float *y);            /* device state -> host AoS */
 int dgtd_state_load_device(dgtd_op *op, const float *d_y); /* device AoS pointer -> state */
 int dgtd_state_store_device(dgtd_op *op, float *d_y);      /* state -> device AoS pointer */
-/* `steps` LSERK4 steps of `h` on the resident state; drive as dgtd_transient
- * with g_samples on the HOST (steps entries, NULL for free). */
+/* `steps` LSERK4 steps of `h` on the resident state (the stepping loop of
+ * GpuOperator::transient, gpu/operator.rs:906); drive as dgtd_transient with
+ * g_samples on the HOST (steps entries, NULL for free). */
 int dgtd_run_lserk(dgtd_op *op, float h, int64_t steps, int drive, int64_t src_dof,
                    const float *g_samples);
-/* Upload the DRIVE_VECTOR pattern used by dgtd_run_lserk. */
+/* Upload the DRIVE_VECTOR pattern (Drive::Vector, session.rs:107-114) used by
+ * dgtd_run_lserk. */
 int dgtd_set_source_vector(dgtd_op *op, const double *src_vec);
-/* dy = A*y on device AoS pointers (f32). */
+/* dy = A*y on device AoS pointers (f32): GpuOperator::apply (gpu/operator.rs:513)
+ * without the host copies. */
 int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
 
 /* `steps` free LSERK4 steps of `h` from the device AoS state d_y_in into
@@ -267,7 +279,8 @@ int dgtd_field_energy(dgtd_op *op, const double *y, double *energy);
 int dgtd_state_energy(dgtd_op *op, double *energy);
 
 /* ---- statistics -------------------------------------------------------- */
-/* Kernel launches issued by this op since creation / the last reset. */
+/* Kernel launches issued by this op since creation / the last reset (no
+ * counterpart in the reference). */
 int dgtd_op_launch_count(const dgtd_op *op, int64_t *count);
 int dgtd_op_reset_launch_count(dgtd_op *op);
 

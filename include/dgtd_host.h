@@ -47,12 +47,16 @@ int dgtd_mesh_box_graded_z(int32_t nx, int32_t ny, int32_t nz, double lx, double
 int dgtd_host_op_build(const double *nodes, int64_t n_nodes, const int32_t *tets, int64_t n_elem,
                        int32_t order, double flux_alpha, const int32_t *face_port,
                        const double *materials, dgtd_host_op **out);
+/* Releases the host operator (MaxwellOperator is dropped in the reference). */
 int dgtd_host_op_destroy(dgtd_host_op *op);
-/* Fill a dgtd_op_desc whose pointers stay valid while `op` lives. */
+/* Fill a dgtd_op_desc whose pointers stay valid while `op` lives: the arrays
+ * GpuOperator::new flattens (gpu/operator.rs:222-292). */
 int dgtd_host_op_desc(const dgtd_host_op *op, dgtd_op_desc *desc);
+/* Np, Nfp, K and n_dof of the operator (no counterpart in the reference). */
 int dgtd_host_op_info(const dgtd_host_op *op, int32_t *np, int32_t *nfp, int64_t *n_elem,
                       int64_t *n_dof);
-/* Copy a named array out as doubles: nodes, mass, dr, ds, dt, lift, face_nodes,
+/* Copy a named array out as doubles (no counterpart in the reference; a test
+ * and inspection aid): nodes, mass, dr, ds, dt, lift, face_nodes,
  * face_w, jinv, jac, origin, det, normal, fscale, nbr, nbr_lf, port, perm,
  * inv_eps, inv_mu, sigma_eps, sigma_mu. */
 int dgtd_host_op_get(const dgtd_host_op *op, const char *name, double *out);
@@ -61,7 +65,8 @@ int dgtd_host_node_coords(const dgtd_host_op *op, double *out);
 /* nearest_node_dof (rhs.rs:1030-1051): field 0=E 1=H, comp 0..2. */
 int dgtd_host_nearest_node_dof(const dgtd_host_op *op, const double *point, int32_t field,
                                int32_t comp, int64_t *dof);
-/* Number of (e,f) faces on port `port`, in (e,f) ascending order. */
+/* Number of (e,f) faces on port `port`, in (e,f) ascending order (the face
+ * set port_source and port_modal_projections walk, rhs.rs:1157-1242). */
 int dgtd_host_port_n_faces(const dgtd_host_op *op, int32_t port, int64_t *n_faces);
 /* RectPort TE_mn (waveguide.rs:124-145) profiles at every node of port
  * `port`'s faces: out[n_faces*Nfp*6] = (e_t xyz, h_t xyz).  The frame is
