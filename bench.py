@@ -105,30 +105,72 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(steps, warmup, n_cells=24, order=4, threads=None):
-    """Oracle (f64 CPU restatement of explicit.rs + rhs.rs apply_into) on the
-    sphere_pulse workload at n_cells^3; returns (DOF-stage/s, info)."""
-    from oracle import oracle as R
+def sphere_pulse_config(cells, order, n_dof, world):
+    """The workload description shared by both arms' JSON lines."""
+    return {"workload": f"sphere_pulse: jittered {cells}^3x6 box ({6 * cells ** 3:,} tets), N={order}, eps_r=4 "
+                        "sphere r=0.25, Gaussian Ez pulse sigma=0.05 at (0.3,0.4,0.5), upwind, PEC, LSERK4",
+            "cells": f"{cells}^3", "order": order, "n_dof": n_dof,
+            "l2": "state 4*n_dof bytes per buffer >> 126 MB L2; no flush",
+            "parallelism": f"replica x{world}" if world > 1 else "single GPU"}
 
-    from rapidfem_b200 import workloads as W
+
+def _oracle_sphere_pulse(R, n_cells, order):
+    """The sphere_pulse workload built by the oracle alone (mesh_gen.rs jitter,
+    seed 2024, +-10% h; eps_r = 4 for element centroids within 0.25 of the
+    centre; the Gaussian E_z pulse at the oracle's nodes): the reference arm
+    and the CPU baseline load no product code."""
+    nodes, tets = R.box_mesh_jittered(n_cells, n_cells, n_cells, 1.0, 1.0, 1.0, 0.10, 2024)
+    cen = nodes[tets].mean(axis=1)
+    eps = np.where(np.linalg.norm(cen - 0.5, axis=1) < 0.25, 4.0, 1.0)
+    mat = np.zeros((eps.size, 8))
+    mat[:, 0:3] = eps[:, None]
+    mat[:, 3:6] = 1.0
+    orc = R.Operator(nodes, tets, order, 1.0, materials=mat)
+    x = orc.node_coords()
+    y = np.zeros((x.shape[0], 6))
+    y[:, 2] = np.exp(-((x - np.array([0.3, 0.4, 0.5])) ** 2).sum(axis=1) / (2 * 0.05 ** 2))
+    return orc, y.ravel()
+
+
+def _oracle_dt(R, n_cells, order):
+    """LSERK4 step 0.5 * 2.8 / rho, rho from 20 power iterations of the oracle
+    at 12^3 scaled by n_cells / 12 (rho grows as 1/h); the step only has to keep
+    a timing run stable."""
+    orc, _ = _oracle_sphere_pulse(R, 12, order)
+    rho, _ = orc.power_rho(20)
+    return 0.5 * 2.8 / (rho * n_cells / 12.0)
+
+
+def cpu_reference_rate(steps, warmup, n_cells=24, order=4, threads=None, budget_s=None):
+    """Oracle (f64 CPU restatement of explicit.rs:100-135 over rhs.rs:1262-1473,
+    OpenMP over all host threads) on the sphere_pulse workload at n_cells^3;
+    returns (DOF-stage/s, info).  With budget_s, at most one warm-up step is
+    run and the timed steps are capped so that they take about budget_s."""
+    from oracle import oracle as R
 
     if threads:
         R.set_threads(threads)
-    wl = W.sphere_pulse(n_cells, order)
-    orc = R.Operator(wl.mesh.nodes, wl.mesh.tets, order, 1.0, materials=wl.materials)
-    prod = wl.build()
-    y = wl.y0(prod)
-    rho, _ = orc.power_rho(8)
-    dt = 0.5 * 2.8 / rho
+    orc, y = _oracle_sphere_pulse(R, n_cells, order)
+    dt = _oracle_dt(R, n_cells, order)
+    t_warm = None
+    if budget_s is not None:
+        warmup = min(warmup, 1)
     if warmup:
+        t0 = time.perf_counter()
         y = orc.lserk(y, dt, warmup)
+        t_warm = (time.perf_counter() - t0) / warmup
+    timed = steps
+    if budget_s is not None and t_warm:
+        timed = max(1, min(steps, int(budget_s / t_warm)))
     t0 = time.perf_counter()
-    y = orc.lserk(y, dt, steps)
+    y = orc.lserk(y, dt, timed)
     el = time.perf_counter() - t0
-    rate = orc.n_dof * 5 * steps / el
-    return rate, {"cores": R.threads(), "seconds": el, "n_dof": orc.n_dof, "steps": steps,
-                  "sample": f"sphere_pulse at {n_cells}^3 x 6 = {wl.mesh.n_tets} tets, N={order}, "
-                            f"{steps} LSERK4 steps (f64, OpenMP)"}
+    rate = orc.n_dof * 5 * timed / el
+    return rate, {"cores": R.threads(), "seconds": el, "n_dof": orc.n_dof, "steps": timed, "warmup": warmup,
+                  "dt": dt, "finite": bool(np.all(np.isfinite(y))),
+                  "sample": f"sphere_pulse at {n_cells}^3 x 6 = {6 * n_cells ** 3} tets, N={order}, "
+                            f"{timed} timed LSERK4 steps after {warmup} warm-up (f64, OpenMP, "
+                            f"{R.threads()} threads)"}
 
 
 def run_reference(args):
@@ -136,19 +178,21 @@ def run_reference(args):
     if rank != 0:
         return 0
     steps, warmup = args.steps, args.warmup
-    rate, info = cpu_reference_rate(steps, warmup, n_cells=args.ref_cells)
+    rate, info = cpu_reference_rate(steps, warmup, n_cells=args.cells, budget_s=args.ref_budget)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "DOF-stage/s", "n_gpus": args.gpus,
-        "steps": steps, "warmup": warmup, "ms_per_step": info["seconds"] / steps * 1e3,
+        "steps": steps, "warmup": warmup, "ms_per_step": info["seconds"] / info["steps"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "sphere_pulse (jittered 48^3 box, N=4, eps_r=4 sphere, Gaussian Ez pulse)",
-                   "sample_cells": f"{args.ref_cells}^3", "order": 4, "integrator": "LSERK4"},
+        "config": sphere_pulse_config(args.cells, 4, info["n_dof"], world),
         "cpu_baseline": {"value": rate, "unit": "DOF-stage/s", "cores": info["cores"], "kind": "port",
                          "sample": info["sample"]},
         "e2e": {"value": rate, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "steps_timed": info["steps"], "warmup_run": info["warmup"], "finite": info["finite"],
         "note": "The reference's Rust CPU path cannot be built here (no Rust toolchain); timed is the "
-                "oracle's C restatement of explicit.rs:100-135 over rhs.rs:1262-1473.",
+                "oracle's C restatement of explicit.rs:100-135 over rhs.rs:1262-1473 on the full workload, "
+                "one warm-up step and as many of the requested steps as fit the time budget "
+                f"({args.ref_budget:.0f} s).",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -261,12 +305,8 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "sphere_pulse: jittered 48^3x6 box (663,552 tets), N=4, eps_r=4 sphere r=0.25, "
-                               "Gaussian Ez pulse sigma=0.05 at (0.3,0.4,0.5), upwind, PEC, LSERK4",
-                   "cells": f"{args.cells}^3", "order": order, "n_dof": n, "dt": dt,
-                   "engine": ["fp32", "tf32x3"][gop.engine],
-                   "l2": "state 4*n_dof bytes per buffer >> 126 MB L2; no flush",
-                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "config": sphere_pulse_config(args.cells, order, n, world),
+        "run": {"dt": dt, "engine": ["fp32", "tf32x3"][gop.engine]},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -721,7 +761,9 @@ def main():
                     help="stage kernel: FP32 CUDA cores, or the tcgen05 tensor-core kernel (3xTF32 products)")
     ap.add_argument("--power-iters", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=10)
-    ap.add_argument("--ref-cells", type=int, default=24)
+    ap.add_argument("--ref-cells", type=int, default=24, help="mesh of the b200 arm's bounded CPU baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of timed steps of the reference arm (full workload)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t", "c2-accuracy"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "

@@ -119,6 +119,13 @@ int dgtd_op_n_dof(const dgtd_op *op, int64_t *n_dof);
  * OpenCL kernel. */
 int dgtd_op_set_engine(dgtd_op *op, int engine);
 int dgtd_op_get_engine(const dgtd_op *op, int *engine);
+/* Synchronises the op's stream and returns DGTD_ERR_TIMEOUT if a tensor-core
+ * kernel of this op gave up one of its bounded waits since the last check
+ * (then clears the flag).  The entry points that synchronise check the flag
+ * themselves; this is for work queued without a synchronisation
+ * (dgtd_run_lserk, dgtd_lserk_stage, dgtd_run_lserk_static).  No counterpart
+ * in the reference, whose OpenCL kernels have no bounded waits. */
+int dgtd_op_check_error(dgtd_op *op);
 
 /* GpuOperator::apply (gpu/operator.rs:513): dy = A*y, host f32 buffers of
  * n_dof, AoS layout. */
@@ -205,6 +212,12 @@ int dgtd_transient_kcl_functionals(dgtd_op *op, const float *y0, float dt, int64
                                    const int64_t *fun_ptr, const int64_t *fun_idx,
                                    const double *fun_w, double *out, float *y_final,
                                    dgtd_kcl_stats *stats);
+/* The accepted substeps of the op's last adaptive run, in order: h[i] (operator
+ * time) and the output frame frame[i] it advanced (whose waveform value it
+ * held).  Up to `cap` entries are written; *n_total receives the run's accepted
+ * count (the device logs the first 65,536).  No counterpart in the reference:
+ * it lets a caller replay the run's exact step sequence, e.g. on a CPU path. */
+int dgtd_kcl_accepted_steps(dgtd_op *op, float *h, int32_t *frame, int64_t cap, int64_t *n_total);
 
 /* GpuOperator::expmv (gpu/operator.rs:1175): exp(t*A)*v by Arnoldi, f64 basis
  * and CGS2 on the device, sub-stepped into chunks of <= 12 (KRYLOV_CHUNK).
@@ -254,12 +267,16 @@ int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
  * cudaMalloc (hosts whose framework owns the device memory budget).  The
  * scratch -- two SoA state buffers and the residual register -- is a
  * file-scope device array of 3 x 2,097,152 floats (24 MiB) that every GPU
- * loading the library holds until exit; ops with n_dof above 2,097,152 are
- * rejected with DGTD_ERR_BAD_ARG.  The first call on a device takes the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls share the one array: calls whose work
- * overlaps on the GPU (other streams, other threads) race.  The work is queued
- * on the op's stream; synchronise before reading d_y_out. */
+ * loading the library holds until exit.  The kernels work on whole tiles of
+ * 20 elements, so the limit applies to n_elem rounded up to a multiple of 20,
+ * times 6*Np: an op above it is rejected with DGTD_ERR_BAD_ARG.  The first
+ * call on a device takes the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  All calls share the one
+ * array: calls whose work overlaps on the GPU (other streams, other threads)
+ * race.  The work is queued on the op's stream and the call does not
+ * synchronise: synchronise before reading d_y_out, then call
+ * dgtd_op_check_error, which reports (DGTD_ERR_TIMEOUT) a tensor-core kernel
+ * that gave up one of its bounded waits during the run. */
 int dgtd_run_lserk_static(dgtd_op *op, const float *d_y_in, float *d_y_out, float h, int64_t steps);
 
 /* ---- session helpers --------------------------------------------------

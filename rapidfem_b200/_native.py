@@ -81,6 +81,7 @@ _sig("dgtd_op_destroy", C.c_int, _vp)
 _sig("dgtd_op_n_dof", C.c_int, _vp, C.POINTER(_i64))
 _sig("dgtd_op_set_engine", C.c_int, _vp, C.c_int)
 _sig("dgtd_op_get_engine", C.c_int, _vp, C.POINTER(C.c_int))
+_sig("dgtd_op_check_error", C.c_int, _vp)
 _sig("dgtd_apply", C.c_int, _vp, _pf, _pf)
 _sig("dgtd_transient", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pf)
 _sig("dgtd_transient_probes", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _vp,
@@ -115,6 +116,7 @@ _sig("dgtd_transient_kcl", C.c_int, _vp, _pf, _f32, _i64, C.c_int, _i64, _vp, _v
      C.c_int, _vp, C.POINTER(KclStats))
 _sig("dgtd_transient_kcl_functionals", C.c_int, _vp, _pf, _f32, _i64, C.c_int, _i64, _vp, _vp,
      C.POINTER(KclController), _i64, _vp, _vp, _vp, _vp, _vp, C.POINTER(KclStats))
+_sig("dgtd_kcl_accepted_steps", C.c_int, _vp, _pf, _pi, _i64, C.POINTER(_i64))
 _sig("dgtd_transient_functionals", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _i64,
      _vp, _vp, _vp, _vp, _vp)
 _sig("dgtd_expmv", C.c_int, _vp, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32))

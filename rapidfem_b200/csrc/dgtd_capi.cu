@@ -182,6 +182,8 @@ struct dgtd_op {
   unsigned long long* phase_clk = nullptr;  // instrumented builds: per-phase cycle counters
   // KCL adaptive stepping: controller, backup, embedded error, stage point, RHS, waveform
   DevBuf<dgtd::KclCtl> kcl_ctl;
+  DevBuf<dgtd::KclLogEntry> kcl_log;
+  int64_t kcl_log_n = 0;  // accepted substeps of the last adaptive run
   DevBuf<float> kcl_bak, kcl_e, kcl_stage, kcl_k, kcl_g;
   DevBuf<double> kcl_part;
 
@@ -193,7 +195,7 @@ struct dgtd_op {
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
     kst.free(); skip.free(); mass.free(); absdet.free();
     tc_bvol.free(); tc_blift.free(); err.free();
-    kcl_ctl.free(); kcl_bak.free(); kcl_e.free(); kcl_stage.free(); kcl_k.free(); kcl_g.free(); kcl_part.free();
+    kcl_ctl.free(); kcl_log.free(); kcl_bak.free(); kcl_e.free(); kcl_stage.free(); kcl_k.free(); kcl_g.free(); kcl_part.free();
   }
 };
 
@@ -656,7 +658,8 @@ extern "C" int dgtd_op_reset_launch_count(dgtd_op* op) {
 
 static int ensure_aos32(dgtd_op* op) { return op->aos32.alloc(op->n_dof + 4); }
 
-// A tensor-core kernel that gave up a bounded wait leaves a flag; report it.
+// A tensor-core kernel that gave up a bounded wait leaves a flag; report it
+// (and clear it, so it is reported once).
 static int check_kernel_flag(dgtd_op* op) {
   int h = 0;
   CUDA_TRY(cudaMemcpyAsync(&h, op->err.p, sizeof(int), cudaMemcpyDeviceToHost, op->stream()));
@@ -666,6 +669,12 @@ static int check_kernel_flag(dgtd_op* op) {
     return set_error(DGTD_ERR_TIMEOUT, "a tensor-core kernel gave up waiting for its copies / MMAs");
   }
   return DGTD_OK;
+}
+
+extern "C" int dgtd_op_check_error(dgtd_op* op) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_check_error: null op");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  return check_kernel_flag(op);
 }
 
 extern "C" int dgtd_state_load_device(dgtd_op* op, const float* d_y) {
@@ -1207,6 +1216,8 @@ int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, co
   DGTD_TRY(check_drive(op, drive, src_dof, g, steps, &src_idx));
   const size_t len = state_len(op);
   DGTD_TRY(op->kcl_ctl.alloc(1));
+  DGTD_TRY(op->kcl_log.alloc(dgtd::kKclLogCap));
+  op->kcl_log_n = 0;
   const bool fresh = op->kcl_stage.n < len;
   DGTD_TRY(op->kcl_bak.alloc(len));
   DGTD_TRY(op->kcl_e.alloc(len));
@@ -1234,6 +1245,7 @@ int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, co
   c.steps = steps; c.attempt_cap = kKclAttemptCap;
   c.status = steps > 0 ? dgtd::kKclRunning : dgtd::kKclDone;
   c.record = -1;
+  c.log = op->kcl_log.p;
   KclCtl* dc = op->kcl_ctl.p;
   CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
   const int* d_skip = &dc->skip;
@@ -1281,6 +1293,7 @@ int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, co
     batch = std::max<int64_t>(1, std::min<int64_t>(batch, 256));
   }
   (void)attempts;
+  op->kcl_log_n = c.n_acc;
   if (stats) {
     stats->accepted = c.n_acc;
     stats->rejected = c.n_rej;
@@ -1363,6 +1376,24 @@ extern "C" int dgtd_kcl_step(dgtd_op* op, const double* y, double h, double* y_o
   CUDA_TRY(cudaMemcpyAsync(err, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   return check_kernel_flag(op);
+}
+
+extern "C" int dgtd_kcl_accepted_steps(dgtd_op* op, float* h, int32_t* frame, int64_t cap, int64_t* n_total) {
+  if (!op || cap < 0 || (cap > 0 && (!h || !frame)) || !n_total)
+    return set_error(DGTD_ERR_BAD_ARG, "kcl_accepted_steps: bad argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  *n_total = op->kcl_log_n;
+  const int64_t n = std::min<int64_t>(std::min<int64_t>(cap, op->kcl_log_n), dgtd::kKclLogCap);
+  if (n == 0) return DGTD_OK;
+  std::vector<dgtd::KclLogEntry> buf((size_t)n);
+  CUDA_TRY(cudaMemcpyAsync(buf.data(), op->kcl_log.p, n * sizeof(dgtd::KclLogEntry), cudaMemcpyDeviceToHost,
+                           op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  for (int64_t i = 0; i < n; ++i) {
+    h[i] = buf[i].h;
+    frame[i] = buf[i].frame;
+  }
+  return DGTD_OK;
 }
 
 extern "C" int dgtd_transient_kcl(dgtd_op* op, const float* y0, float dt, int64_t steps, int drive,
@@ -1905,9 +1936,12 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
   if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: step must be positive");
   const int64_t padded = op->n_elem_pad * 6 * op->np;  // the kernels touch whole tiles
   if (padded > kStaticMaxDof)
-    return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: n_dof " + std::to_string(op->n_dof) +
-                                           " exceeds the static scratch limit of " + std::to_string(kStaticMaxDof) +
-                                           " DOFs; use dgtd_run_lserk");
+    return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: the op's state padded to whole 20-element tiles (" +
+                                           std::to_string(op->n_elem_pad) + " elements x " +
+                                           std::to_string(6 * op->np) + " = " + std::to_string(padded) +
+                                           " values, n_dof " + std::to_string(op->n_dof) +
+                                           ") exceeds the static scratch limit of " + std::to_string(kStaticMaxDof) +
+                                           " values; use dgtd_run_lserk");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   float* base = nullptr;
   DGTD_TRY(lserk_scratch(op->ctx->device, &base));

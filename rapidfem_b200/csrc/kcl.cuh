@@ -50,12 +50,20 @@ constexpr float kKclNonfiniteErr = 10.0f;  // constants.rs:296
 
 enum KclStatus : int { kKclRunning = 0, kKclDone = 1, kKclCollapsed = 2, kKclCapped = 3 };
 
+// One accepted substep of a run: its size and the output frame it belongs to.
+struct KclLogEntry {
+  float h;
+  int frame;
+};
+constexpr long long kKclLogCap = 1 << 16;  // accepted substeps logged per run
+
 struct KclCtl {
   // controller settings (session.rs:130-143)
   double atol, rtol, safety, growth, shrink, alpha, beta, min_step_factor;
   // state, in the f32 of the reference's GPU path (gpu/operator.rs:836-887)
   float dt, h, h_try, prev_err, t_rel, err_norm, h_min_log, h_max_log;
   long long frame, steps, n_acc, n_rej, attempts_in_frame, attempt_cap;
+  KclLogEntry* log;  // accepted substeps, the first kKclLogCap of the run (or null)
   int status;
   int skip;     // nonzero: the attempt in flight does nothing
   int restore;  // the last attempt was rejected
@@ -151,6 +159,7 @@ __global__ void __launch_bounds__(256) k_kcl_control(KclCtl* __restrict__ ctl, c
   const float h_try = c.h_try;
   const bool accept = isfinite(err) && err <= 1.0f;
   if (accept) {
+    if (c.log != nullptr && c.n_acc < kKclLogCap) c.log[c.n_acc] = KclLogEntry{h_try, (int)c.frame};
     c.t_rel += h_try;
     c.n_acc += 1;
     const float factor = (float)kcl_factor(c, (double)err, (double)c.prev_err, false);

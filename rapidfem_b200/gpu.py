@@ -130,6 +130,11 @@ class GpuOperator:
         check(lib.dgtd_op_get_engine(self._h, C.byref(e)))
         return e.value
 
+    def check_error(self) -> None:
+        """Synchronise and raise DgtdError (TIMEOUT) if a tensor-core kernel of
+        this op gave up a bounded wait since the last check."""
+        check(lib.dgtd_op_check_error(self._h))
+
     def launch_count(self) -> int:
         c = C.c_int64()
         check(lib.dgtd_op_launch_count(self._h, C.byref(c)))
@@ -314,6 +319,20 @@ class GpuOperator:
                                      C.byref(ctl), 1 if record else 0, out.ctypes.data, C.byref(st)))
         stats = {"accepted": st.accepted, "rejected": st.rejected, "h_min": st.h_min, "h_max": st.h_max}
         return (out.reshape(steps + 1, self._n) if record else out), stats
+
+    def kcl_accepted_steps(self):
+        """The accepted substeps of the last adaptive run: (h[n], frame[n]),
+        the step sizes in order and the output frame each one advanced."""
+        n = C.c_int64()
+        check(lib.dgtd_kcl_accepted_steps(self._h, np.zeros(1, np.float32), np.zeros(1, np.int32), 0,
+                                          C.byref(n)))
+        cap = min(n.value, 1 << 16)
+        h = np.zeros(max(cap, 1), dtype=np.float32)
+        fr = np.zeros(max(cap, 1), dtype=np.int32)
+        check(lib.dgtd_kcl_accepted_steps(self._h, h, fr, cap, C.byref(n)))
+        if n.value > cap:
+            raise RuntimeError(f"the run accepted {n.value} substeps; the device log holds {cap}")
+        return h[:cap], fr[:cap]
 
     def transient_kcl_functionals(self, y0, dt, steps, drive=None, g=None, controller=None, functionals=()):
         """As transient_kcl, recording per frame the linear functionals

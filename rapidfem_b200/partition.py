@@ -157,26 +157,50 @@ def join_state(parts: list[Part], locals_: list[np.ndarray], np_: int) -> np.nda
 
 class GpuEngine:
     """The device operator of one part, for ShardedLserk / LoopbackLserk.
-    Exchange buffers are torch CUDA tensors on the operator's stream."""
 
-    def __init__(self, gop, device):
+    Every kernel of the operator, the exchange buffers and the transport's
+    collectives run on ONE torch CUDA stream, which the operator's context is
+    bound to.  NCCL point-to-point operations issued under `comm()` wait for
+    the gathers queued before them on that stream, and their completion is
+    waited for on that stream before the scatters that follow, so an exchange
+    needs no host synchronisation.  Engines whose operators share a context
+    (all parts on one device) share its stream: the first engine of a context
+    binds it (`stream`, or a new torch stream), the others reuse it."""
+
+    def __init__(self, gop, device, stream=None):
         import torch
 
         self.torch = torch
         self.gop = gop
         self.device = device
+        bound = getattr(gop.ctx, "_engine_stream", None)
+        if bound is None:
+            bound = stream if stream is not None else torch.cuda.Stream(device=device)
+            gop.ctx.set_stream(bound.cuda_stream)
+            gop.ctx._engine_stream = bound
+        elif stream is not None and stream is not bound:
+            raise ValueError("engines of one context must share its stream")
+        self.stream = bound
         self.bs = 6 * gop.host_op.np
         self._idx = {}
 
     def _index(self, ids: np.ndarray):
         hit = self._idx.get(id(ids))
         if hit is None:
-            hit = (ids, self.torch.from_numpy(np.ascontiguousarray(ids, dtype=np.int64)).to(self.device))
+            with self.torch.cuda.stream(self.stream):
+                t = self.torch.from_numpy(np.ascontiguousarray(ids, dtype=np.int64)).to(self.device)
+            self.stream.synchronize()  # the index list is copied before its first use
+            hit = (ids, t)
             self._idx[id(ids)] = hit  # the list stays referenced, so its id is not reused
         return hit[1]
 
     def new_buffer(self, n_elem: int):
-        return self.torch.empty(n_elem * self.bs, dtype=self.torch.float32, device=self.device)
+        with self.torch.cuda.stream(self.stream):
+            return self.torch.empty(n_elem * self.bs, dtype=self.torch.float32, device=self.device)
+
+    def comm(self):
+        """Context in which the transport issues its operations (this engine's stream)."""
+        return self.torch.cuda.stream(self.stream)
 
     def gather(self, ids: np.ndarray, buf) -> None:
         self.gop.gather_elements(self._index(ids).data_ptr(), ids.size, buf.data_ptr())
@@ -188,7 +212,7 @@ class GpuEngine:
         self.gop.lserk_stage(h, s)
 
     def sync(self) -> None:
-        self.gop.ctx.synchronize()
+        self.stream.synchronize()
 
     def load(self, y_local) -> None:
         self.gop.upload(np.asarray(y_local, dtype=np.float32))
@@ -230,10 +254,17 @@ class ShardedLserk:
         self.rbuf = {q: engine.new_buffer(ids.size) for q, ids in part.recv.items()}
 
     def exchange(self) -> None:
+        """Gather the blocks peers need, move them, scatter the received ones.
+        A device engine orders the three on its stream (no host wait); an
+        engine without `comm()` works synchronously on the host."""
         for q, ids in self.part.send.items():
             self.engine.gather(ids, self.sbuf[q])
-        self.engine.sync()
-        self.transport.exchange(self.sbuf, self.rbuf)
+        comm = getattr(self.engine, "comm", None)
+        if comm is None:
+            self.transport.exchange(self.sbuf, self.rbuf)
+        else:
+            with comm():
+                self.transport.exchange(self.sbuf, self.rbuf)
         for q, ids in self.part.recv.items():
             self.engine.scatter(ids, self.rbuf[q])
 

@@ -10,7 +10,7 @@ live as Rust `const` arrays in
 This script reads those files as text and writes the numbers into JSON
 fixtures, so the tests never need the reference tree at run time.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT
 """
 from __future__ import annotations
 
@@ -69,4 +69,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the rapidfem source tree>")
+    main(sys.argv[1])

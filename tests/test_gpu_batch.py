@@ -51,3 +51,33 @@ def test_batch_matches_solo_runs(ctx):
             else:
                 assert rel_l2(got[i], want) < 1e-6
             assert np.all(np.isfinite(got[i])) and np.max(np.abs(got[i])) > 0
+
+
+def test_batch_instances_match_oracle():
+    """One instance of every order (2..5) of an autotuned, graph-replayed batch
+    of uneven cavities against the f64 oracle run alone with that instance's
+    own dt and initial field: 500 LSERK4 steps (explicit.rs:100-135), relative
+    L2 < 1e-4 at the final step."""
+    from oracle import oracle as R
+
+    inst = B.random_cavities(12, seed=5, cells=(2, 4), orders=(2, 5))
+    assert {i.order for i in inst} == {2, 3, 4, 5}
+    groups = B.build_groups(inst)
+    B.initial_fields(groups, inst)
+    B.assign_steps(ctx_holder := G.GpuContext(0), groups, inst, iters=20)
+    runner = B.BatchRunner(ctx_holder, groups)
+    runner.autotune(trial_steps=1)
+    runner.capture(steps_per_graph=10)
+    steps = 500
+    runner.run(steps)
+    got = runner.states(inst)
+    for g in groups:
+        j = len(g.members) - 1  # the last member: a nonzero element offset in the group
+        i = g.members[j]
+        n = inst[i].cells
+        nodes, tets = R.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+        orc = R.Operator(nodes, tets, g.order, 1.0, materials=inst[i].materials)
+        y0 = g.y0[g.dof_slice(j)].astype(np.float64)
+        want = orc.lserk(y0, float(np.float32(inst[i].dt)), steps)
+        assert rel_l2(got[i], want) < 1e-4, (g.order, rel_l2(got[i], want))
+        assert np.max(np.abs(want)) > 1e-3 * np.max(np.abs(y0))

@@ -33,12 +33,19 @@ def _static(gop, d_in, d_out, h, steps):
     return lib.dgtd_run_lserk_static(gop.handle, d_in, d_out, h, steps)
 
 
-def test_static_lserk_matches_allocating_entry_point_twice():
+@pytest.mark.parametrize("cells,engine", [((5, 4, 4), None), ((3, 3, 3), _native.ENGINE_FP32),
+                                          ((3, 3, 3), _native.ENGINE_TF32X3)],
+                         ids=["whole-tiles", "padded-fp32", "padded-tf32x3"])
+def test_static_lserk_matches_allocating_entry_point_twice(cells, engine):
+    """(5,4,4): 480 tets, whole 20-element tiles.  (3,3,3): 162 tets, so the
+    last tile is padded and the call clears the padding of its scratch."""
     import torch
 
     ctx = G.GpuContext(0)
-    op = O.MaxwellOperator(O.structured_box(5, 4, 4), 3, 1.0)
+    op = O.MaxwellOperator(O.structured_box(*cells), 3, 1.0)
     gop = G.GpuOperator(ctx, op)
+    if engine is not None:
+        gop.set_engine(engine)
     n = gop.n_dof()
     assert n <= STATIC_MAX_DOF
     y0 = np.sin(0.3 + 0.017 * np.arange(n)).astype(np.float32)
@@ -54,9 +61,11 @@ def test_static_lserk_matches_allocating_entry_point_twice():
     torch.cuda.synchronize()
     _native.check(_static(gop, d_in.data_ptr(), d_mid.data_ptr(), h, steps))
     ctx.synchronize()
+    gop.check_error()  # no bounded wait of the run gave up
     got1 = d_mid.cpu().numpy()
     _native.check(_static(gop, d_mid.data_ptr(), d_out.data_ptr(), h, steps))
     ctx.synchronize()
+    gop.check_error()
     got2 = d_out.cpu().numpy()
 
     assert rel_l2(got1, want1) < RUN_TOL
