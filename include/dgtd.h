@@ -178,6 +178,21 @@ int dgtd_lserk_stage(dgtd_op *op, float h, int32_t stage, int drive, int64_t src
 int dgtd_state_gather_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, float *d_buf);
 int dgtd_state_scatter_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, const float *d_buf);
 
+/* ---- FP64 path ---------------------------------------------------------
+ * The same RHS and LSERK4 stage in f64 on the CUDA cores (f64 operators,
+ * element records and state): the arithmetic of the reference's CPU path
+ * (rhs.rs, explicit.rs) on the device, for FP64 runs and as the reference
+ * solution at sizes the CPU cannot reach.  Host AoS f64 buffers.
+ * MaxwellOperator::apply (rhs.rs:1246) in f64: */
+int dgtd_apply_f64(dgtd_op *op, const double *y, double *dy);
+/* dgtd_transient in f64 (LserkWorkspace::step_into, explicit.rs:100-135, driven
+ * as session.rs:107-114): `steps` frames of `dt`, each `substeps` steps,
+ * g_samples[steps*substeps] held per substep; with record != 0 `out` receives
+ * [(steps+1)*n_dof], else the final state. */
+int dgtd_transient_f64(dgtd_op *op, const double *y0, double dt, int64_t steps, int64_t substeps,
+                       int drive, int64_t src_dof, const double *src_vec, const double *g_samples,
+                       int record, double *out);
+
 /* ---- KCL adaptive transient (gpu/operator.rs:823-893, session.rs:130-187)
  * The KCL RK4(3)5[2R+]C embedded pair with the PI step-size controller, the
  * controller running on the device: attempts are queued in batches and the

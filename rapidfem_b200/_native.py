@@ -84,6 +84,8 @@ _sig("dgtd_op_get_engine", C.c_int, _vp, C.POINTER(C.c_int))
 _sig("dgtd_op_check_error", C.c_int, _vp)
 _sig("dgtd_apply", C.c_int, _vp, _pf, _pf)
 _sig("dgtd_transient", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pf)
+_sig("dgtd_apply_f64", C.c_int, _vp, _pd, _pd)
+_sig("dgtd_transient_f64", C.c_int, _vp, _pd, _f64, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pd)
 _sig("dgtd_transient_probes", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _vp,
      _i64, _vp, _vp)
 class KclController(C.Structure):

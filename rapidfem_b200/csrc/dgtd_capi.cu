@@ -157,12 +157,16 @@ struct dgtd_op {
   int order = 0, np = 0, nfp = 0;
   int64_t n_elem = 0, n_dof = 0;
   float alpha = 1.f;
+  double alpha64 = 1.0;
   int engine = DGTD_ENGINE_FP32;
   int64_t launches = 0;
   // operator data
   DevBuf<float> meta, dT, liftT;
   DevBuf<uint8_t> fnodes, gtab;
   int n_gather = 0;
+  // FP64 path: f64 element records and operators, f64 state (allocated on first use)
+  DevBuf<double> meta64, dT64, liftT64, y64[2], p64, src_vec64;
+  int cur64 = 0;
   // state
   DevBuf<float> y[2], p, src_vec, aos32;
   int cur = 0;
@@ -191,6 +195,7 @@ struct dgtd_op {
   ~dgtd_op() {
     cudaSetDevice(device);
     meta.free(); dT.free(); liftT.free(); fnodes.free(); gtab.free();
+    meta64.free(); dT64.free(); liftT64.free(); y64[0].free(); y64[1].free(); p64.free(); src_vec64.free();
     y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
     basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
     kst.free(); skip.free(); mass.free(); absdet.free();
@@ -325,6 +330,39 @@ int launch_rhs_n(dgtd_op* op, const RhsParams& P) {
 }
 
 template <int N, int MODE>
+int launch_rhs64_n(dgtd_op* op, const RhsParamsT<double>& P) {
+  using C = Fp32Cfg<N, double>;
+  static int blocks_per_sm[8] = {0};
+  auto kern = rhs_fp64_kernel<N, MODE>;
+  int& bps = blocks_per_sm[op->ctx->device & 7];
+  if (bps == 0) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, C::THREADS, C::SMEM));
+    if (bps < 1) return set_error(DGTD_ERR_CUDA, "fp64 rhs kernel does not fit on an SM");
+  }
+  OpTablesT<double> T{op->dT64.p, op->liftT64.p, op->fnodes.p, op->gtab.p, op->n_gather};
+  const int64_t tiles = (op->n_elem + C::E - 1) / C::E;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms * bps);
+  kern<<<grid, C::THREADS, C::SMEM, op->stream()>>>(P, T);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+// The FP64 path (CUDA cores, f64 throughout), orders 1-5.
+template <int MODE>
+int launch_rhs64(dgtd_op* op, const RhsParamsT<double>& P) {
+  switch (op->order) {
+    case 1: return launch_rhs64_n<1, MODE>(op, P);
+    case 2: return launch_rhs64_n<2, MODE>(op, P);
+    case 3: return launch_rhs64_n<3, MODE>(op, P);
+    case 4: return launch_rhs64_n<4, MODE>(op, P);
+    case 5: return launch_rhs64_n<5, MODE>(op, P);
+    default: return set_error(DGTD_ERR_UNSUPPORTED, "order outside 1..5");
+  }
+}
+
+template <int N, int MODE>
 int launch_rhs_tc_n(dgtd_op* op, const RhsParams& P) {
   using C = TcCfg<N>;
   static bool attr[8] = {false};
@@ -376,6 +414,16 @@ RhsParams base_params(dgtd_op* op) {
   return P;
 }
 
+RhsParamsT<double> base_params64(dgtd_op* op) {
+  RhsParamsT<double> P;
+  std::memset(&P, 0, sizeof(P));
+  P.meta = op->meta64.p;
+  P.n_elem = op->n_elem;
+  P.src_idx = -1;
+  P.alpha = op->alpha64;
+  return P;
+}
+
 const double kLserkA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
                            -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
 const double kLserkB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
@@ -420,6 +468,8 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   // Host-side packing: element records, gather tables.
   const int64_t Kpad = ((K + dgtd::kTcTileE - 1) / dgtd::kTcTileE) * dgtd::kTcTileE;
   std::vector<float> meta((size_t)Kpad * dgtd::kMetaWords, 0.f);
+  // the same records in f64 for the FP64 path, integer words as exact values
+  std::vector<double> meta64((size_t)Kpad * dgtd::kMetaWords, 0.0);
   {
     // inert padding records: every face a PEC wall with zero normal / scale / metric
     const uint32_t pec = (uint32_t)dgtd::kPec << 8;
@@ -430,6 +480,10 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
       for (int f = 0; f < 4; ++f) std::memcpy(&M[37 + f], &none, 4);
       std::memcpy(&M[41], &w, 4);
       std::memcpy(&M[42], &w, 4);
+      double* M64 = &meta64[(size_t)e * dgtd::kMetaWords];
+      for (int f = 0; f < 4; ++f) M64[37 + f] = -1.0;
+      M64[41] = (double)w;
+      M64[42] = (double)w;
     }
   }
   std::map<std::vector<uint8_t>, int> table_id;
@@ -440,6 +494,16 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
         return set_error(DGTD_ERR_BAD_ARG, "op_create: face_nodes entry out of range");
   for (int64_t e = 0; e < K; ++e) {
     float* M = &meta[(size_t)e * dgtd::kMetaWords];
+    double* M64 = &meta64[(size_t)e * dgtd::kMetaWords];
+    for (int q = 0; q < 9; ++q) M64[q] = d->jinv[9 * e + q];
+    for (int q = 0; q < 12; ++q) M64[9 + q] = d->face_normal[12 * e + q];
+    for (int q = 0; q < 4; ++q) M64[21 + q] = d->face_fscale[4 * e + q];
+    for (int c = 0; c < 3; ++c) {
+      M64[25 + c] = d->inv_eps[3 * e + c];
+      M64[28 + c] = d->inv_mu[3 * e + c];
+      M64[31 + c] = d->sigma_eps[3 * e + c];
+      M64[34 + c] = d->sigma_mu[3 * e + c];
+    }
     for (int q = 0; q < 9; ++q) M[q] = (float)d->jinv[9 * e + q];
     for (int q = 0; q < 12; ++q) M[9 + q] = (float)d->face_normal[12 * e + q];
     for (int q = 0; q < 4; ++q) M[21 + q] = (float)d->face_fscale[4 * e + q];
@@ -483,25 +547,37 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
         }
       }
       std::memcpy(&M[37 + f], &nb_bits, 4);
+      M64[37 + f] = (double)nb_bits;
       codes[f] = (uint32_t)id | ((uint32_t)kind << 8);
     }
     const uint32_t w0 = codes[0] | (codes[1] << 16), w1 = codes[2] | (codes[3] << 16);
     std::memcpy(&M[41], &w0, 4);
     std::memcpy(&M[42], &w1, 4);
+    M64[41] = (double)w0;
+    M64[42] = (double)w1;
     M[43] = 1.0f;
+    M64[43] = 1.0;
     if (d->dt_scale) {
       const double sc = d->dt_scale[e];
       if (!(std::isfinite(sc) && sc > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "op_create: dt_scale must be positive");
       M[43] = (float)sc;
+      M64[43] = sc;
     }
   }
   std::vector<float> dT((size_t)3 * np * np), liftT((size_t)4 * nfp * np);
+  std::vector<double> dT64(dT.size()), liftT64(liftT.size());
   const double* D[3] = {d->diff_r, d->diff_s, d->diff_t};
   for (int k = 0; k < 3; ++k)
     for (int i = 0; i < np; ++i)
-      for (int j = 0; j < np; ++j) dT[((size_t)k * np + j) * np + i] = (float)D[k][i * np + j];
+      for (int j = 0; j < np; ++j) {
+        dT[((size_t)k * np + j) * np + i] = (float)D[k][i * np + j];
+        dT64[((size_t)k * np + j) * np + i] = D[k][i * np + j];
+      }
   for (int i = 0; i < np; ++i)
-    for (int s = 0; s < 4 * nfp; ++s) liftT[(size_t)s * np + i] = (float)d->lift[i * 4 * nfp + s];
+    for (int s = 0; s < 4 * nfp; ++s) {
+      liftT[(size_t)s * np + i] = (float)d->lift[i * 4 * nfp + s];
+      liftT64[(size_t)s * np + i] = d->lift[i * 4 * nfp + s];
+    }
   std::vector<uint8_t> fnodes(4 * nfp);
   for (int q = 0; q < 4 * nfp; ++q) fnodes[q] = (uint8_t)d->face_nodes[q];
   if (gtab.empty()) gtab.assign(nfp, 0);
@@ -516,6 +592,7 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   op->n_elem = K;
   op->n_dof = 6 * (int64_t)np * K;
   op->alpha = (float)d->flux_alpha;
+  op->alpha64 = d->flux_alpha;
   op->n_gather = (int)table_id.size();
   op->n_elem_pad = Kpad;
   const size_t nstate = (size_t)Kpad * 6 * np + 4;
@@ -524,13 +601,17 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   if ((st = op->meta.alloc(meta.size())) || (st = op->dT.alloc(dT.size())) || (st = op->liftT.alloc(liftT.size())) ||
       (st = op->fnodes.alloc(fnodes.size())) || (st = op->gtab.alloc(gtab.size())) ||
       (st = op->y[0].alloc(nstate)) || (st = op->y[1].alloc(nstate)) || (st = op->p.alloc(nstate)) ||
-      (st = op->err.alloc(1)))
+      (st = op->err.alloc(1)) || (st = op->meta64.alloc(meta64.size())) || (st = op->dT64.alloc(dT64.size())) ||
+      (st = op->liftT64.alloc(liftT64.size())))
     return fail(st);
   cudaStream_t s = ctx->stream;
   cudaError_t e = cudaSuccess;
   if (!e) e = cudaMemcpyAsync(op->meta.p, meta.data(), meta.size() * 4, cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemcpyAsync(op->dT.p, dT.data(), dT.size() * 4, cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemcpyAsync(op->liftT.p, liftT.data(), liftT.size() * 4, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->meta64.p, meta64.data(), meta64.size() * 8, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->dT64.p, dT64.data(), dT64.size() * 8, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(op->liftT64.p, liftT64.data(), liftT64.size() * 8, cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemcpyAsync(op->fnodes.p, fnodes.data(), fnodes.size(), cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemcpyAsync(op->gtab.p, gtab.data(), gtab.size(), cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemsetAsync(op->y[0].p, 0, op->y[0].n * 4, s);
@@ -1007,6 +1088,115 @@ extern "C" int dgtd_transient(dgtd_op* op, const float* y0, float dt, int64_t st
     if (record) DGTD_TRY(dgtd_state_download(op, out + (k + 1) * op->n_dof));
   }
   if (!record) DGTD_TRY(dgtd_state_download(op, out));
+  return DGTD_OK;
+}
+
+// ------------------------------------------------------------------ FP64 path
+//
+// The RHS and the LSERK4 stage in f64 on the CUDA cores (rhs_fp64_kernel): the
+// reference's CPU arithmetic (rhs.rs, explicit.rs in f64) on the device, for
+// FP64 runs and as the reference solution at sizes the CPU cannot reach.
+
+namespace {
+
+int ensure_state64(dgtd_op* op) {
+  const size_t len = state_len(op);
+  const bool fresh = op->y64[0].n < len || op->y64[1].n < len || op->p64.n < len;
+  DGTD_TRY(op->y64[0].alloc(len));
+  DGTD_TRY(op->y64[1].alloc(len));
+  DGTD_TRY(op->p64.alloc(len));
+  DGTD_TRY(op->tmp64.alloc(op->n_dof));
+  if (fresh) {  // the padding past n_dof stays zero
+    for (int b = 0; b < 2; ++b) CUDA_TRY(cudaMemsetAsync(op->y64[b].p, 0, len * 8, op->stream()));
+    CUDA_TRY(cudaMemsetAsync(op->p64.p, 0, len * 8, op->stream()));
+  }
+  return DGTD_OK;
+}
+
+int upload64(dgtd_op* op, const double* y) {
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, y, op->n_dof * 8, cudaMemcpyHostToDevice, op->stream()));
+  return to_soa<double, double>(op, op->tmp64.p, op->y64[op->cur64].p);
+}
+
+int download64(dgtd_op* op, const double* soa, double* y) {
+  DGTD_TRY((to_aos<double, double>(op, soa, op->tmp64.p)));
+  CUDA_TRY(cudaMemcpyAsync(y, op->tmp64.p, op->n_dof * 8, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
+  return DGTD_OK;
+}
+
+int lserk_step64(dgtd_op* op, double h, int64_t src_idx, double g, const double* src_vec) {
+  for (int s = 0; s < 5; ++s) {
+    RhsParamsT<double> P = base_params64(op);
+    P.y_in = op->y64[op->cur64].p;
+    P.out = op->y64[op->cur64 ^ 1].p;
+    P.p = op->p64.p;
+    P.a = kLserkA[s];
+    P.b = kLserkB[s];
+    P.dt = h;
+    P.read_p = s > 0;
+    P.write_p = s < 4;
+    P.src_idx = src_idx;
+    P.src_vec = src_vec;
+    P.src_g = g;
+    DGTD_TRY(launch_rhs64<kModeLserk>(op, P));
+    op->cur64 ^= 1;
+  }
+  return DGTD_OK;
+}
+
+}  // namespace
+
+extern "C" int dgtd_apply_f64(dgtd_op* op, const double* y, double* dy) {
+  if (!op || !y || !dy) return set_error(DGTD_ERR_BAD_ARG, "apply_f64: null argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  DGTD_TRY(ensure_state64(op));
+  DGTD_TRY(upload64(op, y));
+  RhsParamsT<double> P = base_params64(op);
+  P.y_in = op->y64[op->cur64].p;
+  P.out = op->y64[op->cur64 ^ 1].p;
+  DGTD_TRY(launch_rhs64<kModeApply>(op, P));
+  return download64(op, op->y64[op->cur64 ^ 1].p, dy);
+}
+
+extern "C" int dgtd_transient_f64(dgtd_op* op, const double* y0, double dt, int64_t steps, int64_t substeps,
+                                  int drive, int64_t src_dof, const double* src_vec, const double* g,
+                                  int record, double* out) {
+  if (!op || !y0 || !out || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "transient_f64: bad argument");
+  if (!(std::isfinite(dt) && dt > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "transient_f64: dt must be positive");
+  substeps = std::max<int64_t>(substeps, 1);
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  int64_t src_idx = -1;
+  if (drive == DGTD_DRIVE_POINT) {
+    if (src_dof < 0 || src_dof >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "source DOF " + std::to_string(src_dof) + " out of range");
+    src_idx = aos_to_soa_index(src_dof, op->np);
+  } else if (drive == DGTD_DRIVE_VECTOR) {
+    if (!src_vec) return set_error(DGTD_ERR_BAD_ARG, "vector drive without src_vec");
+  } else if (drive != DGTD_DRIVE_FREE) {
+    return set_error(DGTD_ERR_BAD_ARG, "unknown drive kind");
+  }
+  if (drive != DGTD_DRIVE_FREE && !g && steps > 0) return set_error(DGTD_ERR_BAD_ARG, "a driven run needs waveform samples");
+  DGTD_TRY(ensure_state64(op));
+  const double* sv = nullptr;
+  if (drive == DGTD_DRIVE_VECTOR) {
+    DGTD_TRY(op->src_vec64.alloc(state_len(op)));
+    CUDA_TRY(cudaMemsetAsync(op->src_vec64.p, 0, state_len(op) * 8, op->stream()));
+    CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, src_vec, op->n_dof * 8, cudaMemcpyHostToDevice, op->stream()));
+    DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->src_vec64.p)));
+    sv = op->src_vec64.p;
+  }
+  DGTD_TRY(upload64(op, y0));
+  const double h = dt / (double)substeps;
+  if (record) std::memcpy(out, y0, op->n_dof * 8);
+  for (int64_t k = 0; k < steps; ++k) {
+    for (int64_t j = 0; j < substeps; ++j) {
+      const double gk = drive == DGTD_DRIVE_FREE ? 0.0 : g[k * substeps + j];
+      DGTD_TRY(lserk_step64(op, h, src_idx, gk, sv));
+    }
+    if (record) DGTD_TRY(download64(op, op->y64[op->cur64].p, out + (k + 1) * op->n_dof));
+  }
+  if (!record) DGTD_TRY(download64(op, op->y64[op->cur64].p, out));
   return DGTD_OK;
 }
 

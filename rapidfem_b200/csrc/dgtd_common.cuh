@@ -40,33 +40,41 @@ enum RhsMode : int {
   kModeArnoldi = 2,  // out64 = dy + s*b64 (f64 SoA), input f64 SoA
 };
 
-struct OpTables {
-  const float* dT;        // 3*Np*Np
-  const float* liftT;     // 4Nfp*Np
+template <class R>
+struct OpTablesT {
+  const R* dT;            // 3*Np*Np
+  const R* liftT;         // 4Nfp*Np
   const uint8_t* fnodes;  // 4*Nfp
   const uint8_t* gtab;    // n_gather*Nfp
   int n_gather;
 };
+using OpTables = OpTablesT<float>;
 
-struct RhsParams {
-  const float* y_in;       // f32 state (modes Apply/Lserk)
+// Launch parameters of the RHS kernels; R is the arithmetic type of the state
+// (float: the FP32 and tensor-core engines; double: the FP64 path, whose
+// element records are the same 44 words stored as doubles, integer words as
+// exact double values).
+template <class R>
+struct RhsParamsT {
+  const R* y_in;           // state (modes Apply/Lserk)
   const double* y_in64;    // f64 input (mode Arnoldi)
-  float* out;              // Apply: dy ; Lserk: y_out
+  R* out;                  // Apply: dy ; Lserk: y_out
   double* out64;           // Arnoldi: w
-  float* p;                // Lserk residual register
-  const float* meta;
-  const float* src_vec;    // Lserk DRIVE_VECTOR pattern (SoA f32) or null
+  R* p;                    // Lserk residual register
+  const R* meta;
+  const R* src_vec;        // Lserk DRIVE_VECTOR pattern (SoA) or null
   const double* src64;     // Arnoldi augmented column b (SoA f64) or null
   const double* aug_s;     // Arnoldi: device scalar s_j (augmented component), or null
   const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop,
                            // adaptive attempts past the end of a run)
   int64_t n_elem;
   int64_t src_idx;         // Lserk DRIVE_POINT: SoA index, or -1
-  float src_g;             // held waveform value of the step
-  float a, b, dt;          // LSERK stage coefficients
+  R src_g;                 // held waveform value of the step
+  R a, b, dt;              // LSERK stage coefficients
   int read_p, write_p;     // stage 0 does not read p; the last stage does not write it
-  float alpha;             // flux blend
+  R alpha;                 // flux blend
   unsigned long long* phase_clk;  // per-phase cycle counters (instrumented builds only), or null
 };
+using RhsParams = RhsParamsT<float>;
 
 }  // namespace dgtd

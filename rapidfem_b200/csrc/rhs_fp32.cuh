@@ -1,4 +1,6 @@
-// rhs_fp32.cuh -- fused DG Maxwell right-hand side on the CUDA cores (FP32).
+// rhs_fp32.cuh -- fused DG Maxwell right-hand side on the CUDA cores, in FP32
+// (rhs_fp32_kernel, the FP32 engine and the Arnoldi matvec) or FP64
+// (rhs_fp64_kernel, the FP64 path: f64 operators, element records and state).
 //
 // One persistent CTA per SM slot walks tiles of E elements.  Per tile:
 //   1. the y tile (E*6*Np floats, contiguous in the SoA layout) and the element
@@ -20,7 +22,7 @@
 
 namespace dgtd {
 
-template <int N>
+template <int N, class R = float>
 struct Fp32Cfg {
   static constexpr int NP = np_of(N);
   static constexpr int NFP = nfp_of(N);
@@ -28,41 +30,55 @@ struct Fp32Cfg {
   // Elements per tile: ~256 threads, E even so the tile start stays 16B aligned.
   static constexpr int E = N == 1 ? 64 : N == 2 ? 24 : N == 3 ? 12 : N == 4 ? 8 : 4;
   static constexpr int THREADS = ((E * NP + 31) / 32) * 32;
-  static constexpr int TILE = E * 6 * NP;  // floats of state per tile
-  // shared memory layout (floats); every region starts on a 16-byte boundary
-  // because the state tile and the element records are filled with float4.
-  static constexpr int al4(int x) { return (x + 3) & ~3; }
+  static constexpr int TILE = E * 6 * NP;  // values of state per tile
+  // shared memory layout (in R); every region starts on a 16-byte boundary
+  // because the state tile and the element records are filled with 16-byte
+  // vectors (4 floats or 2 doubles).
+  static constexpr int PER16 = 16 / (int)sizeof(R);
+  static constexpr int al4(int x) { return (x + PER16 - 1) / PER16 * PER16; }
   static constexpr int OFF_D = 0;
   static constexpr int OFF_L = al4(OFF_D + 3 * NP * NP);
   static constexpr int OFF_Y = al4(OFF_L + NF * NP);
   static constexpr int OFF_F = al4(OFF_Y + TILE);
   static constexpr int OFF_M = al4(OFF_F + E * 6 * NF);
-  static constexpr int OFF_B = al4(OFF_M + E * kMetaWords);  // byte tables start (as floats)
+  static constexpr int OFF_B = al4(OFF_M + E * kMetaWords);  // byte tables start (in R)
   static constexpr int BYTES_TAB = 4 * NFP + kMaxGather * NFP;
-  static constexpr int SMEM = OFF_B * 4 + ((BYTES_TAB + 15) / 16) * 16;
-  static_assert(OFF_Y % 4 == 0 && OFF_M % 4 == 0, "float4 regions must be 16-byte aligned");
-  static_assert((TILE % 4) == 0 || (E % 2) == 0, "tile start must stay 16-byte aligned");
-  static_assert(((E * 6 * NP) % 4) == 0, "consecutive tiles must start 16-byte aligned");
+  static constexpr int SMEM = OFF_B * (int)sizeof(R) + ((BYTES_TAB + 15) / 16) * 16;
+  static_assert(OFF_Y % PER16 == 0 && OFF_M % PER16 == 0, "vector regions must be 16-byte aligned");
+  static_assert(((E * 6 * NP) % PER16) == 0, "consecutive tiles must start 16-byte aligned");
+  static_assert((kMetaWords % PER16) == 0, "element records are whole 16-byte vectors");
 };
 
-__device__ __forceinline__ void cross3f(float ax, float ay, float az, float bx, float by, float bz,
-                                        float& ox, float& oy, float& oz) {
+template <class R> struct Vec16;
+template <> struct Vec16<float> { using T = float4; };
+template <> struct Vec16<double> { using T = double2; };
+
+// Integer words of an element record: bit patterns in the f32 records, exact
+// values in the f64 records.
+__device__ __forceinline__ int rec_int(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int rec_int(double v) { return (int)v; }
+__device__ __forceinline__ uint32_t rec_uint(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ uint32_t rec_uint(double v) { return (uint32_t)v; }
+
+template <class R>
+__device__ __forceinline__ void cross3f(R ax, R ay, R az, R bx, R by, R bz, R& ox, R& oy, R& oz) {
   ox = ay * bz - az * by;
   oy = az * bx - ax * bz;
   oz = ax * by - ay * bx;
 }
 
-template <int N, int MODE>
-__global__ void __launch_bounds__(Fp32Cfg<N>::THREADS)
-rhs_fp32_kernel(RhsParams P, OpTables T) {
-  using C = Fp32Cfg<N>;
+template <int N, int MODE, class R>
+__device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTablesT<R>& T) {
+  using C = Fp32Cfg<N, R>;
+  using V = typename Vec16<R>::T;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, E = C::E;
-  extern __shared__ __align__(16) float smem[];
-  float* sD = smem + C::OFF_D;
-  float* sL = smem + C::OFF_L;
-  float* sY = smem + C::OFF_Y;
-  float* sF = smem + C::OFF_F;
-  float* sM = smem + C::OFF_M;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* smem = reinterpret_cast<R*>(smem_raw);
+  R* sD = smem + C::OFF_D;
+  R* sL = smem + C::OFF_L;
+  R* sY = smem + C::OFF_Y;
+  R* sF = smem + C::OFF_F;
+  R* sM = smem + C::OFF_M;
   uint8_t* sFn = reinterpret_cast<uint8_t*>(smem + C::OFF_B);
   uint8_t* sG = sFn + 4 * NFP;
   const int tid = threadIdx.x;
@@ -90,21 +106,21 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
     const int nfloat = ne * 6 * NP;
     if (MODE == kModeArnoldi) {
       const double* src = P.y_in64 + e0 * 6 * NP;
-      for (int i = tid; i < nfloat; i += blockDim.x) sY[i] = (float)src[i];
+      for (int i = tid; i < nfloat; i += blockDim.x) sY[i] = (R)src[i];
     } else {
-      const float* src = P.y_in + e0 * 6 * NP;
-      if ((nfloat & 3) == 0) {
-        const float4* s4 = reinterpret_cast<const float4*>(src);
-        float4* d4 = reinterpret_cast<float4*>(sY);
-        for (int i = tid; i < nfloat / 4; i += blockDim.x) d4[i] = __ldg(s4 + i);
+      const R* src = P.y_in + e0 * 6 * NP;
+      if ((nfloat % C::PER16) == 0) {
+        const V* s4 = reinterpret_cast<const V*>(src);
+        V* d4 = reinterpret_cast<V*>(sY);
+        for (int i = tid; i < nfloat / C::PER16; i += blockDim.x) d4[i] = __ldg(s4 + i);
       } else {
         for (int i = tid; i < nfloat; i += blockDim.x) sY[i] = __ldg(src + i);
       }
     }
     {
-      const float4* m4 = reinterpret_cast<const float4*>(P.meta + e0 * kMetaWords);
-      float4* d4 = reinterpret_cast<float4*>(sM);
-      for (int i = tid; i < ne * kMetaWords / 4; i += blockDim.x) d4[i] = __ldg(m4 + i);
+      const V* m4 = reinterpret_cast<const V*>(P.meta + e0 * kMetaWords);
+      V* d4 = reinterpret_cast<V*>(sM);
+      for (int i = tid; i < ne * kMetaWords / C::PER16; i += blockDim.x) d4[i] = __ldg(m4 + i);
     }
     __syncthreads();
 
@@ -114,43 +130,43 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
       const int s = q - le * NF;
       const int f = s / NFP;
       const int m = s - f * NFP;
-      const float* M = sM + le * kMetaWords;
-      const float nx = M[9 + 3 * f], ny = M[10 + 3 * f], nz = M[11 + 3 * f];
-      const float coef = 0.5f * M[21 + f];
-      const int nbr = __float_as_int(M[37 + f]);
-      const uint32_t codes = __float_as_uint(M[41 + (f >> 1)]);
+      const R* M = sM + le * kMetaWords;
+      const R nx = M[9 + 3 * f], ny = M[10 + 3 * f], nz = M[11 + 3 * f];
+      const R coef = R(0.5) * M[21 + f];
+      const int nbr = rec_int(M[37 + f]);
+      const uint32_t codes = rec_uint(M[41 + (f >> 1)]);
       const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
       const int kind = (code >> 8) & 3;
       const int vi = sFn[f * NFP + m];
-      const float* Y = sY + le * 6 * NP;
-      const float ex = Y[0 * NP + vi], ey = Y[1 * NP + vi], ez = Y[2 * NP + vi];
-      const float hx = Y[3 * NP + vi], hy = Y[4 * NP + vi], hz = Y[5 * NP + vi];
-      float jex, jey, jez, jhx, jhy, jhz;
-      float a = P.alpha;
+      const R* Y = sY + le * 6 * NP;
+      const R ex = Y[0 * NP + vi], ey = Y[1 * NP + vi], ez = Y[2 * NP + vi];
+      const R hx = Y[3 * NP + vi], hy = Y[4 * NP + vi], hz = Y[5 * NP + vi];
+      R jex, jey, jez, jhx, jhy, jhz;
+      R a = P.alpha;
       if (kind == kPort) {
         // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
         jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
-        a = 1.0f;
+        a = R(1);
       } else if (kind == kPec) {
         // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
-        const float edn = nx * ex + ny * ey + nz * ez;
-        const float hdn = nx * hx + ny * hy + nz * hz;
-        jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
-        jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
+        const R edn = nx * ex + ny * ey + nz * ez;
+        const R hdn = nx * hx + ny * hy + nz * hz;
+        jex = R(2) * (ex - edn * nx); jey = R(2) * (ey - edn * ny); jez = R(2) * (ez - edn * nz);
+        jhx = R(2) * (hdn * nx); jhy = R(2) * (hdn * ny); jhz = R(2) * (hdn * nz);
       } else {
         const int vj = sG[(code & 0xff) * NFP + m];
         const int64_t lo = (int64_t)nbr - e0;
-        float px, py, pz, qx, qy, qz;
+        R px, py, pz, qx, qy, qz;
         if (lo >= 0 && lo < ne) {
-          const float* Z = sY + lo * 6 * NP;
+          const R* Z = sY + lo * 6 * NP;
           px = Z[0 * NP + vj]; py = Z[1 * NP + vj]; pz = Z[2 * NP + vj];
           qx = Z[3 * NP + vj]; qy = Z[4 * NP + vj]; qz = Z[5 * NP + vj];
         } else if (MODE == kModeArnoldi) {
           const double* Z = P.y_in64 + (int64_t)nbr * 6 * NP;
-          px = (float)Z[0 * NP + vj]; py = (float)Z[1 * NP + vj]; pz = (float)Z[2 * NP + vj];
-          qx = (float)Z[3 * NP + vj]; qy = (float)Z[4 * NP + vj]; qz = (float)Z[5 * NP + vj];
+          px = (R)Z[0 * NP + vj]; py = (R)Z[1 * NP + vj]; pz = (R)Z[2 * NP + vj];
+          qx = (R)Z[3 * NP + vj]; qy = (R)Z[4 * NP + vj]; qz = (R)Z[5 * NP + vj];
         } else {
-          const float* Z = P.y_in + (int64_t)nbr * 6 * NP;
+          const R* Z = P.y_in + (int64_t)nbr * 6 * NP;
           px = __ldg(Z + 0 * NP + vj); py = __ldg(Z + 1 * NP + vj); pz = __ldg(Z + 2 * NP + vj);
           qx = __ldg(Z + 3 * NP + vj); qy = __ldg(Z + 4 * NP + vj); qz = __ldg(Z + 5 * NP + vj);
         }
@@ -158,12 +174,12 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
         jhx = hx - qx; jhy = hy - qy; jhz = hz - qz;
       }
       // n x [H], n x [E], n x (n x [E]), n x (n x [H])   (rhs.rs:1420-1432)
-      float nhx, nhy, nhz, nex, ney, nez, pex, pey, pez, phx, phy, phz;
+      R nhx, nhy, nhz, nex, ney, nez, pex, pey, pez, phx, phy, phz;
       cross3f(nx, ny, nz, jhx, jhy, jhz, nhx, nhy, nhz);
       cross3f(nx, ny, nz, jex, jey, jez, nex, ney, nez);
       cross3f(nx, ny, nz, nex, ney, nez, pex, pey, pez);
       cross3f(nx, ny, nz, nhx, nhy, nhz, phx, phy, phz);
-      float* F = sF + le * 6 * NF;
+      R* F = sF + le * 6 * NF;
       F[0 * NF + s] = coef * (-nhx + a * pex);
       F[1 * NF + s] = coef * (-nhy + a * pey);
       F[2 * NF + s] = coef * (-nhz + a * pez);
@@ -173,16 +189,16 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
     }
 
     // ---- 3. volume term: reference derivatives of E and H at my node
-    float dex = 0.f, dey = 0.f, dez = 0.f, dhx = 0.f, dhy = 0.f, dhz = 0.f;
+    R dex = 0, dey = 0, dez = 0, dhx = 0, dhy = 0, dhz = 0;
     const bool active = owns && le_me < ne;
     if (active) {
-      const float* Y = sY + le_me * 6 * NP;
-      float r[3][6];
+      const R* Y = sY + le_me * 6 * NP;
+      R r[3][6];
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 6; ++c) r[k][c] = 0.f;
-      if constexpr (N == 5) {
+        for (int c = 0; c < 6; ++c) r[k][c] = 0;
+      if constexpr (N == 5 && sizeof(R) == 4) {
         // the element's state rows are 16-byte aligned (Np = 56): four nodes of
         // all six components per float4 (broadcast) load, same accumulation
         // order (order 5: 14 % faster; orders 3 and 4 measured no gain)
@@ -209,24 +225,24 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
       } else {
 #pragma unroll 5
         for (int j = 0; j < NP; ++j) {
-          const float d0 = sD[(0 * NP + j) * NP + i_me];
-          const float d1 = sD[(1 * NP + j) * NP + i_me];
-          const float d2 = sD[(2 * NP + j) * NP + i_me];
+          const R d0 = sD[(0 * NP + j) * NP + i_me];
+          const R d1 = sD[(1 * NP + j) * NP + i_me];
+          const R d2 = sD[(2 * NP + j) * NP + i_me];
 #pragma unroll
           for (int c = 0; c < 6; ++c) {
-            const float v = Y[c * NP + j];
-            r[0][c] = fmaf(d0, v, r[0][c]);
-            r[1][c] = fmaf(d1, v, r[1][c]);
-            r[2][c] = fmaf(d2, v, r[2][c]);
+            const R v = Y[c * NP + j];
+            r[0][c] = fma(d0, v, r[0][c]);
+            r[1][c] = fma(d1, v, r[1][c]);
+            r[2][c] = fma(d2, v, r[2][c]);
           }
         }
       }
       // physical derivatives pd[p][c] = sum_k Jinv[k][p] r[k][c] (rhs.rs:62-75)
-      const float* M = sM + le_me * kMetaWords;
-      float pd[3][6];
+      const R* M = sM + le_me * kMetaWords;
+      R pd[3][6];
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
-        const float j0 = M[0 * 3 + p], j1 = M[1 * 3 + p], j2 = M[2 * 3 + p];
+        const R j0 = M[0 * 3 + p], j1 = M[1 * 3 + p], j2 = M[2 * 3 + p];
 #pragma unroll
         for (int c = 0; c < 6; ++c) pd[p][c] = j0 * r[0][c] + j1 * r[1][c] + j2 * r[2][c];
       }
@@ -242,12 +258,12 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
 
     // ---- 4. LIFT, materials, epilogue
     if (active) {
-      const float* F = sF + le_me * 6 * NF;
+      const R* F = sF + le_me * 6 * NF;
       // order 5: the element's flux rows (NF = 4 Nfp values each) are 16-byte
       // aligned, so four face nodes of all six components come per float4
       // (broadcast) load; same accumulation order
       static_assert(NF % 4 == 0, "flux rows are whole float4s");
-      if constexpr (N == 5) {
+      if constexpr (N == 5 && sizeof(R) == 4) {
 #pragma unroll 2
       for (int s0 = 0; s0 < NF; s0 += 4) {
         float4 fv[6];
@@ -268,18 +284,18 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
       } else {
 #pragma unroll 4
         for (int s = 0; s < NF; ++s) {
-          const float w = sL[s * NP + i_me];
-          dex = fmaf(w, F[0 * NF + s], dex);
-          dey = fmaf(w, F[1 * NF + s], dey);
-          dez = fmaf(w, F[2 * NF + s], dez);
-          dhx = fmaf(w, F[3 * NF + s], dhx);
-          dhy = fmaf(w, F[4 * NF + s], dhy);
-          dhz = fmaf(w, F[5 * NF + s], dhz);
+          const R w = sL[s * NP + i_me];
+          dex = fma(w, F[0 * NF + s], dex);
+          dey = fma(w, F[1 * NF + s], dey);
+          dez = fma(w, F[2 * NF + s], dez);
+          dhx = fma(w, F[3 * NF + s], dhx);
+          dhy = fma(w, F[4 * NF + s], dhy);
+          dhz = fma(w, F[5 * NF + s], dhz);
         }
       }
-      const float* M = sM + le_me * kMetaWords;
-      const float* Y = sY + le_me * 6 * NP;
-      float dy[6];
+      const R* M = sM + le_me * kMetaWords;
+      const R* Y = sY + le_me * 6 * NP;
+      R dy[6];
       dy[0] = M[25] * dex - M[31] * Y[0 * NP + i_me];
       dy[1] = M[26] * dey - M[32] * Y[1 * NP + i_me];
       dy[2] = M[27] * dez - M[33] * Y[2 * NP + i_me];
@@ -294,13 +310,13 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
           const int64_t g = base + c * NP;
-          float k = dy[c];
-          if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g), k);
+          R k = dy[c];
+          if (P.src_vec != nullptr) k = fma(P.src_g, __ldg(P.src_vec + g), k);
           if (g == P.src_idx) k += P.src_g;
-          float pv = (P.dt * M[43]) * k;
-          if (P.read_p) pv = fmaf(P.a, P.p[g], pv);
+          R pv = (P.dt * M[43]) * k;
+          if (P.read_p) pv = fma(P.a, P.p[g], pv);
           if (P.write_p) P.p[g] = pv;
-          P.out[g] = fmaf(P.b, pv, Y[c * NP + i_me]);
+          P.out[g] = fma(P.b, pv, Y[c * NP + i_me]);
         }
       } else {
 #pragma unroll
@@ -313,6 +329,20 @@ rhs_fp32_kernel(RhsParams P, OpTables T) {
       }
     }
   }
+}
+
+// FP32 engine (and the Arnoldi matvec: f64 in/out, f32 arithmetic).
+template <int N, int MODE>
+__global__ void __launch_bounds__(Fp32Cfg<N>::THREADS) rhs_fp32_kernel(RhsParams P, OpTables T) {
+  rhs_cc_body<N, MODE, float>(P, T);
+}
+
+// FP64 path: the same algorithm with f64 operators, records and state
+// (mode Arnoldi: f64 in/out, f64 arithmetic).
+template <int N, int MODE>
+__global__ void __launch_bounds__(Fp32Cfg<N, double>::THREADS)
+rhs_fp64_kernel(RhsParamsT<double> P, OpTablesT<double> T) {
+  rhs_cc_body<N, MODE, double>(P, T);
 }
 
 }  // namespace dgtd

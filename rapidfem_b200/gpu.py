@@ -155,6 +155,33 @@ class GpuOperator:
         check(lib.dgtd_apply(self._h, y, dy))
         return dy
 
+    def apply_f64(self, y) -> np.ndarray:
+        """dy = A*y in f64 on the device (the FP64 path; rhs.rs:1246's arithmetic)."""
+        y = _f64(y)
+        self._check_len("state", y)
+        dy = np.empty_like(y)
+        check(lib.dgtd_apply_f64(self._h, y, dy))
+        return dy
+
+    def transient_f64(self, y0, dt, steps, substeps=1, drive=None, g=None, record=False) -> np.ndarray:
+        """LSERK4 transient in f64 on the device (explicit.rs:100-135): as
+        `transient`, with f64 state, step and waveform."""
+        y0 = _f64(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self._check_len("source", vec)
+        substeps = max(int(substeps), 1)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f64(g)
+            if gs.size != steps * substeps:
+                raise ValueError("wrong number of waveform samples")
+        out = np.empty(((steps + 1) * self._n) if record else self._n, dtype=np.float64)
+        check(lib.dgtd_transient_f64(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
+                                     nat.ptr(gs), 1 if record else 0, out))
+        return out.reshape(steps + 1, self._n) if record else out
+
     @staticmethod
     def _drive(drive):
         """drive: None | ('point', dof) | ('vector', b)."""
