@@ -192,6 +192,15 @@ int dgtd_apply_f64(dgtd_op *op, const double *y, double *dy);
 int dgtd_transient_f64(dgtd_op *op, const double *y0, double dt, int64_t steps, int64_t substeps,
                        int drive, int64_t src_dof, const double *src_vec, const double *g_samples,
                        int record, double *out);
+/* As dgtd_transient_f64 with the waveform sampled at the five LSERK4 stage
+ * times: g_stages[5*q + s] = g(t_q + c_s h), q the substep index, c the stage
+ * abscissae of the Carpenter-Kennedy (1994) scheme: c_0 = 0, w_0 = 1,
+ * c_{s+1} = c_s + b_s w_s, w_{s+1} = a_{s+1} w_s + 1 (the time y_{s+1} reaches
+ * for y' = 1).  No counterpart in the reference (which holds g over a step,
+ * first order in h): the fourth-order treatment of a time-dependent source. */
+int dgtd_transient_f64_stages(dgtd_op *op, const double *y0, double dt, int64_t steps, int64_t substeps,
+                              int drive, int64_t src_dof, const double *src_vec, const double *g_stages,
+                              int record, double *out);
 
 /* ---- KCL adaptive transient (gpu/operator.rs:823-893, session.rs:130-187)
  * The KCL RK4(3)5[2R+]C embedded pair with the PI step-size controller, the
@@ -234,8 +243,11 @@ int dgtd_transient_kcl_functionals(dgtd_op *op, const float *y0, float dt, int64
  * it lets a caller replay the run's exact step sequence, e.g. on a CPU path. */
 int dgtd_kcl_accepted_steps(dgtd_op *op, float *h, int32_t *frame, int64_t cap, int64_t *n_total);
 
-/* GpuOperator::expmv (gpu/operator.rs:1175): exp(t*A)*v by Arnoldi, f64 basis
- * and CGS2 on the device, sub-stepped into chunks of <= 12 (KRYLOV_CHUNK).
+/* GpuOperator::expmv (gpu/operator.rs:1175): exp(t*A)*v by Arnoldi with CGS2
+ * on the device, sub-stepped into chunks of <= 12 (KRYLOV_CHUNK).  The basis
+ * is f32 with the matvec on the op's engine and every dot product, norm and
+ * the Hessenberg exponential in f64; after dgtd_op_set_krylov_precision(op,
+ * 64) the basis and the matvec are f64 (the FP64 path).
  * With tol > 0 each chunk also stops on the a-posteriori estimate
  * h_{j+1,j}*|exp(tH)_{d-1,0}| < tol (propagator.rs:278-294); tol = 0 is the
  * reference GPU's fixed-dimension behaviour.  `dim_used` (may be NULL)
@@ -255,6 +267,32 @@ int dgtd_etd_step(dgtd_op *op, const double *y, const double *b, double h, int32
  * adaptive or learned step controller. */
 int dgtd_etd_step_est(dgtd_op *op, const double *y, const double *b, double h, int32_t m, double tol,
                       double *out, int32_t *dim_used, double *est);
+/* The ETD step with a time-varying source b*g(t0 + tau), g a polynomial over
+ * the step: g(t0 + tau) = sum_{k < n_coef} coef[k] tau^k (1 <= n_coef <= 8).
+ * Computes exp(hA)y + sum_k h^k phi_k(hA) w_k through the exponential of the
+ * (n + n_coef)-augmented matrix [[A, W], [0, J]] (J the nilpotent shift; the
+ * reference's etd_step, propagator.rs:338-373, is n_coef = 1, coef = {1}).
+ * No counterpart in the reference, which holds the source over the step.  With
+ * tol > 0 the sub-steps stop at tol/k and `est` (may be NULL) receives the
+ * summed estimate, as dgtd_etd_step_est. */
+int dgtd_etd_step_poly(dgtd_op *op, const double *y, const double *b, int32_t n_coef, const double *coef,
+                       double h, int32_t m, double tol, double *out, int32_t *dim_used, double *est);
+/* Krylov precision of dgtd_expmv / dgtd_etd_step*: 32 (f32 basis, the default)
+ * or 64 (f64 basis and FP64 matvec).  No counterpart in the reference (f64
+ * basis with an f32 matvec). */
+int dgtd_op_set_krylov_precision(dgtd_op *op, int bits);
+/* An ETD step on the resident state (f32 basis, the op's engine): the
+ * candidate exp(hA)y + sum_k h^k phi_k(hA) w_k, with the source of `drive`
+ * (DRIVE_POINT at src_dof, DRIVE_VECTOR with dgtd_set_source_vector's pattern,
+ * DRIVE_FREE: coef ignored) times the polynomial coef[n_coef] as in
+ * dgtd_etd_step_poly, is written to the op's second state buffer; `dim_used`
+ * and `est` (tol > 0; may be NULL) as dgtd_etd_step_est.  dgtd_etd_commit
+ * makes the candidate the state (an accepted step); another dgtd_etd_try
+ * replaces it (a rejected one).  No counterpart in the reference, whose
+ * etd_step copies the state to and from the host every step. */
+int dgtd_etd_try(dgtd_op *op, double h, int32_t m, double tol, int32_t n_coef, const double *coef, int drive,
+                 int64_t src_dof, int32_t *dim_used, double *est);
+int dgtd_etd_commit(dgtd_op *op);
 
 /* ---- device-resident state (no host copies) ---------------------------
  * The op owns a resident f32 state (the reference's device `y` buffer, which
@@ -269,6 +307,11 @@ int dgtd_state_store_device(dgtd_op *op, float *d_y);      /* state -> device Ao
  * g_samples on the HOST (steps entries, NULL for free). */
 int dgtd_run_lserk(dgtd_op *op, float h, int64_t steps, int drive, int64_t src_dof,
                    const float *g_samples);
+/* dgtd_run_lserk with the waveform per stage: g_stages[5*k + s] = g(t_k + c_s h)
+ * at the LSERK4 stage abscissae c_s (see dgtd_transient_f64_stages); the
+ * fourth-order treatment of a time-dependent source (no reference counterpart). */
+int dgtd_run_lserk_stages(dgtd_op *op, float h, int64_t steps, int drive, int64_t src_dof,
+                          const float *g_stages);
 /* Upload the DRIVE_VECTOR pattern (Drive::Vector, session.rs:107-114) used by
  * dgtd_run_lserk. */
 int dgtd_set_source_vector(dgtd_op *op, const double *src_vec);

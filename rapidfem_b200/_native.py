@@ -86,6 +86,7 @@ _sig("dgtd_apply", C.c_int, _vp, _pf, _pf)
 _sig("dgtd_transient", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pf)
 _sig("dgtd_apply_f64", C.c_int, _vp, _pd, _pd)
 _sig("dgtd_transient_f64", C.c_int, _vp, _pd, _f64, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pd)
+_sig("dgtd_transient_f64_stages", C.c_int, _vp, _pd, _f64, _i64, _i64, C.c_int, _i64, _vp, _vp, C.c_int, _pd)
 _sig("dgtd_transient_probes", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int, _i64, _vp, _vp, _vp,
      _i64, _vp, _vp)
 class KclController(C.Structure):
@@ -123,11 +124,17 @@ _sig("dgtd_transient_functionals", C.c_int, _vp, _pf, _f32, _i64, _i64, C.c_int,
      _vp, _vp, _vp, _vp, _vp)
 _sig("dgtd_expmv", C.c_int, _vp, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32))
 _sig("dgtd_etd_step", C.c_int, _vp, _pd, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32))
+_sig("dgtd_etd_step_poly", C.c_int, _vp, _pd, _pd, _i32, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32),
+     C.POINTER(_f64))
+_sig("dgtd_op_set_krylov_precision", C.c_int, _vp, C.c_int)
+_sig("dgtd_etd_try", C.c_int, _vp, _f64, _i32, _f64, _i32, _vp, C.c_int, _i64, C.POINTER(_i32), C.POINTER(_f64))
+_sig("dgtd_etd_commit", C.c_int, _vp)
 _sig("dgtd_state_upload", C.c_int, _vp, _pf)
 _sig("dgtd_state_download", C.c_int, _vp, _pf)
 _sig("dgtd_state_load_device", C.c_int, _vp, _vp)
 _sig("dgtd_state_store_device", C.c_int, _vp, _vp)
 _sig("dgtd_run_lserk", C.c_int, _vp, _f32, _i64, C.c_int, _i64, _vp)
+_sig("dgtd_run_lserk_stages", C.c_int, _vp, _f32, _i64, C.c_int, _i64, _vp)
 _sig("dgtd_set_source_vector", C.c_int, _vp, _pd)
 _sig("dgtd_apply_device", C.c_int, _vp, _vp, _vp)
 _sig("dgtd_op_launch_count", C.c_int, _vp, C.POINTER(_i64))

@@ -172,10 +172,12 @@ struct dgtd_op {
   int cur = 0;
   bool src_vec_set = false;
   // Krylov
-  DevBuf<double> basis, w, partials, src64, tmp64, vin64;
+  DevBuf<double> partials, tmp64, vin64;
+  DevBuf<float> kbasis32, kvec32[2], kb32;
+  DevBuf<double> kbasis64, kvec64[2], kb64, kpoly, kout64;
+  bool krylov_fp64 = false;  // host-API Krylov on the FP64 path
   DevBuf<dgtd::KrylovDev> kst;
   DevBuf<int> skip;
-  int kry_cap = 0;
   // energy: reference mass matrix (f64) and |det J| per element
   DevBuf<double> mass, absdet;
   bool has_mass = false;
@@ -197,7 +199,9 @@ struct dgtd_op {
     meta.free(); dT.free(); liftT.free(); fnodes.free(); gtab.free();
     meta64.free(); dT64.free(); liftT64.free(); y64[0].free(); y64[1].free(); p64.free(); src_vec64.free();
     y[0].free(); y[1].free(); p.free(); src_vec.free(); aos32.free();
-    basis.free(); w.free(); partials.free(); src64.free(); tmp64.free(); vin64.free();
+    partials.free(); tmp64.free(); vin64.free();
+    kbasis32.free(); kvec32[0].free(); kvec32[1].free(); kb32.free();
+    kbasis64.free(); kvec64[0].free(); kvec64[1].free(); kb64.free(); kpoly.free(); kout64.free();
     kst.free(); skip.free(); mass.free(); absdet.free();
     tc_bvol.free(); tc_blift.free(); err.free();
     kcl_ctl.free(); kcl_log.free(); kcl_bak.free(); kcl_e.free(); kcl_stage.free(); kcl_k.free(); kcl_g.free(); kcl_part.free();
@@ -382,7 +386,7 @@ int launch_rhs_tc_n(dgtd_op* op, const RhsParams& P) {
 
 template <int MODE>
 int launch_rhs(dgtd_op* op, const RhsParams& P) {
-  if constexpr (MODE == kModeApply || MODE == kModeLserk) {
+  if constexpr (MODE == kModeApply || MODE == kModeLserk || MODE == kModeKrylov) {
     if (op->engine == DGTD_ENGINE_TF32X3) {
       switch (op->order) {
         case 1: return launch_rhs_tc_n<1, MODE>(op, P);
@@ -432,7 +436,9 @@ const double kLserkB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 
 
 // One LSERK4 step of h on the resident state (explicit.rs:100-135; the
 // residual register restarts at zero each step because a_0 = 0).
-int lserk_step(dgtd_op* op, float h, int64_t src_idx, float g, const float* src_vec) {
+// g5: the waveform per stage (null: g held over the step, as the reference's
+// Source::add_to, explicit.rs:44-56).
+int lserk_step(dgtd_op* op, float h, int64_t src_idx, float g, const float* src_vec, const float* g5 = nullptr) {
   for (int s = 0; s < 5; ++s) {
     RhsParams P = base_params(op);
     P.y_in = op->y[op->cur].p;
@@ -445,7 +451,7 @@ int lserk_step(dgtd_op* op, float h, int64_t src_idx, float g, const float* src_
     P.write_p = s < 4;
     P.src_idx = src_idx;
     P.src_vec = src_vec;
-    P.src_g = g;
+    P.src_g = g5 ? g5[s] : g;
     DGTD_TRY(launch_rhs<kModeLserk>(op, P));
     op->cur ^= 1;
   }
@@ -835,6 +841,20 @@ extern "C" int dgtd_run_lserk(dgtd_op* op, float h, int64_t steps, int drive, in
   return DGTD_OK;
 }
 
+extern "C" int dgtd_run_lserk_stages(dgtd_op* op, float h, int64_t steps, int drive, int64_t src_dof,
+                                     const float* g_stages) {
+  if (!op || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_stages: bad argument");
+  if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_stages: step must be positive");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  int64_t src_idx;
+  DGTD_TRY(check_drive(op, drive, src_dof, g_stages, steps, &src_idx));
+  const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
+  static const float zero5[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int64_t k = 0; k < steps; ++k)
+    DGTD_TRY(lserk_step(op, h, src_idx, 0.f, sv, drive == DGTD_DRIVE_FREE ? zero5 : g_stages + 5 * k));
+  return DGTD_OK;
+}
+
 // Element blocks (6*Np f32, contiguous in the element-major SoA state).
 __global__ void k_gather_blocks(const float* __restrict__ y, const int64_t* __restrict__ elems, int64_t n,
                                 int bs, float* __restrict__ buf) {
@@ -1125,7 +1145,8 @@ int download64(dgtd_op* op, const double* soa, double* y) {
   return DGTD_OK;
 }
 
-int lserk_step64(dgtd_op* op, double h, int64_t src_idx, double g, const double* src_vec) {
+int lserk_step64(dgtd_op* op, double h, int64_t src_idx, double g, const double* src_vec,
+                 const double* g5 = nullptr) {
   for (int s = 0; s < 5; ++s) {
     RhsParamsT<double> P = base_params64(op);
     P.y_in = op->y64[op->cur64].p;
@@ -1138,7 +1159,7 @@ int lserk_step64(dgtd_op* op, double h, int64_t src_idx, double g, const double*
     P.write_p = s < 4;
     P.src_idx = src_idx;
     P.src_vec = src_vec;
-    P.src_g = g;
+    P.src_g = g5 ? g5[s] : g;
     DGTD_TRY(launch_rhs64<kModeLserk>(op, P));
     op->cur64 ^= 1;
   }
@@ -1159,9 +1180,10 @@ extern "C" int dgtd_apply_f64(dgtd_op* op, const double* y, double* dy) {
   return download64(op, op->y64[op->cur64 ^ 1].p, dy);
 }
 
-extern "C" int dgtd_transient_f64(dgtd_op* op, const double* y0, double dt, int64_t steps, int64_t substeps,
-                                  int drive, int64_t src_dof, const double* src_vec, const double* g,
-                                  int record, double* out) {
+namespace {
+int transient_f64_impl(dgtd_op* op, const double* y0, double dt, int64_t steps, int64_t substeps, int drive,
+                       int64_t src_dof, const double* src_vec, const double* g, bool staged, int record,
+                       double* out) {
   if (!op || !y0 || !out || steps < 0) return set_error(DGTD_ERR_BAD_ARG, "transient_f64: bad argument");
   if (!(std::isfinite(dt) && dt > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "transient_f64: dt must be positive");
   substeps = std::max<int64_t>(substeps, 1);
@@ -1191,13 +1213,31 @@ extern "C" int dgtd_transient_f64(dgtd_op* op, const double* y0, double dt, int6
   if (record) std::memcpy(out, y0, op->n_dof * 8);
   for (int64_t k = 0; k < steps; ++k) {
     for (int64_t j = 0; j < substeps; ++j) {
-      const double gk = drive == DGTD_DRIVE_FREE ? 0.0 : g[k * substeps + j];
-      DGTD_TRY(lserk_step64(op, h, src_idx, gk, sv));
+      const int64_t q = k * substeps + j;
+      if (staged) {
+        static const double zero5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        DGTD_TRY(lserk_step64(op, h, src_idx, 0.0, sv, drive == DGTD_DRIVE_FREE ? zero5 : g + 5 * q));
+      } else {
+        DGTD_TRY(lserk_step64(op, h, src_idx, drive == DGTD_DRIVE_FREE ? 0.0 : g[q], sv));
+      }
     }
     if (record) DGTD_TRY(download64(op, op->y64[op->cur64].p, out + (k + 1) * op->n_dof));
   }
   if (!record) DGTD_TRY(download64(op, op->y64[op->cur64].p, out));
   return DGTD_OK;
+}
+}  // namespace
+
+extern "C" int dgtd_transient_f64(dgtd_op* op, const double* y0, double dt, int64_t steps, int64_t substeps,
+                                  int drive, int64_t src_dof, const double* src_vec, const double* g,
+                                  int record, double* out) {
+  return transient_f64_impl(op, y0, dt, steps, substeps, drive, src_dof, src_vec, g, false, record, out);
+}
+
+extern "C" int dgtd_transient_f64_stages(dgtd_op* op, const double* y0, double dt, int64_t steps,
+                                         int64_t substeps, int drive, int64_t src_dof, const double* src_vec,
+                                         const double* g_stages, int record, double* out) {
+  return transient_f64_impl(op, y0, dt, steps, substeps, drive, src_dof, src_vec, g_stages, true, record, out);
 }
 
 // ------------------------------------------------------------------ MLP (learned ETD controller)
@@ -1676,128 +1716,229 @@ extern "C" int dgtd_transient_kcl_functionals(dgtd_op* op, const float* y0, floa
 
 namespace {
 
-int ensure_krylov(dgtd_op* op, int m) {
-  if (m > dgtd::kKrylovMaxDim) return set_error(DGTD_ERR_UNSUPPORTED, "Krylov chunk dimension above 64");
-  if (op->kry_cap < m) {
-    DGTD_TRY(op->basis.alloc((size_t)(m + 1) * op->n_dof));
-    op->kry_cap = m;
+// Krylov buffers of basis type B: the basis slots 1..chunk, two chunk
+// vectors (sub-step input/output) and the source column b, all SoA of
+// state_len (whole tensor-core tiles, zero padding).
+template <class B>
+struct KryBufs {
+  DevBuf<B>* basis;
+  DevBuf<B>* vec;  // [2]
+  DevBuf<B>* b;
+};
+template <class B>
+KryBufs<B> kry_bufs(dgtd_op* op) {
+  if constexpr (sizeof(B) == 4)
+    return {&op->kbasis32, op->kvec32, &op->kb32};
+  else
+    return {&op->kbasis64, op->kvec64, &op->kb64};
+}
+
+template <class B>
+int ensure_krylov(dgtd_op* op, int chunk) {
+  if (chunk < 1 || chunk > dgtd::kKryMaxChunk)
+    return set_error(DGTD_ERR_UNSUPPORTED, "Krylov chunk dimension outside 1..15");
+  const size_t len = state_len(op);
+  cudaStream_t s = op->stream();
+  KryBufs<B> kb = kry_bufs<B>(op);
+  if (kb.basis->n < (size_t)chunk * len) {
+    DGTD_TRY(kb.basis->alloc((size_t)chunk * len));
+    CUDA_TRY(cudaMemsetAsync(kb.basis->p, 0, kb.basis->n * sizeof(B), s));
   }
-  DGTD_TRY(op->w.alloc(op->n_dof));
-  DGTD_TRY(op->partials.alloc((size_t)dgtd::kKrylovBlocks * dgtd::kKrylovMaxDim));
+  for (int i = 0; i < 2; ++i)
+    if (kb.vec[i].n < len) {
+      DGTD_TRY(kb.vec[i].alloc(len));
+      CUDA_TRY(cudaMemsetAsync(kb.vec[i].p, 0, len * sizeof(B), s));
+    }
+  if (kb.b->n < len) {
+    DGTD_TRY(kb.b->alloc(len));
+    CUDA_TRY(cudaMemsetAsync(kb.b->p, 0, len * sizeof(B), s));
+  }
+  DGTD_TRY(op->partials.alloc((size_t)2 * dgtd::kKrylovBlocks * dgtd::kKryCols));
   DGTD_TRY(op->kst.alloc(1));
   DGTD_TRY(op->skip.alloc(1));
-  DGTD_TRY(op->vin64.alloc(op->n_dof));
+  DGTD_TRY(op->kpoly.alloc(dgtd::kAugMax));
   DGTD_TRY(op->tmp64.alloc(op->n_dof));
   static bool attr[8] = {false};  // kernel attributes are per device
   if (!attr[op->ctx->device & 7]) {
-    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
-    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_finish_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
-    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_expm_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgtd::kExpmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_kry_finish_norm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dgtd::kExpmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_kry_finish_coef, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dgtd::kExpmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(dgtd::k_expm_dense, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dgtd::kExpmSmem));
     attr[op->ctx->device & 7] = true;
   }
   return DGTD_OK;
 }
 
-// One Arnoldi chunk: out = first n components of exp(t*Aug)[v; 1] (aug) or
-// exp(t*A) v, from the SoA f64 vector `v` (device).  dim_out gets the dimension.
-int krylov_chunk(dgtd_op* op, const double* v, double t, int m, double tol, bool aug, double* out,
-                 int* dim_out, double* est_out) {
+// w = kry[0] * A v + kry[1] * b on the op's engine (f32 basis) or the FP64 path.
+template <class B>
+int kry_matvec(dgtd_op* op, const B* v, B* w, const B* bvec, int64_t src_idx, const double* kry, const int* skip) {
+  if constexpr (sizeof(B) == 4) {
+    RhsParams P = base_params(op);
+    P.y_in = v;
+    P.out = w;
+    P.src_vec = bvec;
+    P.src_idx = src_idx;
+    P.kry = kry;
+    P.skip = skip;
+    return launch_rhs<kModeKrylov>(op, P);
+  } else {
+    RhsParamsT<double> P = base_params64(op);
+    P.y_in = v;
+    P.out = w;
+    P.src_vec = bvec;
+    P.src_idx = src_idx;
+    P.kry = kry;
+    P.skip = skip;
+    return launch_rhs64<kModeKrylov>(op, P);
+  }
+}
+
+// One Arnoldi chunk from the SoA vector v (basis slot 0) into `out`: the
+// first n components of exp(t*Aug)[v; e_{P-1}/eta] (P > 0, the source
+// polynomial's coefficients in op->kpoly, shifted by `delta`) or exp(t*A) v
+// (P = 0).  The chunk's dimension and estimate are accumulated on the device
+// (KrylovDev::dim_total, est_sum); `first` starts a new accumulation.
+template <class B>
+int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, double delta, const B* bvec,
+                 int64_t src_idx, B* out, bool first) {
   using namespace dgtd;
   cudaStream_t s = op->stream();
   const int64_t n = op->n_dof;
+  const int64_t len = (int64_t)state_len(op);
   const int nb = kKrylovBlocks, nt = kKrylovThreads;
   const int gs = grid_for(n, 256, op->ctx->num_sms);
   KrylovDev* st = op->kst.p;
-  double* V = op->basis.p;
-  CUDA_TRY(cudaMemsetAsync(op->skip.p, 0, sizeof(int), s));
-  k_norm_partials<<<nb, nt, 0, s>>>(v, n, op->partials.p);
-  k_finish_start<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, t, tol, aug ? 1 : 0, m);
-  k_scale<<<gs, 256, 0, s>>>(v, n, &st->inv_beta, V, nullptr);
-  op->launches += 3;
-  CUDA_TRY(cudaGetLastError());
-  for (int j = 0; j < m; ++j) {
-    const int cols = j + 1;
-    RhsParams P = base_params(op);
-    P.y_in64 = V + (int64_t)j * n;
-    P.out64 = op->w.p;
-    P.src64 = aug ? op->src64.p : nullptr;
-    P.aug_s = aug ? &st->s[j] : nullptr;
-    P.skip = op->skip.p;
-    DGTD_TRY(launch_rhs<kModeArnoldi>(op, P));
-    k_dots<<<nb, nt, 0, s>>>(V, n, cols, op->w.p, op->partials.p, op->skip.p);
-    k_finish_proj<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, j, 1, op->skip.p);
-    k_update<<<nb, nt, 0, s>>>(V, n, cols, st->proj, op->w.p, nullptr, op->skip.p);
-    k_dots<<<nb, nt, 0, s>>>(V, n, cols, op->w.p, op->partials.p, op->skip.p);
-    k_finish_proj<<<1, kExpmThreads, 0, s>>>(st, op->partials.p, nb, j, 0, op->skip.p);
-    k_update<<<nb, nt, 0, s>>>(V, n, cols, st->proj, op->w.p, op->partials.p, op->skip.p);
-    k_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, op->partials.p, nb, j, op->skip.p);
-    k_scale<<<gs, 256, 0, s>>>(op->w.p, n, &st->inv_h, V + (int64_t)(j + 1) * n, op->skip.p);
-    op->launches += 8;
-    CUDA_TRY(cudaGetLastError());
-  }
-  k_finish_coef<<<1, kExpmThreads, kExpmSmem, s>>>(st);
-  k_lincomb<<<gs, 256, 0, s>>>(V, n, st, out);
+  B* vb = kry_bufs<B>(op).basis->p;
+  double* pa = op->partials.p;
+  double* pb = pa + (size_t)kKrylovBlocks * kKryCols;
+  if (first) CUDA_TRY(cudaMemsetAsync(&st->dim_total, 0, sizeof(int) * 2 + sizeof(double), s));
+  k_kry_norm_partials<B><<<nb, nt, 0, s>>>(v, n, pa);
+  k_kry_start<<<1, kExpmThreads, 0, s>>>(st, pa, nb, t, tol, P, op->kpoly.p, delta, m, op->skip.p);
   op->launches += 2;
   CUDA_TRY(cudaGetLastError());
-  int dim = 0;
-  double est = -1.0;
-  CUDA_TRY(cudaMemcpyAsync(&dim, &st->dim, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(&est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  *dim_out = dim;
-  if (est_out) *est_out = est;
+  for (int j = 0; j < m; ++j) {
+    B* w = vb + (int64_t)j * len;  // slot j + 1
+    const B* vj = kry_col(v, (const B*)vb, len, j);
+    DGTD_TRY(kry_matvec<B>(op, vj, w, bvec, src_idx, st->mv, op->skip.p));
+    k_kry_dots<B><<<nb, nt, 0, s>>>(v, vb, len, n, j + 1, w, pa, op->skip.p);
+    k_kry_update_dots<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    k_kry_update_norm<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    k_kry_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, pa, nb, j, op->skip.p);
+    op->launches += 4;
+    CUDA_TRY(cudaGetLastError());
+  }
+  k_kry_finish_coef<<<1, kExpmThreads, kExpmSmem, s>>>(st);
+  k_kry_lincomb<B, B><<<gs, 256, 0, s>>>(v, vb, len, n, st, out);
+  op->launches += 2;
+  CUDA_TRY(cudaGetLastError());
   return DGTD_OK;
 }
 
-// exp(t*A)v or the ETD step, sub-stepped into ceil(m/12) chunks
-// (gpu/operator.rs:1175-1197, :1267-1291).
-// With split_tol each of the k sub-steps runs to tol/k, so that the summed
-// estimate of a step whose sub-steps all converged stays within tol.
-int krylov_run(dgtd_op* op, const double* v_host, const double* b_host, double t, int m, double tol,
-               double* out_host, int* dim_used, double* est_sum = nullptr, bool split_tol = false) {
-  if (m < 1) return set_error(DGTD_ERR_BAD_ARG, "Krylov dimension must be >= 1");
-  if (!std::isfinite(t)) return set_error(DGTD_ERR_BAD_ARG, "Krylov time must be finite");
-  CUDA_TRY(cudaSetDevice(op->ctx->device));
+// KRYLOV_CHUNK sub-stepping (gpu/operator.rs:1175-1197, :1267-1291): k =
+// ceil(m/12) chunks of dimension ceil(m/k), each over t/k.  From the SoA
+// vector `in` (not modified) into `out` (may not alias `in`).  With split_tol
+// each sub-step runs to tol/k, so that the summed estimate of a step whose
+// sub-steps all converged stays within tol.  dim/est (may be null) receive the
+// summed dimension and estimate (-1 when no estimate was formed).
+template <class B>
+int krylov_steps(dgtd_op* op, const B* in, B* out, double t, int m, double tol, int P, const B* bvec,
+                 int64_t src_idx, bool split_tol, int* dim, double* est) {
   const int kchunk = 12;
   const int k = std::max(1, (m + kchunk - 1) / kchunk);
   const int chunk = (m + k - 1) / k;
-  DGTD_TRY(ensure_krylov(op, chunk));
-  cudaStream_t s = op->stream();
-  const int64_t n = op->n_dof;
-  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, v_host, n * 8, cudaMemcpyHostToDevice, s));
-  DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->vin64.p)));
-  const bool aug = b_host != nullptr;
-  if (aug) {
-    DGTD_TRY(op->src64.alloc(n));
-    CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, b_host, n * 8, cudaMemcpyHostToDevice, s));
-    DGTD_TRY((to_soa<double, double>(op, op->tmp64.p, op->src64.p)));
-  }
+  DGTD_TRY(ensure_krylov<B>(op, chunk));
+  B* mid = kry_bufs<B>(op).vec[1].p;
   const double tau = t / (double)k;
-  int total = 0;
-  double esum = 0.0;
+  const B* cur = in;
   for (int q = 0; q < k; ++q) {
-    int d = 0;
-    double e = -1.0;
-    DGTD_TRY(krylov_chunk(op, op->vin64.p, tau, chunk, split_tol ? tol / (double)k : tol, aug, op->w.p, &d, &e));
-    total += d;
-    esum = (e < 0.0 || esum < 0.0) ? -1.0 : esum + e;
-    CUDA_TRY(cudaMemcpyAsync(op->vin64.p, op->w.p, n * 8, cudaMemcpyDeviceToDevice, s));
+    B* dst = ((k - 1 - q) % 2 == 0) ? out : mid;
+    DGTD_TRY(krylov_chunk<B>(op, cur, tau, chunk, split_tol ? tol / (double)k : tol, P, q * tau, bvec, src_idx, dst,
+                             q == 0));
+    cur = dst;
   }
-  DGTD_TRY((to_aos<double, double>(op, op->vin64.p, op->tmp64.p)));
-  CUDA_TRY(cudaMemcpyAsync(out_host, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  if (dim_used) *dim_used = total;
-  if (est_sum) *est_sum = esum;
+  if (dim || est) {
+    struct {
+      int dim_total, est_none;
+      double est_sum;
+    } acc;
+    CUDA_TRY(cudaMemcpyAsync(&acc, &op->kst.p->dim_total, sizeof(acc), cudaMemcpyDeviceToHost, op->stream()));
+    CUDA_TRY(cudaStreamSynchronize(op->stream()));
+    if (dim) *dim = acc.dim_total;
+    if (est) *est = acc.est_none ? -1.0 : acc.est_sum;
+  }
   return DGTD_OK;
 }
 
+int set_poly(dgtd_op* op, int P, const double* a) {
+  if (P < 0 || P > dgtd::kAugMax) return set_error(DGTD_ERR_BAD_ARG, "source polynomial: 0..8 coefficients");
+  for (int q = 0; q < P; ++q)
+    if (!std::isfinite(a[q])) return set_error(DGTD_ERR_BAD_ARG, "source polynomial: non-finite coefficient");
+  double buf[dgtd::kAugMax] = {0};
+  for (int q = 0; q < P; ++q) buf[q] = a[q];
+  CUDA_TRY(cudaMemcpyAsync(op->kpoly.p, buf, sizeof(buf), cudaMemcpyHostToDevice, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));  // buf is on the host stack
+  return DGTD_OK;
+}
+
+// Host API: exp(t*A)v, or the ETD step with the source b*g(t0+tau), g a
+// polynomial of P coefficients (host f64 AoS in and out).
+template <class B>
+int krylov_run_t(dgtd_op* op, const double* v_host, const double* b_host, int P, const double* a, double t, int m,
+                 double tol, double* out_host, int* dim_used, double* est_sum, bool split_tol) {
+  cudaStream_t s = op->stream();
+  const int64_t n = op->n_dof;
+  const int k = std::max(1, (m + 11) / 12);
+  DGTD_TRY(ensure_krylov<B>(op, (m + k - 1) / k));
+  KryBufs<B> kb = kry_bufs<B>(op);
+  CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, v_host, n * 8, cudaMemcpyHostToDevice, s));
+  DGTD_TRY((to_soa<double, B>(op, op->tmp64.p, kb.vec[0].p)));
+  const B* bvec = nullptr;
+  if (b_host) {
+    CUDA_TRY(cudaStreamSynchronize(s));  // tmp64 is reused
+    CUDA_TRY(cudaMemcpyAsync(op->tmp64.p, b_host, n * 8, cudaMemcpyHostToDevice, s));
+    DGTD_TRY((to_soa<double, B>(op, op->tmp64.p, kb.b->p)));
+    bvec = kb.b->p;
+  }
+  DGTD_TRY(set_poly(op, b_host ? P : 0, a));
+  // the result: a buffer of state_len doubles holds either basis type
+  DGTD_TRY(op->kout64.alloc(state_len(op)));
+  B* dst = reinterpret_cast<B*>(op->kout64.p);
+  int d = 0;
+  double e = -1.0;
+  DGTD_TRY(krylov_steps<B>(op, kb.vec[0].p, dst, t, m, tol, b_host ? P : 0, bvec, -1, split_tol, &d, &e));
+  DGTD_TRY((to_aos<B, double>(op, dst, op->tmp64.p)));
+  CUDA_TRY(cudaMemcpyAsync(out_host, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (dim_used) *dim_used = d;
+  if (est_sum) *est_sum = e;
+  return check_kernel_flag(op);
+}
+
+int krylov_run(dgtd_op* op, const double* v_host, const double* b_host, int P, const double* a, double t, int m,
+               double tol, double* out_host, int* dim_used, double* est_sum = nullptr, bool split_tol = false) {
+  if (m < 1) return set_error(DGTD_ERR_BAD_ARG, "Krylov dimension must be >= 1");
+  if (!std::isfinite(t)) return set_error(DGTD_ERR_BAD_ARG, "Krylov time must be finite");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (op->krylov_fp64)
+    return krylov_run_t<double>(op, v_host, b_host, P, a, t, m, tol, out_host, dim_used, est_sum, split_tol);
+  return krylov_run_t<float>(op, v_host, b_host, P, a, t, m, tol, out_host, dim_used, est_sum, split_tol);
+}
+
 }  // namespace
+
+extern "C" int dgtd_op_set_krylov_precision(dgtd_op* op, int bits) {
+  if (!op || (bits != 32 && bits != 64)) return set_error(DGTD_ERR_BAD_ARG, "set_krylov_precision: 32 or 64");
+  op->krylov_fp64 = bits == 64;
+  return DGTD_OK;
+}
 
 extern "C" int dgtd_expmv(dgtd_op* op, const double* v, double t, int32_t m, double tol, double* out,
                           int32_t* dim_used) {
   if (!op || !v || !out) return set_error(DGTD_ERR_BAD_ARG, "expmv: null argument");
   int d = 0;
-  DGTD_TRY(krylov_run(op, v, nullptr, t, m, tol, out, &d));
+  DGTD_TRY(krylov_run(op, v, nullptr, 0, nullptr, t, m, tol, out, &d));
   if (dim_used) *dim_used = d;
   return DGTD_OK;
 }
@@ -1805,8 +1946,9 @@ extern "C" int dgtd_expmv(dgtd_op* op, const double* v, double t, int32_t m, dou
 extern "C" int dgtd_etd_step(dgtd_op* op, const double* y, const double* b, double h, int32_t m,
                              double tol, double* out, int32_t* dim_used) {
   if (!op || !y || !b || !out) return set_error(DGTD_ERR_BAD_ARG, "etd_step: null argument");
+  const double one = 1.0;
   int d = 0;
-  DGTD_TRY(krylov_run(op, y, b, h, m, tol, out, &d));
+  DGTD_TRY(krylov_run(op, y, b, 1, &one, h, m, tol, out, &d));
   if (dim_used) *dim_used = d;
   return DGTD_OK;
 }
@@ -1815,9 +1957,63 @@ extern "C" int dgtd_etd_step_est(dgtd_op* op, const double* y, const double* b, 
                                  double tol, double* out, int32_t* dim_used, double* est) {
   if (!op || !y || !b || !out || !est) return set_error(DGTD_ERR_BAD_ARG, "etd_step_est: null argument");
   if (!(tol > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "etd_step_est: the estimate needs tol > 0");
+  const double one = 1.0;
   int d = 0;
-  DGTD_TRY(krylov_run(op, y, b, h, m, tol, out, &d, est, true));
+  DGTD_TRY(krylov_run(op, y, b, 1, &one, h, m, tol, out, &d, est, true));
   if (dim_used) *dim_used = d;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_etd_step_poly(dgtd_op* op, const double* y, const double* b, int32_t n_coef,
+                                  const double* coef, double h, int32_t m, double tol, double* out,
+                                  int32_t* dim_used, double* est) {
+  if (!op || !y || !b || !out || (n_coef > 0 && !coef) || n_coef < 1)
+    return set_error(DGTD_ERR_BAD_ARG, "etd_step_poly: bad argument");
+  int d = 0;
+  double e = -1.0;
+  DGTD_TRY(krylov_run(op, y, b, n_coef, coef, h, m, tol, out, &d, &e, tol > 0.0));
+  if (dim_used) *dim_used = d;
+  if (est) *est = e;
+  return DGTD_OK;
+}
+
+// ETD steps on the resident f32 state: the candidate lands in the other state
+// buffer and becomes the state on dgtd_etd_commit.
+extern "C" int dgtd_etd_try(dgtd_op* op, double h, int32_t m, double tol, int32_t n_coef, const double* coef,
+                            int drive, int64_t src_dof, int32_t* dim_used, double* est) {
+  if (!op || m < 1 || n_coef < 0 || (n_coef > 0 && !coef)) return set_error(DGTD_ERR_BAD_ARG, "etd_try: bad argument");
+  if (!(std::isfinite(h) && h > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "etd_try: step must be positive");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  int64_t src_idx = -1;
+  const float* bvec = nullptr;
+  int P = n_coef;
+  if (drive == DGTD_DRIVE_POINT) {
+    if (src_dof < 0 || src_dof >= op->n_dof) return set_error(DGTD_ERR_BAD_ARG, "etd_try: source DOF out of range");
+    src_idx = aos_to_soa_index(src_dof, op->np);
+  } else if (drive == DGTD_DRIVE_VECTOR) {
+    if (!op->src_vec_set) return set_error(DGTD_ERR_BAD_ARG, "etd_try: vector drive without a source vector");
+    bvec = op->src_vec.p;
+  } else if (drive == DGTD_DRIVE_FREE) {
+    P = 0;
+  } else {
+    return set_error(DGTD_ERR_BAD_ARG, "etd_try: unknown drive kind");
+  }
+  if (drive != DGTD_DRIVE_FREE && P < 1) return set_error(DGTD_ERR_BAD_ARG, "etd_try: a driven step needs coefficients");
+  const int k = std::max(1, (m + 11) / 12);
+  DGTD_TRY(ensure_krylov<float>(op, (m + k - 1) / k));
+  DGTD_TRY(set_poly(op, P, coef));
+  int d = 0;
+  double e = -1.0;
+  DGTD_TRY(krylov_steps<float>(op, op->y[op->cur].p, op->y[op->cur ^ 1].p, h, m, tol, P, bvec, src_idx, tol > 0.0,
+                               &d, &e));
+  if (dim_used) *dim_used = d;
+  if (est) *est = e;
+  return check_kernel_flag(op);
+}
+
+extern "C" int dgtd_etd_commit(dgtd_op* op) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "etd_commit: null op");
+  op->cur ^= 1;
   return DGTD_OK;
 }
 

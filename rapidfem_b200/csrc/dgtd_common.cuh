@@ -37,7 +37,8 @@ __host__ __device__ constexpr int nfp_of(int n) { return (n + 1) * (n + 2) / 2; 
 enum RhsMode : int {
   kModeApply = 0,    // out = dy (f32 SoA)
   kModeLserk = 1,    // fused LSERK4 stage: p = a*p + dt*(dy+src); y_out = y_in + b*p
-  kModeArnoldi = 2,  // out64 = dy + s*b64 (f64 SoA), input f64 SoA
+  kModeKrylov = 3,   // Krylov matvec: out = kry[0]*dy + kry[1]*b (state type in and out;
+                     // b = src_vec or the point src_idx; kry in device memory)
 };
 
 template <class R>
@@ -56,19 +57,16 @@ using OpTables = OpTablesT<float>;
 // exact double values).
 template <class R>
 struct RhsParamsT {
-  const R* y_in;           // state (modes Apply/Lserk)
-  const double* y_in64;    // f64 input (mode Arnoldi)
-  R* out;                  // Apply: dy ; Lserk: y_out
-  double* out64;           // Arnoldi: w
+  const R* y_in;           // state / stored basis vector
+  R* out;                  // Apply: dy ; Lserk: y_out ; Krylov: w
   R* p;                    // Lserk residual register
   const R* meta;
-  const R* src_vec;        // Lserk DRIVE_VECTOR pattern (SoA) or null
-  const double* src64;     // Arnoldi augmented column b (SoA f64) or null
-  const double* aug_s;     // Arnoldi: device scalar s_j (augmented component), or null
+  const R* src_vec;        // DRIVE_VECTOR pattern / Krylov source column b (SoA) or null
   const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop,
                            // adaptive attempts past the end of a run)
+  const double* kry;       // Krylov: device {input scale, source coefficient}
   int64_t n_elem;
-  int64_t src_idx;         // Lserk DRIVE_POINT: SoA index, or -1
+  int64_t src_idx;         // DRIVE_POINT (Lserk, Krylov): SoA index, or -1
   R src_g;                 // held waveform value of the step
   R a, b, dt;              // LSERK stage coefficients
   int read_p, write_p;     // stage 0 does not read p; the last stage does not write it

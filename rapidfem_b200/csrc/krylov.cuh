@@ -2,38 +2,80 @@
 //
 // Follows propagator.rs:186-326 (expmv_into) and :338-373 (etd_step_into) and
 // the reference GPU chunking of gpu/operator.rs:1175-1483, with every scalar of
-// the iteration (Hessenberg H, projections, norms, the augmented component s_j
-// of the ETD basis, the stop flag) kept in device memory.  The reference GPU
-// path downloads the projections of every CGS pass and the norm partials of
-// every step to finish them on the host (gpu/operator.rs:1399-1443); here a
-// one-block "finish" kernel does that work, so a chunk runs without a host
-// round trip.  Basis, dots and H are f64; the matvec runs through the f32 RHS
-// kernel (mode Arnoldi), reading the f64 basis vector and writing f64 w.
+// the iteration (Hessenberg H, projections, norms, the augmented components,
+// the stop flag) kept in device memory: a chunk runs without a host round trip
+// (the reference GPU path downloads the projections of every CGS pass and the
+// norm partials of every step, gpu/operator.rs:1399-1443).
 //
-// Reductions are deterministic: per-warp partials in a fixed order, then a
-// fixed-order sum over blocks.
+// Precision.  The basis is stored in the state type B: f32 for the FP32 and
+// tensor-core engines, f64 for the FP64 path.  Every dot product and norm is
+// accumulated in f64; H, the projections and the dense exponential are f64.
+//
+// Storage.  Basis vector i is sig[i] * (stored vector i): the Gram-Schmidt
+// sweeps update the working vector in place in the slot of the next basis
+// vector, and its normalisation 1/h_{j+1,j} is kept as the scale sig[j+1]
+// instead of a rescaling sweep.
+//
+// Augmented system (the ETD step with a time-polynomial source).  With the
+// source b*g(t0+tau), g(t0+tau) = sum_{m<P} a_m tau^m over the step, the
+// exponential of
+//     [[A, W], [0, J]],  W = b * (a_{P-1} (P-1)!, ..., a_1 1!, a_0 0!),
+//     J the P x P upper shift,
+// applied to [y; e_{P-1}] gives y(tau) = e^{tau A} y + sum_k tau^k
+// phi_k(tau A) w_k in its first n components (Al-Mohy & Higham, SIAM J. Sci.
+// Comput. 33 (2011), Theorem 2.1).  P = 1 with a_0 = 1 is the reference's
+// held-source step exp(h[[A, b],[0, 0]])[y; 1] (propagator.rs:338-373); P = 0
+// is expmv.  The augmented coordinates are scaled to the chunk's duration t
+// (u_q -> u_q / t^(P-1-q), so J's entries become 1/t and W's columns
+// a_{P-1-q} (P-1-q)! t^(P-1-q) b, the polynomial in scaled time) and by eta =
+// 1/max(1, max|column coefficient|) (W -> eta W, e_{P-1} -> e_{P-1}/eta), so
+// that the augmented part of the basis stays comparable to the state part.
+// A basis vector's augmented part is the P-vector s[i]; the matvec of [v; u]
+// is [A v + b*(c.u); J u] with c the scaled coefficients, so the RHS kernel
+// adds (c.u) b with one device scalar (RhsParams::kry).
+//
+// One Arnoldi step j (cols = j+1 basis vectors), five launches:
+//   RHS (mode Krylov)   w = sig_j A V_j + g_j b          (w in slot j+1)
+//   k_kry_dots          block partials of V_i . w, i <= j
+//   k_kry_update_dots   proj (every block reduces the partials itself), then
+//                       w -= sum proj_i V_i and the second pass's partials in
+//                       the same sweep (one read of each V_i)
+//   k_kry_update_norm   second-pass proj, w -= sum proj_i V_i, partials of |w|^2
+//   k_kry_finish_norm   h_{j+1,j}, breakdown / last dimension / a-posteriori
+//                       estimate h_{j+1,j}|exp(tH)_{d-1,0}| < tol (expm of H in
+//                       one block), the next scale and augmented part
+// Reductions are deterministic: fixed per-thread order, a fixed tree per
+// block, a fixed-order sum over blocks.
 #pragma once
 #include <cstdint>
 
 namespace dgtd {
 
-constexpr int kKrylovMaxDim = 64;     // per-chunk Krylov dimension cap (H is 64x64)
+constexpr int kKrylovMaxDim = 64;     // H capacity (64 x 64)
+constexpr int kKryCols = 16;          // basis vectors of one chunk in the fused sweeps (chunk dim <= 15)
+constexpr int kKryMaxChunk = kKryCols - 1;
+constexpr int kAugMax = 8;            // polynomial source terms
 constexpr int kKrylovBlocks = 296;    // persistent reduction grid (2 per SM)
 constexpr int kKrylovThreads = 256;
 
 // Device-side scalar state of one Arnoldi chunk.
 struct KrylovDev {
   double h[kKrylovMaxDim * kKrylovMaxDim];  // H, row-major, stride kKrylovMaxDim
-  double proj[kKrylovMaxDim + 1];
-  double s[kKrylovMaxDim + 1];              // augmented component of each basis vector (ETD)
-  double coef[kKrylovMaxDim];               // final combination coefficients
-  double w_s;                               // augmented component of the working vector
-  double beta, inv_beta, inv_h, t, tol;
-  double est;                               // last a-posteriori estimate (tol > 0), 0 on breakdown
+  double sig[kKryCols];                     // basis vector i = sig[i] * stored vector i
+  double s[kKryCols][kAugMax];              // augmented part of basis vector i
+  double c[kAugMax];                        // scaled W / b (augmented source coefficients)
+  double wa[3][kAugMax];                    // augmented part of w: after the matvec, pass 1, pass 2
+  double coef[kKryCols];                    // result = sum coef[i] * stored vector i
+  double mv[2];                             // next matvec: input scale, source coefficient
+  double beta, t, tol, est;
   int dim;                                  // dimension decided so far (the final one when done)
   int done;                                 // 1: stop growing the space
-  int aug;                                  // 1: ETD augmented system
+  int naug;                                 // P
   int max_dim;
+  // accumulated over the chunks of one step (cleared by the host at its first chunk)
+  int dim_total;                            // summed dimension
+  int est_none;                             // a chunk formed no estimate
+  double est_sum;                           // summed a-posteriori estimates
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -42,105 +84,175 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// partials[b*kKrylovMaxDim + i] = sum over this block's k of V_i[k]*w[k], i < cols.
-// Skipped (no writes) when *skip != 0.
-__global__ void __launch_bounds__(kKrylovThreads)
-k_dots(const double* __restrict__ V, int64_t n, int cols, const double* __restrict__ w,
-       double* __restrict__ partials, const int* skip) {
-  if (*skip) return;
-  __shared__ double acc[kKrylovMaxDim + 1][kKrylovThreads / 32];
+// Basis slot i: slot 0 is the chunk's input vector, slots 1.. are contiguous.
+template <class B>
+__device__ __forceinline__ const B* kry_col(const B* v0, const B* vb, int64_t len, int i) {
+  return i == 0 ? v0 : vb + (int64_t)(i - 1) * len;
+}
+
+// Block sums of per-thread f64 values acc[0..cols) -> out[0..cols) (thread 0).
+template <int NC>
+__device__ __forceinline__ void block_sums(double (&acc)[NC], int cols, double* red /* [NC][8] shared */,
+                                           double* out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < (kKrylovMaxDim + 1) * (kKrylovThreads / 32); i += blockDim.x)
-    (&acc[0][0])[i] = 0.0;
-  __syncthreads();
-  const int64_t wstride = (int64_t)gridDim.x * (kKrylovThreads / 32) * 32;
-  for (int64_t k0 = ((int64_t)blockIdx.x * (kKrylovThreads / 32) + warp) * 32; k0 < n; k0 += wstride) {
-    const int64_t k = k0 + lane;
-    const double wk = k < n ? w[k] : 0.0;
-    for (int i = 0; i < cols; ++i) {
-      double v = k < n ? V[(int64_t)i * n + k] * wk : 0.0;
-      v = warp_sum(v);
-      if (lane == 0) acc[i][warp] += v;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+    if (i < cols) {
+      const double v = warp_sum(acc[i]);
+      if (lane == 0) red[i * (kKrylovThreads / 32) + warp] = v;
     }
-  }
   __syncthreads();
-  for (int i = threadIdx.x; i < cols; i += blockDim.x) {
+  if (threadIdx.x < cols) {
     double s = 0.0;
-    for (int q = 0; q < kKrylovThreads / 32; ++q) s += acc[i][q];
-    partials[(int64_t)blockIdx.x * kKrylovMaxDim + i] = s;
+    for (int q = 0; q < kKrylovThreads / 32; ++q) s += red[threadIdx.x * (kKrylovThreads / 32) + q];
+    out[threadIdx.x] = s;
   }
 }
 
-// w -= sum_i coef[i]*V_i (coef from device), optional partial sum of w^2 into
-// partials[b*kKrylovMaxDim + 0].
+// partials[b*kKryCols + i] = sum over this block's k of V_i[k] * w[k], i < cols.
+template <class B>
 __global__ void __launch_bounds__(kKrylovThreads)
-k_update(const double* __restrict__ V, int64_t n, int cols, const double* __restrict__ coef,
-         double* __restrict__ w, double* __restrict__ norm_partials, const int* skip) {
+k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, int cols,
+           const B* __restrict__ w, double* __restrict__ partials, const int* skip) {
   if (*skip) return;
-  __shared__ double c[kKrylovMaxDim];
-  __shared__ double acc[kKrylovThreads / 32];
-  for (int i = threadIdx.x; i < cols; i += blockDim.x) c[i] = coef[i];
-  if (threadIdx.x < kKrylovThreads / 32) acc[threadIdx.x] = 0.0;
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double red[kKryCols * (kKrylovThreads / 32)];
+  double acc[kKryCols];
+#pragma unroll
+  for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  double sq = 0.0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    double wk = w[k];
-    for (int i = 0; i < cols; ++i) wk -= c[i] * V[(int64_t)i * n + k];
-    w[k] = wk;
-    sq += wk * wk;
+    const double wk = (double)w[k];
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < cols) acc[i] = fma((double)kry_col(v0, vb, len, i)[k], wk, acc[i]);
   }
-  if (norm_partials) {
-    sq = warp_sum(sq);
-    if (lane == 0) acc[warp] = sq;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0.0;
-      for (int q = 0; q < kKrylovThreads / 32; ++q) s += acc[q];
-      norm_partials[(int64_t)blockIdx.x * kKrylovMaxDim] = s;
+  block_sums<kKryCols>(acc, cols, red, partials + (int64_t)blockIdx.x * kKryCols);
+}
+
+// The projections of a pass from the block partials (every block computes them
+// identically): proj_i = sig_i * (sum_b partials) + s_i . wa_in.  Block 0 adds
+// them to H[:, j] and writes wa_out = wa_in - sum_i proj_i s_i.  Returns, in
+// shared u[], the update coefficients u_i = proj_i * sig_i of the stored vectors.
+__device__ __forceinline__ void kry_proj(KrylovDev* st, const double* partials, int nblocks, int j, int pass,
+                                         double* u) {
+  __shared__ double proj[kKryCols];
+  const int cols = j + 1;
+  const int P = st->naug;
+  if ((int)threadIdx.x < cols) {
+    const int i = threadIdx.x;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKryCols + i];
+    s *= st->sig[i];
+    for (int q = 0; q < P; ++q) s += st->s[i][q] * st->wa[pass][q];
+    proj[i] = s;
+    u[i] = s * st->sig[i];
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < cols; ++i) st->h[i * kKrylovMaxDim + j] += proj[i];
+    for (int q = 0; q < P; ++q) {
+      double d = st->wa[pass][q];
+      for (int i = 0; i < cols; ++i) d -= proj[i] * st->s[i][q];
+      st->wa[pass + 1][q] = d;
     }
   }
 }
 
-// partial sums of x^2 (slot 0 of each block's partial row).
+// First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
+template <class B>
 __global__ void __launch_bounds__(kKrylovThreads)
-k_norm_partials(const double* __restrict__ x, int64_t n, double* __restrict__ partials) {
-  __shared__ double acc[kKrylovThreads / 32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double sq = 0.0;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    sq += x[k] * x[k];
-  sq = warp_sum(sq);
-  if (lane == 0) acc[warp] = sq;
+k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
+                  int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
+                  double* __restrict__ partials_out, const int* skip) {
+  if (*skip) return;
+  __shared__ double u[kKryCols];
+  __shared__ double red[kKryCols * (kKrylovThreads / 32)];
+  kry_proj(st, partials_in, nb_in, j, 0, u);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int q = 0; q < kKrylovThreads / 32; ++q) s += acc[q];
-    partials[(int64_t)blockIdx.x * kKrylovMaxDim] = s;
+  const int cols = j + 1;
+  double c[kKryCols], acc[kKryCols];
+#pragma unroll
+  for (int i = 0; i < kKryCols; ++i) {
+    c[i] = i < cols ? u[i] : 0.0;
+    acc[i] = 0.0;
   }
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    B vk[kKryCols];
+    double wk = (double)w[k];
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < cols) {
+        vk[i] = kry_col(v0, vb, len, i)[k];
+        wk = fma(-c[i], (double)vk[i], wk);
+      }
+    const B wn = (B)wk;
+    w[k] = wn;
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < cols) acc[i] = fma((double)vk[i], (double)wn, acc[i]);
+  }
+  block_sums<kKryCols>(acc, cols, red, partials_out + (int64_t)blockIdx.x * kKryCols);
 }
 
-// out[k] = x[k] * (*scale)   (skipped when *skip)
-__global__ void k_scale(const double* __restrict__ x, int64_t n, const double* scale,
-                        double* __restrict__ out, const int* skip) {
-  if (skip && *skip) return;
-  const double s = *scale;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    out[k] = x[k] * s;
+// Second-pass update and the partial sums of |w|^2 (slot 0 of each block's row).
+template <class B>
+__global__ void __launch_bounds__(kKrylovThreads)
+k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
+                  int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
+                  double* __restrict__ partials_out, const int* skip) {
+  if (*skip) return;
+  __shared__ double u[kKryCols];
+  __shared__ double red[kKryCols * (kKrylovThreads / 32)];
+  kry_proj(st, partials_in, nb_in, j, 1, u);
+  __syncthreads();
+  const int cols = j + 1;
+  double c[kKryCols];
+#pragma unroll
+  for (int i = 0; i < kKryCols; ++i) c[i] = i < cols ? u[i] : 0.0;
+  double acc[1] = {0.0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    double wk = (double)w[k];
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < cols) wk = fma(-c[i], (double)kry_col(v0, vb, len, i)[k], wk);
+    const B wn = (B)wk;
+    w[k] = wn;
+    acc[0] = fma((double)wn, (double)wn, acc[0]);
+  }
+  block_sums<1>(acc, 1, red, partials_out + (int64_t)blockIdx.x * kKryCols);
 }
 
-// out[k] = sum_{i<dim} coef[i]*V_i[k], dim and coef from the device state.
-__global__ void k_lincomb(const double* __restrict__ V, int64_t n, const KrylovDev* st,
-                          double* __restrict__ out) {
-  __shared__ double c[kKrylovMaxDim];
+// Partial sums of x^2 (slot 0 of each block's row).
+template <class B>
+__global__ void __launch_bounds__(kKrylovThreads)
+k_kry_norm_partials(const B* __restrict__ x, int64_t n, double* __restrict__ partials) {
+  __shared__ double red[kKrylovThreads / 32];
+  double acc[1] = {0.0};
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const double v = (double)x[k];
+    acc[0] = fma(v, v, acc[0]);
+  }
+  block_sums<1>(acc, 1, red, partials + (int64_t)blockIdx.x * kKryCols);
+}
+
+// out[k] = sum_{i<dim} coef[i] * stored_i[k] (f64 accumulation), dim and coef
+// from the device state; O is the output type.
+template <class B, class O>
+__global__ void __launch_bounds__(kKrylovThreads)
+k_kry_lincomb(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, const KrylovDev* st,
+              O* __restrict__ out) {
+  __shared__ double c[kKryCols];
   const int dim = st->dim;
-  for (int i = threadIdx.x; i < dim; i += blockDim.x) c[i] = st->coef[i];
+  if ((int)threadIdx.x < kKryCols) c[threadIdx.x] = (int)threadIdx.x < dim ? st->coef[threadIdx.x] : 0.0;
   __syncthreads();
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int i = 0; i < dim; ++i) s += c[i] * V[(int64_t)i * n + k];
-    out[k] = s;
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < dim) s = fma(c[i], (double)kry_col(v0, vb, len, i)[k], s);
+    out[k] = (O)s;
   }
 }
 
@@ -162,10 +274,8 @@ __device__ void block_matmul(const double* A, const double* B, double* C, int d)
   }
 }
 
-// a: d*d input (shared), out: d*d result (shared), w1..w3 scratch (shared).
-__device__ void block_expm(const double* a, int d, double* out, double* b, double* term,
-                           double* term2) {
-  __shared__ double s_norm;
+// a: d*d input (shared), out: d*d result (shared), b, term, term2 scratch (shared).
+__device__ void block_expm(const double* a, int d, double* out, double* b, double* term, double* term2) {
   __shared__ int s_sq;
   if (threadIdx.x == 0) {
     double nrm = 0.0;
@@ -179,7 +289,6 @@ __device__ void block_expm(const double* a, int d, double* out, double* b, doubl
       long v = (long)ceil(log2(nrm)) + 1;
       sq = v > 0 ? (int)v : 0;
     }
-    s_norm = nrm;
     s_sq = sq;
   }
   __syncthreads();
@@ -218,75 +327,88 @@ constexpr size_t kExpmSmem = 5 * kKrylovMaxDim * kKrylovMaxDim * sizeof(double);
 // ---------------------------------------------------------------- finishers
 // All run as one block of kExpmThreads threads.
 
-// Start of a chunk: beta = sqrt(sum partials (+1 for the augmented [v;1])),
-// zero H, s[0] = 1/beta, inv_beta.
-__global__ void k_finish_start(KrylovDev* st, const double* partials, int nblocks, double t,
-                               double tol, int aug, int max_dim) {
+// Start of a chunk of duration t.  `a[P]` are the source polynomial's monomial
+// coefficients about the step start, `delta` the chunk's offset in the step:
+// the chunk's own coefficients are the Taylor shift
+// a'_m = sum_{l>=m} a_l C(l,m) delta^(l-m).  beta = |[v; e_{P-1}/eta]|,
+// sig[0] = 1/beta, s[0] = e_{P-1}/(eta beta).
+__global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, double t, double tol, int P,
+                            const double* a, double delta, int max_dim, int* skip) {
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKrylovMaxDim];
-    if (aug) s += 1.0;
-    const double beta = sqrt(s);
+    double shifted[kAugMax], cu[kAugMax];
+    double cmax = 0.0;
+    for (int m = 0; m < P; ++m) {
+      double acc = 0.0, binom = 1.0, dp = 1.0;  // C(l, m) delta^(l-m), l = m, m+1, ...
+      for (int l = m; l < P; ++l) {
+        acc += a[l] * binom * dp;
+        binom = binom * (double)(l + 1) / (double)(l + 1 - m);
+        dp *= delta;
+      }
+      shifted[m] = acc;
+    }
+    double fact = 1.0, tp = 1.0;
+    for (int k = 0; k < P; ++k) {  // c_q = a'_{P-1-q} (P-1-q)! t^(P-1-q)
+      if (k > 0) {
+        fact *= (double)k;
+        tp *= t;
+      }
+      cu[P - 1 - k] = shifted[k] * fact * tp;
+    }
+    for (int q = 0; q < P; ++q) cmax = fmax(cmax, fabs(cu[q]));
+    const double eta = 1.0 / fmax(1.0, cmax);
+    double s2 = 0.0;
+    for (int b = 0; b < nblocks; ++b) s2 += partials[(int64_t)b * kKryCols];
+    const double u_last = P > 0 ? 1.0 / eta : 0.0;
+    s2 += u_last * u_last;
+    const double beta = sqrt(s2);
     st->beta = beta;
-    st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
     st->t = t;
     st->tol = tol;
     st->est = beta == 0.0 ? 0.0 : -1.0;  // -1: no estimate formed (tol = 0)
-    st->aug = aug;
+    st->naug = P;
     st->max_dim = max_dim;
-    st->dim = max_dim;
+    st->dim = beta == 0.0 ? 0 : max_dim;
     st->done = beta == 0.0 ? 1 : 0;
-    st->w_s = 0.0;
-    for (int i = 0; i <= kKrylovMaxDim; ++i) st->s[i] = 0.0;
-    st->s[0] = aug ? st->inv_beta : 0.0;
-    if (beta == 0.0) st->dim = 0;
+    for (int i = 0; i < kKryCols; ++i) {
+      st->sig[i] = 0.0;
+      st->coef[i] = 0.0;
+      for (int q = 0; q < kAugMax; ++q) st->s[i][q] = 0.0;
+    }
+    for (int q = 0; q < kAugMax; ++q) {
+      st->c[q] = q < P ? eta * cu[q] : 0.0;
+      st->wa[0][q] = st->wa[1][q] = st->wa[2][q] = 0.0;
+    }
+    const double ib = beta > 0.0 ? 1.0 / beta : 0.0;
+    st->sig[0] = ib;
+    if (P > 0) st->s[0][P - 1] = u_last * ib;
+    // the first matvec: scale of V_0, source coefficient c . s_0; and J s_0
+    double g = 0.0;
+    for (int q = 0; q < P; ++q) g += st->c[q] * st->s[0][q];
+    st->mv[0] = ib;
+    st->mv[1] = g;
+    const double inv_t = t != 0.0 ? 1.0 / t : 0.0;  // J's scaled entries (unused when t = 0)
+    for (int q = 0; q + 1 < P; ++q) st->wa[0][q] = st->s[0][q + 1] * inv_t;
+    *skip = beta == 0.0 ? 1 : 0;
   }
   for (int i = threadIdx.x; i < kKrylovMaxDim * kKrylovMaxDim; i += blockDim.x) st->h[i] = 0.0;
 }
 
-// After a matvec: the augmented operator's last row is zero (w_s = 0).
-// After a dots pass: proj = sum partials (+ s_i*w_s), H[:,j] += proj,
-// w_s -= sum proj_i s_i (gpu/operator.rs:1399-1410; propagator.rs:236-270).
-__global__ void k_finish_proj(KrylovDev* st, const double* partials, int nblocks, int j,
-                              int reset_ws, const int* skip) {
-  if (*skip) return;
-  __shared__ double proj[kKrylovMaxDim];
-  const int cols = j + 1;
-  if (reset_ws && threadIdx.x == 0) st->w_s = 0.0;
-  __syncthreads();
-  const double ws = st->w_s;
-  for (int i = threadIdx.x; i < cols; i += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKrylovMaxDim + i];
-    if (st->aug) s += st->s[i] * ws;
-    proj[i] = s;
-    st->proj[i] = s;
-    st->h[i * kKrylovMaxDim + j] += s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && st->aug) {
-    double d = 0.0;
-    for (int i = 0; i < cols; ++i) d += proj[i] * st->s[i];
-    st->w_s = ws - d;
-  }
-}
-
-// After the second pass: hnext = ||[w; w_s]||; stop on breakdown, on the last
-// dimension, or (tol > 0) on the a-posteriori estimate
+// After the second pass: hnext = |[w; wa]|; stop on breakdown (1e-12), on the
+// last dimension, or (tol > 0) on the a-posteriori estimate
 // hnext*|exp(tH)_{d-1,0}| < tol (propagator.rs:271-301).  Otherwise record
-// H[j+1,j], inv_h and s[j+1].
-__global__ void k_finish_norm(KrylovDev* st, const double* partials, int nblocks, int j,
-                              int* skip) {
+// H[j+1,j], the scale and augmented part of V_{j+1} and the next matvec's scalars.
+__global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nblocks, int j, int* skip) {
   if (*skip) return;
   extern __shared__ double sm[];
   __shared__ double s_hnext;
   __shared__ int s_stop;
   __shared__ int s_break;
   const int d = j + 1;
+  const int P = st->naug;
   if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKrylovMaxDim];
-    if (st->aug) s += st->w_s * st->w_s;
+    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKryCols];
+    for (int q = 0; q < P; ++q) s += st->wa[2][q] * st->wa[2][q];
     s_hnext = sqrt(s);
     s_break = s_hnext < 1e-12 ? 1 : 0;
     s_stop = (s_break || d == st->max_dim) ? 1 : 0;
@@ -321,17 +443,33 @@ __global__ void k_finish_norm(KrylovDev* st, const double* partials, int nblocks
       st->done = 1;
       *skip = 1;
     } else {
+      const double ih = 1.0 / hnext;
       st->h[(j + 1) * kKrylovMaxDim + j] = hnext;
-      st->inv_h = 1.0 / hnext;
-      if (st->aug) st->s[j + 1] = st->w_s / hnext;
+      st->sig[j + 1] = ih;
+      double g = 0.0;
+      for (int q = 0; q < P; ++q) {
+        st->s[j + 1][q] = st->wa[2][q] * ih;
+        g += st->c[q] * st->s[j + 1][q];
+      }
+      st->mv[0] = ih;
+      st->mv[1] = g;
+      const double inv_t = st->t != 0.0 ? 1.0 / st->t : 0.0;
+      for (int q = 0; q < kAugMax; ++q) st->wa[0][q] = q + 1 < P ? st->s[j + 1][q + 1] * inv_t : 0.0;
     }
   }
 }
 
-// End of a chunk: coef_i = beta * exp(tH)_{i,0} over the final dim.
-__global__ void k_finish_coef(KrylovDev* st) {
+// End of a chunk: coef_i = beta * exp(tH)_{i,0} * sig_i over the final dim.
+__global__ void k_kry_finish_coef(KrylovDev* st) {
   extern __shared__ double sm[];
   const int d = st->dim;
+  if (threadIdx.x == 0) {
+    st->dim_total += d;
+    if (st->est < 0.0)
+      st->est_none = 1;
+    else
+      st->est_sum += st->est;
+  }
   if (d == 0) return;
   double* a = sm;
   double* out = a + kKrylovMaxDim * kKrylovMaxDim;
@@ -345,7 +483,7 @@ __global__ void k_finish_coef(KrylovDev* st) {
   }
   __syncthreads();
   block_expm(a, d, out, b, t1, t2);
-  for (int i = threadIdx.x; i < d; i += blockDim.x) st->coef[i] = st->beta * out[i * d];
+  for (int i = threadIdx.x; i < d; i += blockDim.x) st->coef[i] = st->beta * out[i * d] * st->sig[i];
 }
 
 // Standalone dense expm for tests: a (d*d, global) -> out (global).

@@ -13,7 +13,8 @@
 //   4. the LIFT sum over the 4*Nfp flux values (rhs.rs:1433-1439), the
 //      material scaling (rhs.rs:1443-1454), and the mode's epilogue:
 //      plain dy, the fused LSERK4 stage update (explicit.rs:122-133, so dy
-//      never reaches HBM), or the f64 Arnoldi matvec output.
+//      never reaches HBM), or the Krylov matvec output (scaled dy plus the
+//      augmented source column).
 // D and LIFT live in shared memory for the whole kernel.
 #pragma once
 #include <cstdint>
@@ -90,8 +91,11 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
   for (int i = tid; i < 4 * NFP; i += blockDim.x) sFn[i] = T.fnodes[i];
   for (int i = tid; i < T.n_gather * NFP; i += blockDim.x) sG[i] = T.gtab[i];
 
-  double aug_s = 0.0;
-  if (MODE == kModeArnoldi && P.aug_s != nullptr) aug_s = *P.aug_s;
+  R kry_sig = 1, kry_g = 0;
+  if (MODE == kModeKrylov) {
+    kry_sig = (R)P.kry[0];
+    kry_g = (R)P.kry[1];
+  }
 
   const int64_t n_tiles = (P.n_elem + E - 1) / E;
   const int le_me = tid / NP;
@@ -104,10 +108,7 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
     __syncthreads();  // previous tile fully consumed (and tables loaded on the first pass)
     // ---- 1. state tile and element records -> shared memory
     const int nfloat = ne * 6 * NP;
-    if (MODE == kModeArnoldi) {
-      const double* src = P.y_in64 + e0 * 6 * NP;
-      for (int i = tid; i < nfloat; i += blockDim.x) sY[i] = (R)src[i];
-    } else {
+    {
       const R* src = P.y_in + e0 * 6 * NP;
       if ((nfloat % C::PER16) == 0) {
         const V* s4 = reinterpret_cast<const V*>(src);
@@ -161,10 +162,6 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
           const R* Z = sY + lo * 6 * NP;
           px = Z[0 * NP + vj]; py = Z[1 * NP + vj]; pz = Z[2 * NP + vj];
           qx = Z[3 * NP + vj]; qy = Z[4 * NP + vj]; qz = Z[5 * NP + vj];
-        } else if (MODE == kModeArnoldi) {
-          const double* Z = P.y_in64 + (int64_t)nbr * 6 * NP;
-          px = (R)Z[0 * NP + vj]; py = (R)Z[1 * NP + vj]; pz = (R)Z[2 * NP + vj];
-          qx = (R)Z[3 * NP + vj]; qy = (R)Z[4 * NP + vj]; qz = (R)Z[5 * NP + vj];
         } else {
           const R* Z = P.y_in + (int64_t)nbr * 6 * NP;
           px = __ldg(Z + 0 * NP + vj); py = __ldg(Z + 1 * NP + vj); pz = __ldg(Z + 2 * NP + vj);
@@ -319,26 +316,29 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
           P.out[g] = fma(P.b, pv, Y[c * NP + i_me]);
         }
       } else {
+        // Krylov matvec of a stored basis vector: its scale and the source
+        // coefficient of the augmented system come from device memory
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
           const int64_t g = base + c * NP;
-          double w = (double)dy[c];
-          if (P.src64 != nullptr) w += aug_s * P.src64[g];
-          P.out64[g] = w;
+          R w = kry_sig * dy[c];
+          if (P.src_vec != nullptr) w = fma(kry_g, __ldg(P.src_vec + g), w);
+          if (g == P.src_idx) w += kry_g;
+          P.out[g] = w;
         }
       }
     }
   }
 }
 
-// FP32 engine (and the Arnoldi matvec: f64 in/out, f32 arithmetic).
+// FP32 engine (stage, RHS and the Krylov matvec of an f32 basis).
 template <int N, int MODE>
 __global__ void __launch_bounds__(Fp32Cfg<N>::THREADS) rhs_fp32_kernel(RhsParams P, OpTables T) {
   rhs_cc_body<N, MODE, float>(P, T);
 }
 
-// FP64 path: the same algorithm with f64 operators, records and state
-// (mode Arnoldi: f64 in/out, f64 arithmetic).
+// FP64 path: the same algorithm with f64 operators, records and state (and
+// the Krylov matvec of an f64 basis).
 template <int N, int MODE>
 __global__ void __launch_bounds__(Fp32Cfg<N, double>::THREADS)
 rhs_fp64_kernel(RhsParamsT<double> P, OpTablesT<double> T) {

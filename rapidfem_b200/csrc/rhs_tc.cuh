@@ -489,6 +489,11 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     const float e_sign = e_fld == 0 ? 1.f : -1.f;
     const int e_cA = (e_t + 2) % 3, e_cB = (e_t + 1) % 3;
     const int e_row_off = (e_le * 6 + e_c) * NP;
+    float kry_sig = 1.f, kry_g = 0.f;
+    if (MODE == kModeKrylov) {
+      kry_sig = (float)P.kry[0];
+      kry_g = (float)P.kry[1];
+    }
     int ys = 0;
     uint32_t ld_par = 0u;
     for (int64_t it = 0; it < n_my; ++it) {
@@ -517,8 +522,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       float* const prow = sP0 + ps * kYStride + e_row_off;  // p in, p out (LSERK) / dy out (Apply)
       const int64_t t0 = tile * C::TILE_F;
       // do the step's sources reach this tile? (uniform per tile)
-      const bool src_here =
-          MODE == kModeLserk && (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
+      const bool src_here = (MODE == kModeLserk || MODE == kModeKrylov) &&
+                            (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
       const int64_t g_row = t0 + e_row_off;  // SoA index of node 0 of this row
       const uint32_t acc = tmem + (uint32_t)(ps * C::ACC) + ((uint32_t)(q4 * 32) << 16);
 #pragma unroll
@@ -555,6 +560,15 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
                 if (P.read_p) pv = fmaf(P.a, prow[i], pv);
                 prow[i] = pv;
                 yrow[i] = fmaf(P.b, pv, yv);
+              } else if (MODE == kModeKrylov) {
+                // Krylov matvec of a stored basis vector: its scale and the
+                // augmented source coefficient from device memory
+                float w = kry_sig * dy;
+                if (src_here) {
+                  if (P.src_vec != nullptr) w = fmaf(kry_g, __ldg(P.src_vec + g_row + i), w);
+                  if (P.src_idx == g_row + i) w += kry_g;
+                }
+                prow[i] = w;
               } else {
                 prow[i] = dy;
               }
@@ -602,7 +616,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const int64_t gb = ((int64_t)blockIdx.x + j * gridDim.x) * C::TILE_F;
       const float* sy = sY0 + (int)(j % 3) * kYStride;
       const float* sp = sP0 + (int)(j & 1) * kYStride;
-      if (MODE == kModeApply) {
+      if (MODE == kModeApply || MODE == kModeKrylov) {
         tc::bulk_s2g(P.out + gb, sp, C::TILE_B);
       } else {
         tc::bulk_s2g(P.out + gb, sy, C::TILE_B);

@@ -1,11 +1,12 @@
 """Adaptive exponential (ETD) time stepping on the device with an a-posteriori
 Krylov error check, and a learned step proposer.
 
-A step of dy/dt = A y + b g(t) is the augmented exponential
-exp(h [[A, b g_n],[0, 0]]) [y; 1] (propagator.rs:338-373, g held at the step
-start); the device Arnoldi reports its a-posteriori estimate
+A step of dy/dt = A y + b g(t) is the exponential of the system augmented
+with the step's source polynomial (dgtd_etd_try; with one coefficient held at
+the step start it is the reference's exp(h [[A, b g_n],[0, 0]]) [y; 1],
+propagator.rs:338-373); the device Arnoldi reports its a-posteriori estimate
 h_{d+1,d}|exp(tH)_{d-1,0}| (propagator.rs:278-294), and a step is accepted when
-the estimate is at most `tol`.
+the estimate is at most `tol`.  The state stays on the device between steps.
 
 PlainEtd is the adaptive controller: after a step it scales h by
 0.9 (tol/est)^(1/(d+1)) (d the Krylov dimension per sub-step), clipped to
@@ -33,7 +34,6 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _native as nat
 from ._native import check, lib
 
 N_FEATURES = 16
@@ -173,12 +173,33 @@ class LearnedEtd:
 
 
 def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEtd | None = None,
-            log: list | None = None, max_attempts=100000):
-    """ETD from t = 0 to t_end; returns (y, EtdStats).  `log`, if given, gets a
-    (features, target) pair per accepted step of the plain controller for
-    training (the look-ahead target of the module docstring)."""
-    y = np.asarray(y0, dtype=np.float64).copy()
-    b = np.zeros_like(y) if b is None else np.asarray(b, dtype=np.float64)
+            log: list | None = None, max_attempts=100000, point_dof=None, n_coef=8, src_tol=None):
+    """ETD from t = 0 to t_end on the device-resident state; returns (y, EtdStats).
+
+    The source is b*g(t) (b a vector, or the unit vector of `point_dof`), g =
+    `waveform` (None: a free run).  Over each step g is replaced by its
+    degree-(n_coef-1) interpolant at the step's Chebyshev points
+    (sources.step_polynomial) and the step is the exponential of the
+    polynomial-augmented system (dgtd_etd_try); a step whose interpolant
+    deviates from g by more than `src_tol` (default: plain.tol) is shortened
+    before it is tried.  n_coef = 1 with the value at the step start is the
+    reference's held source (propagator.rs:338-373).  The state stays on the
+    device: each try reads back only the Krylov dimension and estimate.
+    `log`, if given, gets a (features, target) pair per accepted step of the
+    plain controller for training (the look-ahead target of the module
+    docstring)."""
+    from . import sources as S
+
+    driven = waveform is not None and (b is not None or point_dof is not None)
+    drive = None
+    if driven:
+        if point_dof is not None:
+            drive = ("point", int(point_dof))
+        else:
+            gop.set_source_vector(np.asarray(b, dtype=np.float64))
+            drive = ("vector", None)
+    src_tol = plain.tol if src_tol is None else float(src_tol)
+    gop.upload(np.asarray(y0, dtype=np.float32))
     st = EtdStats()
     pending = []  # (features, index of the accepted step, previous step) awaiting look-ahead targets
     hist: list[StepRecord] = []
@@ -186,11 +207,30 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
     rejects = 0
     w0 = time.perf_counter()
     attempts = 0
+
+    def coef_for(t0, hh):
+        """(coef, hh): the step's source polynomial, hh shortened until it fits."""
+        if not driven:
+            return None, hh
+        for _ in range(60):
+            if n_coef == 1:
+                return np.array([float(waveform(t0))]), hh
+            c, err = S.step_polynomial(waveform, t0, hh, n_coef)
+            if err * hh <= src_tol:
+                return c, hh
+            hh *= 0.5
+        raise RuntimeError("source polynomial does not converge")
+
+    def attempt(hh, mm):
+        c, hh = coef_for(t, hh)
+        dim, est = gop.etd_try(hh, mm, plain.tol, coef=c, drive=drive)
+        st.matvecs += dim
+        return hh, dim, est
+
     while t < t_end * (1 - 1e-12):
         attempts += 1
         if attempts > max_attempts:
             raise RuntimeError("ETD run exceeded the attempt limit")
-        g = 0.0 if waveform is None else float(waveform(t))
         feat = features(hist, plain.tol, plain.m_max, h0)
         tried_learned = False
         if learned is not None:
@@ -198,28 +238,26 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             # never below the plain controller's own next step: the network
             # can only skip ahead of it
             hp = min(max(hp, h), t_end - t)
-            y_new, dim, est = gop.etd_step_est(y, b * g, hp, mp, plain.tol)
-            st.matvecs += dim
+            hp, dim, est = attempt(hp, mp)
             tried_learned = True
             if est <= plain.tol:
+                gop.etd_commit()
                 st.proposals_kept += 1
                 st.accepted += 1
                 t += hp
-                y = y_new
                 hist.append(StepRecord(hp, dim, est, rejects))
                 rejects = 0
                 h, m = plain.next_after(hp, est, dim, mp, True)
                 continue
             st.proposals_failed += 1
         h_try = min(h, t_end - t)
-        y_new, dim, est = gop.etd_step_est(y, b * g, h_try, m, plain.tol)
-        st.matvecs += dim
+        h_try, dim, est = attempt(h_try, m)
         if est <= plain.tol:
+            gop.etd_commit()
             st.accepted += 1
             if log is not None and not tried_learned:
                 pending.append((feat, len(hist), hist[-1].h if hist else h0))
             t += h_try
-            y = y_new
             hist.append(StepRecord(h_try, dim, est, rejects))
             rejects = 0
             h, m = plain.next_after(h_try, est, dim, m, True)
@@ -227,6 +265,7 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             st.rejected += 1
             rejects += 1
             h, m = plain.next_after(h_try, est, dim, m, False)
+    y = gop.download().astype(np.float64)
     st.seconds = time.perf_counter() - w0
     st.history = [(r.h, r.dim, r.est) for r in hist]
     if log is not None:

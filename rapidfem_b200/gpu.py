@@ -182,6 +182,25 @@ class GpuOperator:
                                      nat.ptr(gs), 1 if record else 0, out))
         return out.reshape(steps + 1, self._n) if record else out
 
+    def transient_f64_stages(self, y0, dt, steps, substeps=1, drive=None, g=None, record=False) -> np.ndarray:
+        """As transient_f64 with g sampled at the LSERK4 stage times: 5 samples
+        per substep (sources.stage_samples)."""
+        y0 = _f64(y0)
+        self._check_len("state", y0)
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self._check_len("source", vec)
+        substeps = max(int(substeps), 1)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f64(g)
+            if gs.size != 5 * steps * substeps:
+                raise ValueError("need 5 waveform samples per substep")
+        out = np.empty(((steps + 1) * self._n) if record else self._n, dtype=np.float64)
+        check(lib.dgtd_transient_f64_stages(self._h, y0, float(dt), int(steps), substeps, kind, dof, nat.ptr(vec),
+                                            nat.ptr(gs), 1 if record else 0, out))
+        return out.reshape(steps + 1, self._n) if record else out
+
     @staticmethod
     def _drive(drive):
         """drive: None | ('point', dof) | ('vector', b)."""
@@ -407,6 +426,41 @@ class GpuOperator:
         check(lib.dgtd_etd_step(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim)))
         return out, dim.value
 
+    def etd_step_poly(self, y, b, coef, h, m, tol=0.0):
+        """ETD step with the source b*g(t0+tau), g(t0+tau) = sum_k coef[k] tau^k:
+        (out, dim_used, est)."""
+        y = _f64(y)
+        b = _f64(b)
+        a = _f64(coef)
+        self._check_len("state", y)
+        self._check_len("source", b)
+        out = np.empty_like(y)
+        dim = C.c_int32()
+        est = C.c_double()
+        check(lib.dgtd_etd_step_poly(self._h, y, b, a.size, a, float(h), int(m), float(tol), out, C.byref(dim),
+                                     C.byref(est)))
+        return out, dim.value, est.value
+
+    def set_krylov_precision(self, bits: int) -> None:
+        """32: f32 basis on the op's engine (default); 64: f64 basis and FP64 matvec."""
+        check(lib.dgtd_op_set_krylov_precision(self._h, int(bits)))
+
+    def etd_try(self, h, m, tol=0.0, coef=None, drive=None):
+        """ETD step candidate from the resident state (see dgtd_etd_try):
+        returns (dim_used, est); `etd_commit` accepts it."""
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            raise ValueError("set a vector drive with set_source_vector first and pass ('vector', None)")
+        a = None if coef is None else _f64(coef)
+        dim = C.c_int32()
+        est = C.c_double()
+        check(lib.dgtd_etd_try(self._h, float(h), int(m), float(tol), 0 if a is None else a.size, nat.ptr(a),
+                               kind, dof, C.byref(dim), C.byref(est)))
+        return dim.value, est.value
+
+    def etd_commit(self) -> None:
+        check(lib.dgtd_etd_commit(self._h))
+
     # ---- device-resident state
     def upload(self, y) -> None:
         y = _f32(y)
@@ -439,6 +493,19 @@ class GpuOperator:
             if gs.size != steps:
                 raise ValueError("wrong number of waveform samples")
         check(lib.dgtd_run_lserk(self._h, float(h), int(steps), kind, dof, nat.ptr(gs)))
+
+    def run_lserk_stages(self, h, steps, drive=None, g_stages=None) -> None:
+        """`steps` LSERK4 steps on the resident state with the waveform sampled
+        at the stage times (5 per step, sources.stage_samples)."""
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            self.set_source_vector(vec)
+        gs = None
+        if kind != nat.DRIVE_FREE:
+            gs = _f32(g_stages)
+            if gs.size != 5 * steps:
+                raise ValueError("need 5 waveform samples per step")
+        check(lib.dgtd_run_lserk_stages(self._h, float(h), int(steps), kind, dof, nat.ptr(gs)))
 
     def apply_device(self, d_y: int, d_dy: int) -> None:
         check(lib.dgtd_apply_device(self._h, C.c_void_p(d_y), C.c_void_p(d_dy)))
