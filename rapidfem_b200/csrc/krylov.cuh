@@ -86,7 +86,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Basis slot i: slot 0 is the chunk's input vector, slots 1.. are contiguous.
 template <class B>
-__device__ __forceinline__ const B* kry_col(const B* v0, const B* vb, int64_t len, int i) {
+__host__ __device__ __forceinline__ const B* kry_col(const B* v0, const B* vb, int64_t len, int i) {
   return i == 0 ? v0 : vb + (int64_t)(i - 1) * len;
 }
 
