@@ -1902,8 +1902,11 @@ int krylov_run_t(dgtd_op* op, const double* v_host, const double* b_host, int P,
     bvec = kb.b->p;
   }
   DGTD_TRY(set_poly(op, b_host ? P : 0, a));
-  // the result: a buffer of state_len doubles holds either basis type
+  // the result: a buffer of state_len doubles holds either basis type; it is
+  // also an intermediate sub-step's input, so its padding must be zero (and a
+  // run of the other basis type may have left values there)
   DGTD_TRY(op->kout64.alloc(state_len(op)));
+  CUDA_TRY(cudaMemsetAsync(op->kout64.p, 0, state_len(op) * 8, s));
   B* dst = reinterpret_cast<B*>(op->kout64.p);
   int d = 0;
   double e = -1.0;

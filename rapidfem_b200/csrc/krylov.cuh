@@ -109,22 +109,56 @@ __device__ __forceinline__ void block_sums(double (&acc)[NC], int cols, double* 
   }
 }
 
+// The sweeps read whole 16-byte vectors (4 floats or 2 doubles): every vector
+// is a state buffer of state length (whole tiles plus slack) whose entries
+// past n are zero and stay zero, and every slot starts 16-byte aligned, so a
+// sweep covers ceil(n / VW) vectors.  Each thread holds one vector of every
+// column in registers before it accumulates, which keeps up to kKryCols
+// 16-byte loads per thread in flight.
+template <class B> struct KryVec;
+template <> struct KryVec<float> {
+  using T = float4;
+  static constexpr int W = 4;
+  __device__ static double at(const float4& v, int q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; }
+  __device__ static void set(float4& v, int q, double x) {
+    const float f = (float)x;
+    if (q == 0) v.x = f; else if (q == 1) v.y = f; else if (q == 2) v.z = f; else v.w = f;
+  }
+};
+template <> struct KryVec<double> {
+  using T = double2;
+  static constexpr int W = 2;
+  __device__ static double at(const double2& v, int q) { return q == 0 ? v.x : v.y; }
+  __device__ static void set(double2& v, int q, double x) {
+    if (q == 0) v.x = x; else v.y = x;
+  }
+};
+
 // partials[b*kKryCols + i] = sum over this block's k of V_i[k] * w[k], i < cols.
 template <class B>
 __global__ void __launch_bounds__(kKrylovThreads)
 k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, int cols,
            const B* __restrict__ w, double* __restrict__ partials, const int* skip) {
   if (*skip) return;
+  using KV = KryVec<B>;
+  using T = typename KV::T;
   __shared__ double red[kKryCols * (kKrylovThreads / 32)];
   double acc[kKryCols];
 #pragma unroll
   for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
+  const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const double wk = (double)w[k];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
+    const T wk = reinterpret_cast<const T*>(w)[k];
+    T vk[kKryCols];
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) acc[i] = fma((double)kry_col(v0, vb, len, i)[k], wk, acc[i]);
+      if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+#pragma unroll
+    for (int i = 0; i < kKryCols; ++i)
+      if (i < cols)
+#pragma unroll
+        for (int q = 0; q < KV::W; ++q) acc[i] = fma(KV::at(vk[i], q), KV::at(wk, q), acc[i]);
   }
   block_sums<kKryCols>(acc, cols, red, partials + (int64_t)blockIdx.x * kKryCols);
 }
@@ -165,32 +199,38 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
   if (*skip) return;
+  using KV = KryVec<B>;
+  using T = typename KV::T;
   __shared__ double u[kKryCols];
   __shared__ double red[kKryCols * (kKrylovThreads / 32)];
   kry_proj(st, partials_in, nb_in, j, 0, u);
   __syncthreads();
   const int cols = j + 1;
-  double c[kKryCols], acc[kKryCols];
+  double acc[kKryCols];
 #pragma unroll
-  for (int i = 0; i < kKryCols; ++i) {
-    c[i] = i < cols ? u[i] : 0.0;
-    acc[i] = 0.0;
-  }
+  for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
+  const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    B vk[kKryCols];
-    double wk = (double)w[k];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
+    T wk = reinterpret_cast<const T*>(w)[k];
+    T vk[kKryCols];
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) {
-        vk[i] = kry_col(v0, vb, len, i)[k];
-        wk = fma(-c[i], (double)vk[i], wk);
-      }
-    const B wn = (B)wk;
-    w[k] = wn;
+      if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+#pragma unroll
+    for (int q = 0; q < KV::W; ++q) {
+      double x = KV::at(wk, q);
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
+      KV::set(wk, q, x);
+    }
+    reinterpret_cast<T*>(w)[k] = wk;
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) acc[i] = fma((double)vk[i], (double)wn, acc[i]);
+      if (i < cols)
+#pragma unroll
+        for (int q = 0; q < KV::W; ++q) acc[i] = fma(KV::at(vk[i], q), KV::at(wk, q), acc[i]);
   }
   block_sums<kKryCols>(acc, cols, red, partials_out + (int64_t)blockIdx.x * kKryCols);
 }
@@ -202,24 +242,33 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
   if (*skip) return;
+  using KV = KryVec<B>;
+  using T = typename KV::T;
   __shared__ double u[kKryCols];
   __shared__ double red[kKryCols * (kKrylovThreads / 32)];
   kry_proj(st, partials_in, nb_in, j, 1, u);
   __syncthreads();
   const int cols = j + 1;
-  double c[kKryCols];
-#pragma unroll
-  for (int i = 0; i < kKryCols; ++i) c[i] = i < cols ? u[i] : 0.0;
   double acc[1] = {0.0};
+  const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    double wk = (double)w[k];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
+    T wk = reinterpret_cast<const T*>(w)[k];
+    T vk[kKryCols];
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) wk = fma(-c[i], (double)kry_col(v0, vb, len, i)[k], wk);
-    const B wn = (B)wk;
-    w[k] = wn;
-    acc[0] = fma((double)wn, (double)wn, acc[0]);
+      if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+#pragma unroll
+    for (int q = 0; q < KV::W; ++q) {
+      double x = KV::at(wk, q);
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
+      KV::set(wk, q, x);
+      const double xs = KV::at(wk, q);  // the stored (rounded) value
+      acc[0] = fma(xs, xs, acc[0]);
+    }
+    reinterpret_cast<T*>(w)[k] = wk;
   }
   block_sums<1>(acc, 1, red, partials_out + (int64_t)blockIdx.x * kKryCols);
 }

@@ -10,7 +10,7 @@ independent references:
   * the resident-state step (dgtd_etd_try / commit) against the host-API step.
 
 Tolerances: 1e-4 relative L2 with the f32 basis (the Krylov parity bar), 1e-10
-on the FP64 path at tol = 1e-12.
+on the FP64 path against the oracle's Arnoldi over the same sub-steps.
 """
 import numpy as np
 import pytest
@@ -78,10 +78,17 @@ def test_fp64_krylov_matches_oracle(ctx):
     v = np.sin(0.3 + 0.017 * np.arange(n))
     b = np.cos(0.05 * np.arange(n))
     t = 8.0 / rho
-    want, _ = orc.expmv(v, t, 40, 0.0)
+    # m = 40 runs as 4 sub-steps of dimension 10 over t/4 (KRYLOV_CHUNK,
+    # gpu/operator.rs:1175-1197); the oracle's CPU Arnoldi does not sub-step,
+    # so it is composed over the same sub-steps (exact for the held source)
+    want = v
+    for _ in range(4):
+        want, _ = orc.expmv(want, t / 4, 10, 0.0)
     got, _ = gop.expmv(v, t, 40)
     assert rel_l2(got, want) < KRY_TOL64
-    want, _ = orc.etd_step(v, b, t, 40, 0.0)
+    want = v
+    for _ in range(4):
+        want, _ = orc.etd_step(want, b, t / 4, 10, 0.0)
     got, _ = gop.etd_step(v, b, t, 40)
     assert rel_l2(got, want) < KRY_TOL64
 
