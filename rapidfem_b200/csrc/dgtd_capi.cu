@@ -1736,7 +1736,7 @@ KryBufs<B> kry_bufs(dgtd_op* op) {
 template <class B>
 int ensure_krylov(dgtd_op* op, int chunk) {
   if (chunk < 1 || chunk > dgtd::kKryMaxChunk)
-    return set_error(DGTD_ERR_UNSUPPORTED, "Krylov chunk dimension outside 1..15");
+    return set_error(DGTD_ERR_UNSUPPORTED, "Krylov chunk dimension outside 1..12");
   const size_t len = state_len(op);
   cudaStream_t s = op->stream();
   KryBufs<B> kb = kry_bufs<B>(op);
@@ -1830,7 +1830,7 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
     CUDA_TRY(cudaGetLastError());
   }
   k_kry_finish_coef<<<1, kExpmThreads, kExpmSmem, s>>>(st);
-  k_kry_lincomb<B, B><<<gs, 256, 0, s>>>(v, vb, len, n, st, out);
+  k_kry_lincomb<B><<<nb, nt, 0, s>>>(v, vb, len, n, st, out);
   op->launches += 2;
   CUDA_TRY(cudaGetLastError());
   return DGTD_OK;

@@ -52,8 +52,8 @@
 namespace dgtd {
 
 constexpr int kKrylovMaxDim = 64;     // H capacity (64 x 64)
-constexpr int kKryCols = 16;          // basis vectors of one chunk in the fused sweeps (chunk dim <= 15)
-constexpr int kKryMaxChunk = kKryCols - 1;
+constexpr int kKryCols = 12;          // basis vectors of one chunk in the fused sweeps
+constexpr int kKryMaxChunk = kKryCols;  // chunk dimension (the reference's KRYLOV_CHUNK is 12)
 constexpr int kAugMax = 8;            // polynomial source terms
 constexpr int kKrylovBlocks = 296;    // persistent reduction grid (2 per SM)
 constexpr int kKrylovThreads = 256;
@@ -109,6 +109,30 @@ __device__ __forceinline__ void block_sums(double (&acc)[NC], int cols, double* 
   }
 }
 
+// Sum over the blocks of a sweep's partial rows, columns i < cols, into out[]
+// (shared), by all threads of a block of >= 256 threads: thread t adds the
+// rows r, r + R, ... (r = t / kKryCols, R = 256 / kKryCols) of column
+// t % kKryCols, then the R values per column are added in a fixed order
+// (deterministic, and the same in every block).
+__device__ __forceinline__ void sum_partials(const double* partials, int nblocks, int cols, double* out) {
+  constexpr int R = 256 / kKryCols;  // row groups
+  __shared__ double tmp[R * kKryCols];
+  const int i = threadIdx.x % kKryCols, r = threadIdx.x / kKryCols;
+  if (r < R) {
+    double s = 0.0;
+    if (i < cols)
+      for (int b = r; b < nblocks; b += R) s += partials[(int64_t)b * kKryCols + i];
+    tmp[threadIdx.x] = s;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < cols) {
+    double t = 0.0;
+    for (int q = 0; q < R; ++q) t += tmp[q * kKryCols + threadIdx.x];
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
 // The sweeps read whole 16-byte vectors (4 floats or 2 doubles): every vector
 // is a state buffer of state length (whole tiles plus slack) whose entries
 // past n are zero and stay zero, and every slot starts 16-byte aligned, so a
@@ -136,7 +160,7 @@ template <> struct KryVec<double> {
 
 // partials[b*kKryCols + i] = sum over this block's k of V_i[k] * w[k], i < cols.
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads)
+__global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, int cols,
            const B* __restrict__ w, double* __restrict__ partials, const int* skip) {
   if (*skip) return;
@@ -170,13 +194,13 @@ k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int6
 __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* partials, int nblocks, int j, int pass,
                                          double* u) {
   __shared__ double proj[kKryCols];
+  __shared__ double sums[kKryCols];
   const int cols = j + 1;
   const int P = st->naug;
+  sum_partials(partials, nblocks, cols, sums);
   if ((int)threadIdx.x < cols) {
     const int i = threadIdx.x;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKryCols + i];
-    s *= st->sig[i];
+    double s = sums[i] * st->sig[i];
     for (int q = 0; q < P; ++q) s += st->s[i][q] * st->wa[pass][q];
     proj[i] = s;
     u[i] = s * st->sig[i];
@@ -194,7 +218,7 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* partials, 
 
 // First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads)
+__global__ void __launch_bounds__(kKrylovThreads, 1)
 k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
@@ -217,6 +241,8 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+    // per lane: the update, then the second pass's products with the stored
+    // (rounded) value, so that only one lane's converted values are live
 #pragma unroll
     for (int q = 0; q < KV::W; ++q) {
       double x = KV::at(wk, q);
@@ -224,20 +250,19 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
       for (int i = 0; i < kKryCols; ++i)
         if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
       KV::set(wk, q, x);
+      const double xs = KV::at(wk, q);
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < cols) acc[i] = fma(KV::at(vk[i], q), xs, acc[i]);
     }
     reinterpret_cast<T*>(w)[k] = wk;
-#pragma unroll
-    for (int i = 0; i < kKryCols; ++i)
-      if (i < cols)
-#pragma unroll
-        for (int q = 0; q < KV::W; ++q) acc[i] = fma(KV::at(vk[i], q), KV::at(wk, q), acc[i]);
   }
   block_sums<kKryCols>(acc, cols, red, partials_out + (int64_t)blockIdx.x * kKryCols);
 }
 
 // Second-pass update and the partial sums of |w|^2 (slot 0 of each block's row).
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads)
+__global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
@@ -275,7 +300,7 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
 
 // Partial sums of x^2 (slot 0 of each block's row).
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads)
+__global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_norm_partials(const B* __restrict__ x, int64_t n, double* __restrict__ partials) {
   __shared__ double red[kKrylovThreads / 32];
   double acc[1] = {0.0};
@@ -287,21 +312,34 @@ k_kry_norm_partials(const B* __restrict__ x, int64_t n, double* __restrict__ par
 }
 
 // out[k] = sum_{i<dim} coef[i] * stored_i[k] (f64 accumulation), dim and coef
-// from the device state; O is the output type.
-template <class B, class O>
-__global__ void __launch_bounds__(kKrylovThreads)
+// from the device state; whole 16-byte vectors as the sweeps (the output's
+// entries past n are written as the zero combination of zero entries).
+template <class B>
+__global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_lincomb(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, const KrylovDev* st,
-              O* __restrict__ out) {
+              B* __restrict__ out) {
+  using KV = KryVec<B>;
+  using T = typename KV::T;
   __shared__ double c[kKryCols];
   const int dim = st->dim;
   if ((int)threadIdx.x < kKryCols) c[threadIdx.x] = (int)threadIdx.x < dim ? st->coef[threadIdx.x] : 0.0;
   __syncthreads();
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    double s = 0.0;
+  const int64_t nv = (n + KV::W - 1) / KV::W;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += (int64_t)gridDim.x * blockDim.x) {
+    T vk[kKryCols];
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < dim) s = fma(c[i], (double)kry_col(v0, vb, len, i)[k], s);
-    out[k] = (O)s;
+      if (i < dim) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+    T o;
+#pragma unroll
+    for (int q = 0; q < KV::W; ++q) {
+      double x = 0.0;
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < dim) x = fma(c[i], KV::at(vk[i], q), x);
+      KV::set(o, q, x);
+    }
+    reinterpret_cast<T*>(out)[k] = o;
   }
 }
 
@@ -383,6 +421,8 @@ constexpr size_t kExpmSmem = 5 * kKrylovMaxDim * kKrylovMaxDim * sizeof(double);
 // sig[0] = 1/beta, s[0] = e_{P-1}/(eta beta).
 __global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, double t, double tol, int P,
                             const double* a, double delta, int max_dim, int* skip) {
+  __shared__ double s_norm2[1];
+  sum_partials(partials, nblocks, 1, s_norm2);
   if (threadIdx.x == 0) {
     double shifted[kAugMax], cu[kAugMax];
     double cmax = 0.0;
@@ -405,8 +445,7 @@ __global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, 
     }
     for (int q = 0; q < P; ++q) cmax = fmax(cmax, fabs(cu[q]));
     const double eta = 1.0 / fmax(1.0, cmax);
-    double s2 = 0.0;
-    for (int b = 0; b < nblocks; ++b) s2 += partials[(int64_t)b * kKryCols];
+    double s2 = s_norm2[0];
     const double u_last = P > 0 ? 1.0 / eta : 0.0;
     s2 += u_last * u_last;
     const double beta = sqrt(s2);
@@ -452,11 +491,12 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
   __shared__ double s_hnext;
   __shared__ int s_stop;
   __shared__ int s_break;
+  __shared__ double s_norm2[1];
   const int d = j + 1;
   const int P = st->naug;
+  sum_partials(partials, nblocks, 1, s_norm2);
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * kKryCols];
+    double s = s_norm2[0];
     for (int q = 0; q < P; ++q) s += st->wa[2][q] * st->wa[2][q];
     s_hnext = sqrt(s);
     s_break = s_hnext < 1e-12 ? 1 : 0;
