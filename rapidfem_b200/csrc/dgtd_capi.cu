@@ -1753,7 +1753,7 @@ int ensure_krylov(dgtd_op* op, int chunk) {
     DGTD_TRY(kb.b->alloc(len));
     CUDA_TRY(cudaMemsetAsync(kb.b->p, 0, len * sizeof(B), s));
   }
-  DGTD_TRY(op->partials.alloc((size_t)2 * dgtd::kKrylovBlocks * dgtd::kKryCols));
+  DGTD_TRY(op->partials.alloc((size_t)2 * dgtd::kKrylovBlocks * dgtd::kKryRow));
   DGTD_TRY(op->kst.alloc(1));
   DGTD_TRY(op->skip.alloc(1));
   DGTD_TRY(op->kpoly.alloc(dgtd::kAugMax));
@@ -1812,7 +1812,7 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
   KrylovDev* st = op->kst.p;
   B* vb = kry_bufs<B>(op).basis->p;
   double* pa = op->partials.p;
-  double* pb = pa + (size_t)kKrylovBlocks * kKryCols;
+  double* pb = pa + (size_t)kKrylovBlocks * kKryRow;
   if (first) CUDA_TRY(cudaMemsetAsync(&st->dim_total, 0, sizeof(int) * 2 + sizeof(double), s));
   k_kry_norm_partials<B><<<nb, nt, 0, s>>>(v, n, pa);
   k_kry_start<<<1, kExpmThreads, 0, s>>>(st, pa, nb, t, tol, P, op->kpoly.p, delta, m, op->skip.p);

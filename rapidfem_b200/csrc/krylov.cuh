@@ -36,11 +36,13 @@
 //
 // One Arnoldi step j (cols = j+1 basis vectors), five launches:
 //   RHS (mode Krylov)   w = sig_j A V_j + g_j b          (w in slot j+1)
-//   k_kry_dots          block partials of V_i . w, i <= j
+//   k_kry_dots          block partials of V_i . w, i <= j, and of |w|^2
 //   k_kry_update_dots   proj (every block reduces the partials itself), then
-//                       w -= sum proj_i V_i and the second pass's partials in
-//                       the same sweep (one read of each V_i)
-//   k_kry_update_norm   second-pass proj, w -= sum proj_i V_i, partials of |w|^2
+//                       w -= sum proj_i V_i, the second pass's partials and
+//                       |w|^2 in the same sweep (one read of each V_i)
+//   k_kry_update_norm   the second pass, only when the first removed more than
+//                       half of |w|^2 (kReorth2): second-pass proj,
+//                       w -= sum proj_i V_i, partials of |w|^2
 //   k_kry_finish_norm   h_{j+1,j}, breakdown / last dimension / a-posteriori
 //                       estimate h_{j+1,j}|exp(tH)_{d-1,0}| < tol (expm of H in
 //                       one block), the next scale and augmented part
@@ -54,6 +56,13 @@ namespace dgtd {
 constexpr int kKrylovMaxDim = 64;     // H capacity (64 x 64)
 constexpr int kKryCols = 12;          // basis vectors of one chunk in the fused sweeps
 constexpr int kKryMaxChunk = kKryCols;  // chunk dimension (the reference's KRYLOV_CHUNK is 12)
+constexpr int kKryRow = 16;           // doubles per block row of sweep partials
+constexpr int kKryNormCol = kKryRow - 1;  // the row's squared-norm column
+// Second Gram-Schmidt pass only when the first one removed more than half of
+// |w|^2, i.e. |w'| < |w| / sqrt(2) (Daniel, Gragg, Kaufman & Stewart, Math.
+// Comp. 30 (1976): "twice is enough"); otherwise w' is orthogonal to the
+// basis to working precision and the pass would not change it.
+constexpr double kReorth2 = 0.5;
 constexpr int kAugMax = 8;            // polynomial source terms
 constexpr int kKrylovBlocks = 296;    // persistent reduction grid (2 per SM)
 constexpr int kKrylovThreads = 256;
@@ -67,6 +76,9 @@ struct KrylovDev {
   double wa[3][kAugMax];                    // augmented part of w: after the matvec, pass 1, pass 2
   double coef[kKryCols];                    // result = sum coef[i] * stored vector i
   double mv[2];                             // next matvec: input scale, source coefficient
+  double wn2;                               // |[w; wa]|^2 after the matvec (the pass-1 input)
+  double hn2;                               // |[w'; wa]|^2 after pass 1, when pass 2 is skipped
+  int reorth;                               // 1: pass 2 ran for the current step
   double beta, t, tol, est;
   int dim;                                  // dimension decided so far (the final one when done)
   int done;                                 // 1: stop growing the space
@@ -109,25 +121,25 @@ __device__ __forceinline__ void block_sums(double (&acc)[NC], int cols, double* 
   }
 }
 
-// Sum over the blocks of a sweep's partial rows, columns i < cols, into out[]
-// (shared), by all threads of a block of >= 256 threads: thread t adds the
-// rows r, r + R, ... (r = t / kKryCols, R = 256 / kKryCols) of column
-// t % kKryCols, then the R values per column are added in a fixed order
+// Sum over the blocks of a sweep's partial rows into out[kKryRow] (shared):
+// the dot columns i < cols and the norm column, by all threads of a block of
+// >= 256 threads: thread t adds the rows r, r + 16, ... (r = t / 16) of column
+// t % 16, then the 16 values per column are added in a fixed order
 // (deterministic, and the same in every block).
 __device__ __forceinline__ void sum_partials(const double* partials, int nblocks, int cols, double* out) {
-  constexpr int R = 256 / kKryCols;  // row groups
-  __shared__ double tmp[R * kKryCols];
-  const int i = threadIdx.x % kKryCols, r = threadIdx.x / kKryCols;
+  constexpr int R = 256 / kKryRow;
+  __shared__ double tmp[R * kKryRow];
+  const int i = threadIdx.x % kKryRow, r = threadIdx.x / kKryRow;
   if (r < R) {
     double s = 0.0;
-    if (i < cols)
-      for (int b = r; b < nblocks; b += R) s += partials[(int64_t)b * kKryCols + i];
+    if (i < cols || i == kKryNormCol)
+      for (int b = r; b < nblocks; b += R) s += partials[(int64_t)b * kKryRow + i];
     tmp[threadIdx.x] = s;
   }
   __syncthreads();
-  if ((int)threadIdx.x < cols) {
+  if ((int)threadIdx.x < kKryRow) {
     double t = 0.0;
-    for (int q = 0; q < R; ++q) t += tmp[q * kKryCols + threadIdx.x];
+    for (int q = 0; q < R; ++q) t += tmp[q * kKryRow + threadIdx.x];
     out[threadIdx.x] = t;
   }
   __syncthreads();
@@ -158,7 +170,8 @@ template <> struct KryVec<double> {
   }
 };
 
-// partials[b*kKryCols + i] = sum over this block's k of V_i[k] * w[k], i < cols.
+// partials[b*kKryRow + i] = sum over this block's k of V_i[k] * w[k], i < cols,
+// and w . w in the norm column.
 template <class B>
 __global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n, int cols,
@@ -170,6 +183,7 @@ k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int6
   double acc[kKryCols];
 #pragma unroll
   for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
+  double wn[1] = {0.0};
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
@@ -179,25 +193,28 @@ k_kry_dots(const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int6
     for (int i = 0; i < kKryCols; ++i)
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
 #pragma unroll
+    for (int q = 0; q < KV::W; ++q) wn[0] = fma(KV::at(wk, q), KV::at(wk, q), wn[0]);
+#pragma unroll
     for (int i = 0; i < kKryCols; ++i)
       if (i < cols)
 #pragma unroll
         for (int q = 0; q < KV::W; ++q) acc[i] = fma(KV::at(vk[i], q), KV::at(wk, q), acc[i]);
   }
-  block_sums<kKryCols>(acc, cols, red, partials + (int64_t)blockIdx.x * kKryCols);
+  double* row = partials + (int64_t)blockIdx.x * kKryRow;
+  block_sums<kKryCols>(acc, cols, red, row);
+  __syncthreads();
+  block_sums<1>(wn, 1, red, row + kKryNormCol);
 }
 
-// The projections of a pass from the block partials (every block computes them
-// identically): proj_i = sig_i * (sum_b partials) + s_i . wa_in.  Block 0 adds
-// them to H[:, j] and writes wa_out = wa_in - sum_i proj_i s_i.  Returns, in
-// shared u[], the update coefficients u_i = proj_i * sig_i of the stored vectors.
-__device__ __forceinline__ void kry_proj(KrylovDev* st, const double* partials, int nblocks, int j, int pass,
-                                         double* u) {
+// The projections of a pass from the summed partials (every block computes them
+// identically): proj_i = sig_i * sums[i] + s_i . wa_in.  Block 0 adds them to
+// H[:, j] and writes wa_out = wa_in - sum_i proj_i s_i (pass 0 also records
+// |[w; wa]|^2).  Returns, in shared u[], the update coefficients
+// u_i = proj_i * sig_i of the stored vectors.
+__device__ __forceinline__ void kry_proj(KrylovDev* st, const double* sums, int j, int pass, double* u) {
   __shared__ double proj[kKryCols];
-  __shared__ double sums[kKryCols];
   const int cols = j + 1;
   const int P = st->naug;
-  sum_partials(partials, nblocks, cols, sums);
   if ((int)threadIdx.x < cols) {
     const int i = threadIdx.x;
     double s = sums[i] * st->sig[i];
@@ -213,6 +230,11 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* partials, 
       for (int i = 0; i < cols; ++i) d -= proj[i] * st->s[i][q];
       st->wa[pass + 1][q] = d;
     }
+    if (pass == 0) {
+      double wa2 = 0.0;
+      for (int q = 0; q < P; ++q) wa2 += st->wa[0][q] * st->wa[0][q];
+      st->wn2 = sums[kKryNormCol] + wa2;
+    }
   }
 }
 
@@ -226,13 +248,16 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   using KV = KryVec<B>;
   using T = typename KV::T;
   __shared__ double u[kKryCols];
+  __shared__ double sums[kKryRow];
   __shared__ double red[kKryCols * (kKrylovThreads / 32)];
-  kry_proj(st, partials_in, nb_in, j, 0, u);
-  __syncthreads();
   const int cols = j + 1;
+  sum_partials(partials_in, nb_in, cols, sums);
+  kry_proj(st, sums, j, 0, u);
+  __syncthreads();
   double acc[kKryCols];
 #pragma unroll
   for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
+  double wn[1] = {0.0};
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
@@ -251,16 +276,23 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
         if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
       KV::set(wk, q, x);
       const double xs = KV::at(wk, q);
+      wn[0] = fma(xs, xs, wn[0]);
 #pragma unroll
       for (int i = 0; i < kKryCols; ++i)
         if (i < cols) acc[i] = fma(KV::at(vk[i], q), xs, acc[i]);
     }
     reinterpret_cast<T*>(w)[k] = wk;
   }
-  block_sums<kKryCols>(acc, cols, red, partials_out + (int64_t)blockIdx.x * kKryCols);
+  double* row = partials_out + (int64_t)blockIdx.x * kKryRow;
+  block_sums<kKryCols>(acc, cols, red, row);
+  __syncthreads();
+  block_sums<1>(wn, 1, red, row + kKryNormCol);
 }
 
-// Second-pass update and the partial sums of |w|^2 (slot 0 of each block's row).
+// The second pass, when it is needed: every block decides from the summed
+// partials of pass 1 (|w'|^2 < kReorth2 |w|^2); without it block 0 records
+// |[w'; wa]|^2 for the norm finisher and the sweep is skipped.  With it, the
+// second-pass update and the partial sums of |w|^2 (the norm column).
 template <class B>
 __global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
@@ -270,10 +302,25 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   using KV = KryVec<B>;
   using T = typename KV::T;
   __shared__ double u[kKryCols];
+  __shared__ double sums[kKryRow];
   __shared__ double red[kKryCols * (kKrylovThreads / 32)];
-  kry_proj(st, partials_in, nb_in, j, 1, u);
-  __syncthreads();
   const int cols = j + 1;
+  sum_partials(partials_in, nb_in, cols, sums);
+  const int P = st->naug;
+  double wa2 = 0.0;
+  for (int q = 0; q < P; ++q) wa2 += st->wa[1][q] * st->wa[1][q];
+  const double wn2_1 = sums[kKryNormCol] + wa2;
+  if (!(wn2_1 < kReorth2 * st->wn2)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->reorth = 0;
+      st->hn2 = wn2_1;
+      for (int q = 0; q < kAugMax; ++q) st->wa[2][q] = st->wa[1][q];
+    }
+    return;  // uniform: every block takes the same decision
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->reorth = 1;
+  kry_proj(st, sums, j, 1, u);
+  __syncthreads();
   double acc[1] = {0.0};
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -295,7 +342,7 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
     }
     reinterpret_cast<T*>(w)[k] = wk;
   }
-  block_sums<1>(acc, 1, red, partials_out + (int64_t)blockIdx.x * kKryCols);
+  block_sums<1>(acc, 1, red, partials_out + (int64_t)blockIdx.x * kKryRow + kKryNormCol);
 }
 
 // Partial sums of x^2 (slot 0 of each block's row).
@@ -308,7 +355,7 @@ k_kry_norm_partials(const B* __restrict__ x, int64_t n, double* __restrict__ par
     const double v = (double)x[k];
     acc[0] = fma(v, v, acc[0]);
   }
-  block_sums<1>(acc, 1, red, partials + (int64_t)blockIdx.x * kKryCols);
+  block_sums<1>(acc, 1, red, partials + (int64_t)blockIdx.x * kKryRow + kKryNormCol);
 }
 
 // out[k] = sum_{i<dim} coef[i] * stored_i[k] (f64 accumulation), dim and coef
@@ -421,8 +468,8 @@ constexpr size_t kExpmSmem = 5 * kKrylovMaxDim * kKrylovMaxDim * sizeof(double);
 // sig[0] = 1/beta, s[0] = e_{P-1}/(eta beta).
 __global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, double t, double tol, int P,
                             const double* a, double delta, int max_dim, int* skip) {
-  __shared__ double s_norm2[1];
-  sum_partials(partials, nblocks, 1, s_norm2);
+  __shared__ double s_sums[kKryRow];
+  sum_partials(partials, nblocks, 0, s_sums);
   if (threadIdx.x == 0) {
     double shifted[kAugMax], cu[kAugMax];
     double cmax = 0.0;
@@ -445,7 +492,7 @@ __global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, 
     }
     for (int q = 0; q < P; ++q) cmax = fmax(cmax, fabs(cu[q]));
     const double eta = 1.0 / fmax(1.0, cmax);
-    double s2 = s_norm2[0];
+    double s2 = s_sums[kKryNormCol];
     const double u_last = P > 0 ? 1.0 / eta : 0.0;
     s2 += u_last * u_last;
     const double beta = sqrt(s2);
@@ -491,13 +538,19 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
   __shared__ double s_hnext;
   __shared__ int s_stop;
   __shared__ int s_break;
-  __shared__ double s_norm2[1];
+  __shared__ double s_sums[kKryRow];
   const int d = j + 1;
   const int P = st->naug;
-  sum_partials(partials, nblocks, 1, s_norm2);
+  const bool reorth = st->reorth != 0;
+  if (reorth) sum_partials(partials, nblocks, 0, s_sums);  // uniform
   if (threadIdx.x == 0) {
-    double s = s_norm2[0];
-    for (int q = 0; q < P; ++q) s += st->wa[2][q] * st->wa[2][q];
+    double s;
+    if (reorth) {
+      s = s_sums[kKryNormCol];
+      for (int q = 0; q < P; ++q) s += st->wa[2][q] * st->wa[2][q];
+    } else {
+      s = st->hn2;
+    }
     s_hnext = sqrt(s);
     s_break = s_hnext < 1e-12 ? 1 : 0;
     s_stop = (s_break || d == st->max_dim) ? 1 : 0;
