@@ -18,7 +18,8 @@ controller logged) for the next step size and Krylov cap from the history of
 the last four accepted steps; the proposed step is never below the plain
 controller's own next step, it is tried and kept only if its estimate passes,
 otherwise the plain controller decides the step (and its estimate alone decides
-acceptance).  The training target of a logged step is what its
+acceptance).  A proposal within 5 % of the plain step is not tried on its own,
+and after a failed proposal the next attempt is the plain controller's.  The training target of a logged step is what its
 run says in hindsight: the largest step the plain controller itself took
 within the next LOOKAHEAD accepted steps (a step size it reached and passed
 from a similar state), relative to the previous step, and that step's Krylov
@@ -207,6 +208,7 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
     rejects = 0
     w0 = time.perf_counter()
     attempts = 0
+    failed_last = False
 
     def coef_for(t0, hh):
         """(coef, hh): the step's source polynomial, hh shortened until it fits."""
@@ -233,11 +235,17 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             raise RuntimeError("ETD run exceeded the attempt limit")
         feat = features(hist, plain.tol, plain.m_max, h0)
         tried_learned = False
-        if learned is not None:
+        hp = mp = None
+        if learned is not None and not failed_last:
             hp, mp = learned.propose(hist, h0)
             # never below the plain controller's own next step: the network
-            # can only skip ahead of it
+            # can only skip ahead of it; a proposal no longer than that step
+            # is the plain step, which is tried below anyway
             hp = min(max(hp, h), t_end - t)
+            if hp <= 1.05 * min(h, t_end - t):
+                hp = None
+        failed_last = False
+        if hp is not None:
             hp, dim, est = attempt(hp, mp)
             tried_learned = True
             if est <= plain.tol:
@@ -250,6 +258,7 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
                 h, m = plain.next_after(hp, est, dim, mp, True)
                 continue
             st.proposals_failed += 1
+            failed_last = True  # the next attempt is the plain controller's alone
         h_try = min(h, t_end - t)
         h_try, dim, est = attempt(h_try, m)
         if est <= plain.tol:
