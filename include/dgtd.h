@@ -263,8 +263,10 @@ int dgtd_etd_step(dgtd_op *op, const double *y, const double *b, double h, int32
  * estimate h_{d+1,d}*|exp(tH)_{d-1,0}| (propagator.rs:278-294, relative to |y|)
  * summed over the KRYLOV_CHUNK sub-steps, each of the k sub-steps stopping at
  * tol/k; the estimate is formed at the final dimension too, so `est` > tol
- * reports a step whose space was too small.  The accept/reject test of an
- * adaptive or learned step controller. */
+ * reports a step whose space was too small.  A sub-step that misses tol/k ends
+ * the step: the later sub-steps are skipped and `est` is that sub-step's
+ * estimate times k (> tol), so a rejected step costs one sub-step.  The
+ * accept/reject test of an adaptive or learned step controller. */
 int dgtd_etd_step_est(dgtd_op *op, const double *y, const double *b, double h, int32_t m, double tol,
                       double *out, int32_t *dim_used, double *est);
 /* The ETD step with a time-varying source b*g(t0 + tau), g a polynomial over

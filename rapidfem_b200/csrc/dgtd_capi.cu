@@ -1799,10 +1799,11 @@ int kry_matvec(dgtd_op* op, const B* v, B* w, const B* bvec, int64_t src_idx, co
 // first n components of exp(t*Aug)[v; e_{P-1}/eta] (P > 0, the source
 // polynomial's coefficients in op->kpoly, shifted by `delta`) or exp(t*A) v
 // (P = 0).  The chunk's dimension and estimate are accumulated on the device
-// (KrylovDev::dim_total, est_sum); `first` starts a new accumulation.
+// (KrylovDev::dim_total, est_sum); `first` starts a new accumulation, in
+// abort mode when abort_chunks > 0 (see k_kry_finish_coef).
 template <class B>
 int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, double delta, const B* bvec,
-                 int64_t src_idx, B* out, bool first) {
+                 int64_t src_idx, B* out, bool first, int abort_chunks) {
   using namespace dgtd;
   cudaStream_t s = op->stream();
   const int64_t n = op->n_dof;
@@ -1813,7 +1814,17 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
   B* vb = kry_bufs<B>(op).basis->p;
   double* pa = op->partials.p;
   double* pb = pa + (size_t)kKrylovBlocks * kKryRow;
-  if (first) CUDA_TRY(cudaMemsetAsync(&st->dim_total, 0, sizeof(int) * 2 + sizeof(double), s));
+  if (first) {
+    struct {
+      int dim_total, est_none;
+      double est_sum;
+      int aborted, abort_chunks;
+    } acc = {0, 0, 0.0, 0, abort_chunks};
+    static_assert(sizeof(acc) == offsetof(KrylovDev, abort_chunks) + sizeof(int) - offsetof(KrylovDev, dim_total),
+                  "accumulator layout");
+    CUDA_TRY(cudaMemcpyAsync(&st->dim_total, &acc, sizeof(acc), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));  // acc is on the host stack
+  }
   k_kry_norm_partials<B><<<nb, nt, 0, s>>>(v, n, pa);
   k_kry_start<<<1, kExpmThreads, 0, s>>>(st, pa, nb, t, tol, P, op->kpoly.p, delta, m, op->skip.p);
   op->launches += 2;
@@ -1840,8 +1851,11 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
 // ceil(m/12) chunks of dimension ceil(m/k), each over t/k.  From the SoA
 // vector `in` (not modified) into `out` (may not alias `in`).  With split_tol
 // each sub-step runs to tol/k, so that the summed estimate of a step whose
-// sub-steps all converged stays within tol.  dim/est (may be null) receive the
-// summed dimension and estimate (-1 when no estimate was formed).
+// sub-steps all converged stays within tol, and a sub-step that misses tol/k
+// ends the step (the later sub-steps are skipped and the estimate reported is
+// that sub-step's times k, above tol): a step that will be rejected costs one
+// sub-step.  dim/est (may be null) receive the summed dimension and estimate
+// (-1 when no estimate was formed).
 template <class B>
 int krylov_steps(dgtd_op* op, const B* in, B* out, double t, int m, double tol, int P, const B* bvec,
                  int64_t src_idx, bool split_tol, int* dim, double* est) {
@@ -1855,7 +1869,7 @@ int krylov_steps(dgtd_op* op, const B* in, B* out, double t, int m, double tol, 
   for (int q = 0; q < k; ++q) {
     B* dst = ((k - 1 - q) % 2 == 0) ? out : mid;
     DGTD_TRY(krylov_chunk<B>(op, cur, tau, chunk, split_tol ? tol / (double)k : tol, P, q * tau, bvec, src_idx, dst,
-                             q == 0));
+                             q == 0, split_tol ? k : 0));
     cur = dst;
   }
   if (dim || est) {

@@ -88,6 +88,8 @@ struct KrylovDev {
   int dim_total;                            // summed dimension
   int est_none;                             // a chunk formed no estimate
   double est_sum;                           // summed a-posteriori estimates
+  int aborted;                              // a chunk missed its tolerance: later chunks are skipped
+  int abort_chunks;                         // > 0: abort mode, the step's number of chunks
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -469,6 +471,14 @@ constexpr size_t kExpmSmem = 5 * kKrylovMaxDim * kKrylovMaxDim * sizeof(double);
 __global__ void k_kry_start(KrylovDev* st, const double* partials, int nblocks, double t, double tol, int P,
                             const double* a, double delta, int max_dim, int* skip) {
   __shared__ double s_sums[kKryRow];
+  if (st->aborted) {  // uniform: an earlier chunk of the step missed its tolerance
+    if (threadIdx.x == 0) {
+      st->dim = 0;
+      st->est = 0.0;
+      *skip = 1;
+    }
+    return;
+  }
   sum_partials(partials, nblocks, 0, s_sums);
   if (threadIdx.x == 0) {
     double shifted[kAugMax], cu[kAugMax];
@@ -605,14 +615,21 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
 __global__ void k_kry_finish_coef(KrylovDev* st) {
   extern __shared__ double sm[];
   const int d = st->dim;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && !st->aborted) {
     st->dim_total += d;
-    if (st->est < 0.0)
+    if (st->est < 0.0) {
       st->est_none = 1;
-    else
+    } else if (st->abort_chunks > 0 && st->est > st->tol) {
+      // abort mode: the chunk ran to its dimension without reaching its
+      // tolerance, so the step fails whatever the later chunks give; they are
+      // skipped and the reported sum is this estimate times the chunk count
+      st->aborted = 1;
+      st->est_sum = st->est * (double)st->abort_chunks;
+    } else {
       st->est_sum += st->est;
+    }
   }
-  if (d == 0) return;
+  if (d == 0 || st->aborted) return;
   double* a = sm;
   double* out = a + kKrylovMaxDim * kKrylovMaxDim;
   double* b = out + kKrylovMaxDim * kKrylovMaxDim;
