@@ -42,8 +42,11 @@ int dgtd_mesh_box_graded_z(int32_t nx, int32_t ny, int32_t nz, double lx, double
                            double ratio, double *nodes, int32_t *tets);
 
 /* MaxwellOperator::new (rhs.rs:805-1000) on a tet mesh.
- * face_port: 4K ints (-1 none) or NULL; materials: K*8 doubles
- * (eps_xyz, mu_xyz, sigma, sigma_m) or NULL for vacuum. */
+ * face_port: 4K ints or NULL: a port index (>= 0), -1 none, or -2 for a face
+ * of an internal PEC plate (OperatorOptions::pec_plates: the face is severed
+ * from its neighbour and gets the PEC ghost state, rhs.rs:862-880; both sides
+ * of the plate carry the code); materials: K*8 doubles (eps_xyz, mu_xyz,
+ * sigma, sigma_m) or NULL for vacuum. */
 int dgtd_host_op_build(const double *nodes, int64_t n_nodes, const int32_t *tets, int64_t n_elem,
                        int32_t order, double flux_alpha, const int32_t *face_port,
                        const double *materials, dgtd_host_op **out);

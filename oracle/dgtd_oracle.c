@@ -379,7 +379,9 @@ static void map_point(const orc_op *op, int e, const double *xi, double *x) {
     }
 }
 
-/* Build the operator.  `face_port` (4K, -1 = none) tags port faces; it may
+#define ORC_PEC_PLATE (-2)
+/* Build the operator.  `face_port` (4K, -1 = none, -2 = a face of an internal
+ * PEC plate, severed from its neighbour on both sides) tags port faces; it may
  * be NULL.  `mat` (K*8: eps[3], mu[3], sigma, sigma_m) may be NULL (vacuum). */
 orc_op *orc_op_build(const double *nodes, int n_nodes, const int *tets, int n_elem, int order,
                      double flux_alpha, const int *face_port, const double *mat) {
@@ -496,6 +498,13 @@ orc_op *orc_op_build(const double *nodes, int n_nodes, const int *tets, int n_el
             int ef = 4 * e + f;
             op->fscale[ef] = 2.0 * area[ef] / fabs(op->det[e]);
             op->port[ef] = face_port ? face_port[ef] : ORC_NONE;
+            if (op->port[ef] == ORC_PEC_PLATE) {
+                /* internal PEC plate: sever the face on this side, the PEC
+                 * ghost state applies (rhs.rs:862-880) */
+                op->port[ef] = ORC_NONE;
+                op->nbr[ef] = ORC_NONE;
+                op->nbr_lf[ef] = 0;
+            }
             if (op->nbr[ef] == ORC_NONE) continue;
             int en = op->nbr[ef], fn = op->nbr_lf[ef];
             for (int m = 0; m < nfp; m++) {

@@ -1795,6 +1795,20 @@ int kry_matvec(dgtd_op* op, const B* v, B* w, const B* bvec, int64_t src_idx, co
   }
 }
 
+// Debug builds (-DDGTD_KRY_TRACE): synchronise after every Krylov launch and
+// report it on stderr.
+#ifdef DGTD_KRY_TRACE
+#define KRY_TRACE(what, j)                                                                       \
+  do {                                                                                         \
+    cudaError_t e__ = cudaStreamSynchronize(s);                                                \
+    std::fprintf(stderr, "kry %s j=%d: %s\n", what, (int)(j), cudaGetErrorString(e__));         \
+  } while (0)
+#else
+#define KRY_TRACE(what, j) \
+  do {                     \
+  } while (0)
+#endif
+
 // One Arnoldi chunk from the SoA vector v (basis slot 0) into `out`: the
 // first n components of exp(t*Aug)[v; e_{P-1}/eta] (P > 0, the source
 // polynomial's coefficients in op->kpoly, shifted by `delta`) or exp(t*A) v
@@ -1826,22 +1840,31 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
     CUDA_TRY(cudaStreamSynchronize(s));  // acc is on the host stack
   }
   k_kry_norm_partials<B><<<nb, nt, 0, s>>>(v, n, pa);
+  KRY_TRACE("norm_partials", -1);
   k_kry_start<<<1, kExpmThreads, 0, s>>>(st, pa, nb, t, tol, P, op->kpoly.p, delta, m, op->skip.p);
+  KRY_TRACE("start", -1);
   op->launches += 2;
   CUDA_TRY(cudaGetLastError());
   for (int j = 0; j < m; ++j) {
     B* w = vb + (int64_t)j * len;  // slot j + 1
     const B* vj = kry_col(v, (const B*)vb, len, j);
     DGTD_TRY(kry_matvec<B>(op, vj, w, bvec, src_idx, st->mv, op->skip.p));
+    KRY_TRACE("matvec", j);
     k_kry_dots<B><<<nb, nt, 0, s>>>(v, vb, len, n, j + 1, w, pa, op->skip.p);
+    KRY_TRACE("dots", j);
     k_kry_update_dots<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    KRY_TRACE("update_dots", j);
     k_kry_update_norm<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    KRY_TRACE("update_norm", j);
     k_kry_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, pa, nb, j, op->skip.p);
+    KRY_TRACE("finish_norm", j);
     op->launches += 4;
     CUDA_TRY(cudaGetLastError());
   }
   k_kry_finish_coef<<<1, kExpmThreads, kExpmSmem, s>>>(st);
+  KRY_TRACE("finish_coef", -1);
   k_kry_lincomb<B><<<nb, nt, 0, s>>>(v, vb, len, n, st, out);
+  KRY_TRACE("lincomb", -1);
   op->launches += 2;
   CUDA_TRY(cudaGetLastError());
   return DGTD_OK;

@@ -226,6 +226,7 @@ struct RefElement {
 // ---------------------------------------------------------------- operator
 
 static const int kFaceLocal[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 2, 3}};
+static const int kPecPlate = -2;  // face_port code of a face of an internal PEC plate
 static const int kFaceOpposite[4] = {3, 1, 2, 0};
 
 struct Operator {
@@ -343,6 +344,14 @@ struct Operator {
         const int64_t ef = 4 * e + f;
         fscale[ef] = 2.0 * area[ef] / std::fabs(det[e]);
         if (face_port) port[ef] = face_port[ef];
+        if (port[ef] == kPecPlate) {
+          // a face of an internal PEC plate: severed from its neighbour (the
+          // other side carries the code too), the PEC ghost state applies
+          // (rhs.rs:862-880)
+          port[ef] = -1;
+          nbr[ef] = -1;
+          nbr_lf[ef] = 0;
+        }
         if (nbr[ef] < 0) continue;
         const int64_t en = nbr[ef];
         const int fn = nbr_lf[ef];

@@ -420,11 +420,12 @@ __device__ void block_expm(const double* a, int d, double* out, double* b, doubl
       for (int j = 0; j < d; ++j) row += fabs(a[i * d + j]);
       nrm = fmax(nrm, row);
     }
+    // squarings: ceil(log2 |a|) + 1 for |a| > 1/2; a non-finite norm (a
+    // Hessenberg matrix that overflowed) gets none, so the result is
+    // non-finite and the caller rejects it, and a finite norm needs at most
+    // 1025 (doubles stay below 2^1024)
     int sq = 0;
-    if (nrm > 0.5) {
-      long v = (long)ceil(log2(nrm)) + 1;
-      sq = v > 0 ? (int)v : 0;
-    }
+    if (nrm > 0.5 && nrm <= 1.7e308) sq = min(1025, (int)ceil(log2(nrm)) + 1);
     s_sq = sq;
   }
   __syncthreads();
@@ -563,8 +564,13 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
     }
     s_hnext = sqrt(s);
     s_break = s_hnext < 1e-12 ? 1 : 0;
-    s_stop = (s_break || d == st->max_dim) ? 1 : 0;
+    const bool bad = !(s_hnext <= 1.7e308);  // a non-finite vector: stop, never passes
+    s_stop = (s_break || bad || d == st->max_dim) ? 1 : 0;
     if (s_break) st->est = 0.0;
+    if (bad) {
+      st->est = INFINITY;
+      s_break = 1;  // no estimate to form
+    }
   }
   __syncthreads();
   const double hnext = s_hnext;
@@ -583,7 +589,8 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
     __syncthreads();
     block_expm(a, d, out, b, t1, t2);
     if (threadIdx.x == 0) {
-      const double est = hnext * fabs(out[(d - 1) * d]);
+      double est = hnext * fabs(out[(d - 1) * d]);
+      if (!(est == est) || isinf(est)) est = INFINITY;  // a non-finite space never passes
       st->est = est;
       if (est < st->tol) s_stop = 1;
     }

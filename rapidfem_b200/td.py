@@ -103,6 +103,26 @@ class TdSession:
         op = O.MaxwellOperator(mesh, order, flux_alpha(flux), face_port=face_port, materials=materials)
         return TdSession(op, c, ports=port_ids)
 
+    @staticmethod
+    def from_model(tagged_mesh, model, order, flux="upwind", c=1.0):
+        """TdSession::from_model (td.rs:203, build.rs:74-259): the operator of a
+        `model.Model` on a `model.TaggedMesh`.  Ports are named by their face
+        tag; a rectangular port's inward normal is the mean inward normal of
+        its faces."""
+        from . import model as M
+
+        mo = M.operator_from_model(tagged_mesh, model, order, flux_alpha(flux), c)
+        normals = mo.op.get("normal").reshape(-1, 4, 3)
+        ports = {}
+        for k, (tag, mode) in enumerate(zip(mo.port_tags, mo.port_modes)):
+            faces = mo.face_port == k
+            n_out = normals[faces].mean(axis=0)
+            n_in = -n_out / max(np.linalg.norm(n_out), 1e-300)
+            ports[tag] = (k, {"faces": faces, "inward_normal": tuple(n_in), "mode": mode})
+        sess = TdSession(mo.op, c, ports=ports)
+        sess.model_operator = mo
+        return sess
+
     # ---- sizes
     def n_dofs(self) -> int:
         return self.op.n_dof
@@ -313,6 +333,17 @@ class ProblemTD:
         self._op = TdSession.from_mesh(mesh, order, flux, self.c, materials, ports)
         self.order = order
         self.flux = flux
+
+    @classmethod
+    def from_model(cls, tagged_mesh, model, *, order=2, flux="upwind", c=C_LIGHT):
+        """ProblemTD(g) of problem/td.py:256-283 for a model on a tagged mesh
+        (this package has no geometry / meshing layer): materials, PML
+        absorbers, rectangular / ABC ports and PEC plates of `model`."""
+        obj = cls.__new__(cls)
+        obj.c = float(c)
+        obj._op = TdSession.from_model(tagged_mesh, model, order, flux, obj.c)
+        obj.order, obj.flux = order, flux
+        return obj
 
     @classmethod
     def box(cls, *, size, cells, order=2, flux="upwind", c=1.0):
