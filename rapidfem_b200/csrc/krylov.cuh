@@ -621,22 +621,28 @@ __global__ void k_kry_finish_norm(KrylovDev* st, const double* partials, int nbl
 // End of a chunk: coef_i = beta * exp(tH)_{i,0} * sig_i over the final dim.
 __global__ void k_kry_finish_coef(KrylovDev* st) {
   extern __shared__ double sm[];
+  __shared__ int s_done;
   const int d = st->dim;
-  if (threadIdx.x == 0 && !st->aborted) {
-    st->dim_total += d;
-    if (st->est < 0.0) {
-      st->est_none = 1;
-    } else if (st->abort_chunks > 0 && st->est > st->tol) {
-      // abort mode: the chunk ran to its dimension without reaching its
-      // tolerance, so the step fails whatever the later chunks give; they are
-      // skipped and the reported sum is this estimate times the chunk count
-      st->aborted = 1;
-      st->est_sum = st->est * (double)st->abort_chunks;
-    } else {
-      st->est_sum += st->est;
+  if (threadIdx.x == 0) {
+    if (!st->aborted) {
+      st->dim_total += d;
+      if (st->est < 0.0) {
+        st->est_none = 1;
+      } else if (st->abort_chunks > 0 && st->est > st->tol) {
+        // abort mode: the chunk ran to its dimension without reaching its
+        // tolerance, so the step fails whatever the later chunks give; they
+        // are skipped and the reported sum is this estimate times the chunk
+        // count
+        st->aborted = 1;
+        st->est_sum = st->est * (double)st->abort_chunks;
+      } else {
+        st->est_sum += st->est;
+      }
     }
+    s_done = (d == 0 || st->aborted) ? 1 : 0;
   }
-  if (d == 0 || st->aborted) return;
+  __syncthreads();
+  if (s_done) return;  // uniform: thread 0 decided for the block
   double* a = sm;
   double* out = a + kKrylovMaxDim * kKrylovMaxDim;
   double* b = out + kKrylovMaxDim * kKrylovMaxDim;
