@@ -289,8 +289,9 @@ int dgtd_op_set_krylov_precision(dgtd_op *op, int bits);
  * DRIVE_FREE: coef ignored) times the polynomial coef[n_coef] as in
  * dgtd_etd_step_poly, is written to the op's second state buffer; `dim_used`
  * and `est` (tol > 0; may be NULL) as dgtd_etd_step_est.  dgtd_etd_commit
- * makes the candidate the state (an accepted step); another dgtd_etd_try
- * replaces it (a rejected one).  No counterpart in the reference, whose
+ * makes the candidate the state (an accepted step, est <= tol); another
+ * dgtd_etd_try replaces it (a rejected one, whose candidate is not a valid
+ * state: its later sub-steps were skipped).  No counterpart in the reference, whose
  * etd_step copies the state to and from the host every step. */
 int dgtd_etd_try(dgtd_op *op, double h, int32_t m, double tol, int32_t n_coef, const double *coef, int drive,
                  int64_t src_dof, int32_t *dim_used, double *est);

@@ -161,12 +161,21 @@ def test_resident_etd_step_matches_host_api(ctx, engine):
     b = np.zeros(n)
     b[dof] = 1.0
     y0 = (0.1 * np.sin(0.3 + 0.017 * np.arange(n))).astype(np.float32)
-    h = 5.0 / rho
     coef = [0.2, 3.0, -10.0]
     gop.upload(y0)
+    # a step too long for its space is rejected (est > tol) after its first
+    # sub-step; halve it until one passes
+    h = 12.0 / rho
     d1, e1 = gop.etd_try(h, 30, 1e-6, coef=coef, drive=("point", dof))
+    tries = 1
+    while e1 > 1e-6:
+        assert d1 <= 10 and tries < 8  # a rejected step stopped after one sub-step of <= 10
+        h *= 0.5
+        d1, e1 = gop.etd_try(h, 30, 1e-6, coef=coef, drive=("point", dof))
+        tries += 1
+    assert tries > 1  # the first try was rejected
     d2, e2 = gop.etd_try(h, 30, 1e-6, coef=coef, drive=("point", dof))  # a retry replaces the candidate
-    assert (d1, e1) == (d2, e2) and 0 <= e1
+    assert (d1, e1) == (d2, e2) and 0 <= e1 <= 1e-6
     gop.etd_commit()
     got = gop.download()
     want, dw, ew = gop.etd_step_poly(y0.astype(np.float64), b, coef, h, 30, 1e-6)
