@@ -146,8 +146,11 @@ def assign_steps(ctx: G.GpuContext, groups: list[BatchGroup], instances: list[In
 class BatchRunner:
     """The groups on the device: one operator per order group with its
     per-element steps, the autotuned stage kernel, and a CUDA graph of
-    `steps_per_graph` LSERK4 steps of every group.  All work goes to one torch
-    stream (`self.stream`); time it with events on that stream."""
+    `steps_per_graph` LSERK4 steps of every group.  Each group runs on its own
+    context and torch stream; the graph forks from the runner's stream
+    (`self.stream`) to the group streams and joins back, so the groups' stage
+    launches overlap (one group's launch tails are filled by the others).
+    Time it with events on `self.stream`."""
 
     def __init__(self, ctx: G.GpuContext, groups: list[BatchGroup], device=0):
         import torch
@@ -155,42 +158,77 @@ class BatchRunner:
         self.torch = torch
         self.ctx = ctx
         self.groups = groups
+        self.device = device
         self.stream = torch.cuda.Stream(device=device)
         ctx.set_stream(self.stream.cuda_stream)
-        self.gops = [G.GpuOperator(ctx, g.op, dt_scale=g.dt_scale) for g in groups]
+        # one context (and stream) per group, so that the groups can overlap
+        self.ctxs = [G.GpuContext(ctx.device) for _ in groups]
+        self.streams = [torch.cuda.Stream(device=device) for _ in groups]
+        for c, st in zip(self.ctxs, self.streams):
+            c.set_stream(st.cuda_stream)
+        self.gops = [G.GpuOperator(c, g.op, dt_scale=g.dt_scale) for c, g in zip(self.ctxs, groups)]
         self.graph = None
         self.steps_per_graph = 0
         self.tuning = []
+
+    def _fork(self):
+        """Group streams wait for the runner's stream."""
+        for st in self.streams:
+            st.wait_stream(self.stream)
+
+    def _join(self):
+        """The runner's stream waits for every group stream."""
+        for st in self.streams:
+            self.stream.wait_stream(st)
 
     @property
     def n_dof(self) -> int:
         return sum(g.n_dof for g in self.groups)
 
+    def load_device(self, ptrs) -> None:
+        """Each group's AoS state from a device pointer, ordered after the work
+        queued on the runner's stream and before what follows it."""
+        self._fork()
+        for gop, ptr in zip(self.gops, ptrs):
+            gop.load_device(ptr)
+        self._join()
+
+    def store_device(self, ptrs) -> None:
+        """Each group's AoS state to a device pointer (ordered as load_device)."""
+        self._fork()
+        for gop, ptr in zip(self.gops, ptrs):
+            gop.store_device(ptr)
+        self._join()
+
     def load(self) -> None:
+        self._fork()
         for g, gop in zip(self.groups, self.gops):
             gop.upload(g.y0)
+        self._join()
 
-    def _time_steps(self, gop, steps: int) -> float:
+    def _time_steps(self, k: int, steps: int) -> float:
+        st = self.streams[k]
         t0 = self.torch.cuda.Event(enable_timing=True)
         t1 = self.torch.cuda.Event(enable_timing=True)
-        t0.record(self.stream)
-        gop.run_lserk(1.0, steps)
-        t1.record(self.stream)
-        self.stream.synchronize()
+        t0.record(st)
+        self.gops[k].run_lserk(1.0, steps)
+        t1.record(st)
+        st.synchronize()
         return t0.elapsed_time(t1) / steps
 
     def autotune(self, trial_steps: int = 2) -> list:
         """Time each available stage kernel per group (after one warm-up step)
         and keep the fastest.  Leaves the initial states loaded."""
         self.tuning = []
-        for g, gop in zip(self.groups, self.gops):
+        self.stream.synchronize()
+        for k, (g, gop) in enumerate(zip(self.groups, self.gops)):
             cands = [nat.ENGINE_FP32] + ([nat.ENGINE_TF32X3] if g.order <= 4 else [])
             times = {}
             for eng in cands:
                 gop.set_engine(eng)
                 gop.upload(g.y0)
                 gop.run_lserk(1.0, 1)
-                times[eng] = self._time_steps(gop, trial_steps)
+                times[eng] = self._time_steps(k, trial_steps)
             best = min(times, key=times.get)
             gop.set_engine(best)
             name = {nat.ENGINE_FP32: "fp32", nat.ENGINE_TF32X3: "tf32x3"}
@@ -207,16 +245,21 @@ class BatchRunner:
         torch = self.torch
         if steps_per_graph < 2 or steps_per_graph % 2:
             raise ValueError("steps_per_graph must be even (the state buffers ping-pong 5 times per step)")
+        self._fork()
         for gop in self.gops:  # kernel attributes are set on the first launch, outside the capture
             gop.run_lserk(1.0, 2)
+        self._join()
         self.load()
         self.stream.synchronize()
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self.ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.graph(g, stream=self.stream):
+            # fork from the capture stream to the group streams, join back
+            for st in self.streams:
+                st.wait_stream(self.stream)
             for gop in self.gops:
                 gop.run_lserk(1.0, steps_per_graph)
-        self.ctx.set_stream(self.stream.cuda_stream)
+            for st in self.streams:
+                self.stream.wait_stream(st)
         self.graph = g
         self.steps_per_graph = steps_per_graph
 
@@ -224,8 +267,10 @@ class BatchRunner:
         """`steps` LSERK4 steps of every instance on `self.stream` (graph
         replays when a graph is captured: steps must be a multiple of it)."""
         if self.graph is None:
+            self._fork()
             for gop in self.gops:
                 gop.run_lserk(1.0, steps)
+            self._join()
             return
         if steps % self.steps_per_graph:
             raise ValueError("steps must be a multiple of steps_per_graph")
@@ -236,6 +281,8 @@ class BatchRunner:
     def states(self, instances: list[Instance]) -> list[np.ndarray]:
         """The AoS f32 state of every instance, in instance order."""
         self.stream.synchronize()
+        for st in self.streams:
+            st.synchronize()
         out = [None] * len(instances)
         for g, gop in zip(self.groups, self.gops):
             y = gop.download()

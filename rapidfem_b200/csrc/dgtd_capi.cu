@@ -386,7 +386,7 @@ int launch_rhs_tc_n(dgtd_op* op, const RhsParams& P) {
 
 template <int MODE>
 int launch_rhs(dgtd_op* op, const RhsParams& P) {
-  if constexpr (MODE == kModeApply || MODE == kModeLserk || MODE == kModeKrylov) {
+  if constexpr (MODE == kModeApply || MODE == kModeLserk || MODE == kModeKrylov || MODE == kModeKcl) {
     if (op->engine == DGTD_ENGINE_TF32X3) {
       switch (op->order) {
         case 1: return launch_rhs_tc_n<1, MODE>(op, P);
@@ -1434,6 +1434,34 @@ namespace {
 
 constexpr long long kKclAttemptCap = 10000000;  // per output frame
 
+// The five stages of one KCL attempt as fused RHS + stage launches: stage s
+// evaluates the RHS at its point (stage 0: the backup of y the attempt began
+// from; later stages: the point the previous stage wrote) and updates y and
+// the embedded error in place, writing the next stage's point into the other
+// of two stage buffers (explicit_adaptive.rs:84-152).
+int kcl_stages(dgtd_op* op, dgtd::KclCtl* dc, float* y, int64_t src_idx, const float* sv, const float* gv) {
+  float* stage_buf[2] = {op->kcl_stage.p, op->kcl_k.p};
+  for (int st = 0; st < 5; ++st) {
+    RhsParams P = base_params(op);
+    P.y_in = st == 0 ? op->kcl_bak.p : stage_buf[(st - 1) & 1];
+    P.skip = &dc->skip;
+    P.src_idx = src_idx;
+    P.src_vec = sv;
+    P.kcl_y = y;
+    P.kcl_e = op->kcl_e.p;
+    P.kcl_next = st < 4 ? stage_buf[st & 1] : nullptr;
+    P.kcl_h = &dc->h_try;
+    P.kcl_frame = &dc->frame;
+    P.kcl_g = gv;
+    P.kcl_b = (float)dgtd::kKclB[st];
+    P.kcl_ew = (float)(dgtd::kKclBhat[st] - dgtd::kKclB[st]);
+    P.kcl_amb = st < 4 ? (float)(dgtd::kKclA[st] - dgtd::kKclB[st]) : 0.f;
+    P.kcl_stage = st;
+    DGTD_TRY(launch_rhs<kModeKcl>(op, P));
+  }
+  return DGTD_OK;
+}
+
 // One adaptive run on the resident state.  Frames are recorded into d_traj
 // (SoA rows, may be null) or as functionals into d_fun (may be null).
 int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, const float* g,
@@ -1483,24 +1511,14 @@ int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, co
   float* y = op->y[op->cur].p;
   auto attempt = [&]() -> int {
     dgtd::k_kcl_begin<<<ng, nt, 0, s>>>(dc, y, op->kcl_bak.p, n);
-    for (int st = 0; st < 5; ++st) {
-      RhsParams P = base_params(op);
-      P.y_in = st == 0 ? y : op->kcl_stage.p;
-      P.out = op->kcl_k.p;
-      P.skip = d_skip;
-      DGTD_TRY(launch_rhs<kModeApply>(op, P));
-      const float b = (float)dgtd::kKclB[st], ew = (float)(dgtd::kKclBhat[st] - dgtd::kKclB[st]);
-      const float amb = st < 4 ? (float)(dgtd::kKclA[st] - dgtd::kKclB[st]) : 0.f;
-      dgtd::k_kcl_stage<<<ng, nt, 0, s>>>(dc, st, b, ew, amb, y, op->kcl_e.p, op->kcl_k.p, op->kcl_stage.p,
-                                          src_idx, sv, gv, n);
-    }
+    DGTD_TRY(kcl_stages(op, dc, y, src_idx, sv, gv));
     dgtd::k_kcl_err<<<ng, 256, 0, s>>>(dc, op->kcl_bak.p, y, op->kcl_e.p, op->kcl_part.p, n);
     dgtd::k_kcl_control<<<1, 256, 0, s>>>(dc, op->kcl_part.p, ng, n);
     dgtd::k_kcl_restore<<<ng, nt, 0, s>>>(dc, y, op->kcl_bak.p, n);
     if (d_traj) dgtd::k_kcl_record_state<<<ng, nt, 0, s>>>(dc, y, d_traj, n);
     if (n_fun > 0)
       dgtd::k_kcl_record_fun<<<(unsigned)n_fun, 256, 0, s>>>(dc, y, d_ptr, d_idx, d_w, d_fun, n_fun);
-    op->launches += 10;
+    op->launches += 5;
     CUDA_TRY(cudaGetLastError());
     return DGTD_OK;
   };
@@ -1585,20 +1603,9 @@ extern "C" int dgtd_kcl_step(dgtd_op* op, const double* y, double h, double* y_o
   c.record = -1;
   dgtd::KclCtl* dc = op->kcl_ctl.p;
   CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
-  const int nt = 256, ng = grid_for(n, nt, op->ctx->num_sms);
   float* yd = op->y[op->cur].p;
-  for (int st = 0; st < 5; ++st) {
-    RhsParams P = base_params(op);
-    P.y_in = st == 0 ? yd : op->kcl_stage.p;
-    P.out = op->kcl_k.p;
-    DGTD_TRY(launch_rhs<kModeApply>(op, P));
-    const float b = (float)dgtd::kKclB[st], ew = (float)(dgtd::kKclBhat[st] - dgtd::kKclB[st]);
-    const float amb = st < 4 ? (float)(dgtd::kKclA[st] - dgtd::kKclB[st]) : 0.f;
-    dgtd::k_kcl_stage<<<ng, nt, 0, s>>>(dc, st, b, ew, amb, yd, op->kcl_e.p, op->kcl_k.p, op->kcl_stage.p, -1,
-                                        nullptr, nullptr, n);
-    op->launches++;
-    CUDA_TRY(cudaGetLastError());
-  }
+  CUDA_TRY(cudaMemcpyAsync(op->kcl_bak.p, yd, state_len(op) * 4, cudaMemcpyDeviceToDevice, s));
+  DGTD_TRY(kcl_stages(op, dc, yd, -1, nullptr, nullptr));
   DGTD_TRY((to_aos<float, double>(op, yd, op->tmp64.p)));
   CUDA_TRY(cudaMemcpyAsync(y_out, op->tmp64.p, n * 8, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));

@@ -39,6 +39,8 @@ enum RhsMode : int {
   kModeLserk = 1,    // fused LSERK4 stage: p = a*p + dt*(dy+src); y_out = y_in + b*p
   kModeKrylov = 3,   // Krylov matvec: out = kry[0]*dy + kry[1]*b (state type in and out;
                      // b = src_vec or the point src_idx; kry in device memory)
+  kModeKcl = 4,      // fused KCL RK4(3)5 stage: f = h (dy + src); y += b f; e (=|+=) ew f;
+                     // next stage point = y + amb f (h, the frame's waveform from device memory)
 };
 
 template <class R>
@@ -65,6 +67,17 @@ struct RhsParamsT {
   const int* skip;         // device flag: when nonzero the launch does nothing (Arnoldi early stop,
                            // adaptive attempts past the end of a run)
   const double* kry;       // Krylov: device {input scale, source coefficient}
+  // KCL stage (kModeKcl): the solution y and embedded error e updated in place,
+  // the next stage's evaluation point (null after the last stage), the
+  // controller's step and frame in device memory, the per-frame waveform
+  R* kcl_y;
+  R* kcl_e;
+  R* kcl_next;
+  const float* kcl_h;
+  const long long* kcl_frame;
+  const float* kcl_g;
+  R kcl_b, kcl_ew, kcl_amb;
+  int kcl_stage;
   int64_t n_elem;
   int64_t src_idx;         // DRIVE_POINT (Lserk, Krylov): SoA index, or -1
   R src_g;                 // held waveform value of the step

@@ -7,7 +7,9 @@
 // memory (KclCtl) and one attempt is a fixed sequence of launches:
 //
 //   k_kcl_begin      back up y, h_try = min(h, dt - t_rel) (session.rs:874)
-//   5 x [RHS apply -> k_kcl_stage]          (explicit_adaptive.rs:84-152)
+//   5 x fused RHS + stage launches (mode kModeKcl of the RHS kernels: the
+//                    stage update of explicit_adaptive.rs:84-152 in the RHS
+//                    epilogue, so the stage derivative never reaches HBM)
 //   k_kcl_err        block partials of sum((e / (atol + rtol max(|y0|,|y1|)))^2)
 //   k_kcl_control    err_norm, accept / reject, PI factor (session.rs:130-187),
 //                    frame bookkeeping, step-collapse check
@@ -89,29 +91,6 @@ __global__ void k_kcl_begin(KclCtl* __restrict__ ctl, const float* __restrict__ 
     if (run) ctl->h_try = fminf(ctl->h, ctl->dt - ctl->t_rel);
     ctl->restore = 0;
     ctl->record = -1;
-  }
-}
-
-// Stage s after k = A Y_s: f = h (k + source), y += b_s f, e (=|+=) (bhat_s - b_s) f,
-// and the next stage's evaluation point Y_{s+1} = y + (a_s - b_s) f.
-// b = b_s, ew = bhat_s - b_s, amb = a_s - b_s (f32 of the f64 rationals, as the
-// reference passes them to kcl.cl).
-__global__ void k_kcl_stage(const KclCtl* __restrict__ ctl, int s, float b, float ew, float amb,
-                            float* __restrict__ y, float* __restrict__ e, const float* __restrict__ k,
-                            float* __restrict__ stage, int64_t src_idx, const float* __restrict__ src_vec,
-                            const float* __restrict__ gvals, int64_t n) {
-  if (ctl->skip) return;
-  const float h = ctl->h_try;
-  const float g = gvals != nullptr ? gvals[ctl->frame] : 0.f;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float kk = k[i];
-    if (src_vec != nullptr) kk += src_vec[i] * g;
-    if (i == src_idx) kk += g;
-    const float f = h * kk;
-    const float yn = y[i] + b * f;
-    y[i] = yn;
-    e[i] = s == 0 ? ew * f : e[i] + ew * f;
-    if (s < 4) stage[i] = yn + amb * f;
   }
 }
 

@@ -315,6 +315,23 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
           if (P.write_p) P.p[g] = pv;
           P.out[g] = fma(P.b, pv, Y[c * NP + i_me]);
         }
+      } else if (MODE == kModeKcl) {
+        // KCL stage (explicit_adaptive.rs:84-152), in the operation order of
+        // the separate stage kernel (kcl.cuh k_kcl_stage)
+        const R h = (R)*P.kcl_h;
+        const R gs = P.kcl_g != nullptr ? (R)P.kcl_g[*P.kcl_frame] : R(0);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const int64_t g = base + c * NP;
+          R kk = dy[c];
+          if (P.src_vec != nullptr) kk += P.src_vec[g] * gs;
+          if (g == P.src_idx) kk += gs;
+          const R f = h * kk;
+          const R yn = P.kcl_y[g] + P.kcl_b * f;
+          P.kcl_y[g] = yn;
+          P.kcl_e[g] = P.kcl_stage == 0 ? P.kcl_ew * f : P.kcl_e[g] + P.kcl_ew * f;
+          if (P.kcl_next != nullptr) P.kcl_next[g] = yn + P.kcl_amb * f;
+        }
       } else {
         // Krylov matvec of a stored basis vector: its scale and the source
         // coefficient of the augmented system come from device memory

@@ -494,6 +494,11 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       kry_sig = (float)P.kry[0];
       kry_g = (float)P.kry[1];
     }
+    float kcl_h = 0.f, kcl_gs = 0.f;
+    if (MODE == kModeKcl) {
+      kcl_h = *P.kcl_h;
+      kcl_gs = P.kcl_g != nullptr ? P.kcl_g[*P.kcl_frame] : 0.f;
+    }
     int ys = 0;
     uint32_t ld_par = 0u;
     for (int64_t it = 0; it < n_my; ++it) {
@@ -522,7 +527,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       float* const prow = sP0 + ps * kYStride + e_row_off;  // p in, p out (LSERK) / dy out (Apply)
       const int64_t t0 = tile * C::TILE_F;
       // do the step's sources reach this tile? (uniform per tile)
-      const bool src_here = (MODE == kModeLserk || MODE == kModeKrylov) &&
+      const bool src_here = (MODE == kModeLserk || MODE == kModeKrylov || MODE == kModeKcl) &&
                             (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
       const int64_t g_row = t0 + e_row_off;  // SoA index of node 0 of this row
       const uint32_t acc = tmem + (uint32_t)(ps * C::ACC) + ((uint32_t)(q4 * 32) << 16);
@@ -560,6 +565,21 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
                 if (P.read_p) pv = fmaf(P.a, prow[i], pv);
                 prow[i] = pv;
                 yrow[i] = fmaf(P.b, pv, yv);
+              } else if (MODE == kModeKcl) {
+                // KCL stage (explicit_adaptive.rs:84-152) straight to global
+                // memory, in the operation order of the separate stage kernel
+                // (kcl.cuh k_kcl_stage); nothing is staged for the bulk store
+                const int64_t g = g_row + i;
+                float kk = dy;
+                if (src_here) {
+                  if (P.src_vec != nullptr) kk += __ldg(P.src_vec + g) * kcl_gs;
+                  if (P.src_idx == g) kk += kcl_gs;
+                }
+                const float f = kcl_h * kk;
+                const float yn = P.kcl_y[g] + P.kcl_b * f;
+                P.kcl_y[g] = yn;
+                P.kcl_e[g] = P.kcl_stage == 0 ? P.kcl_ew * f : P.kcl_e[g] + P.kcl_ew * f;
+                if (P.kcl_next != nullptr) P.kcl_next[g] = yn + P.kcl_amb * f;
               } else if (MODE == kModeKrylov) {
                 // Krylov matvec of a stored basis vector: its scale and the
                 // augmented source coefficient from device memory
@@ -618,10 +638,10 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const float* sp = sP0 + (int)(j & 1) * kYStride;
       if (MODE == kModeApply || MODE == kModeKrylov) {
         tc::bulk_s2g(P.out + gb, sp, C::TILE_B);
-      } else {
+      } else if (MODE == kModeLserk) {
         tc::bulk_s2g(P.out + gb, sy, C::TILE_B);
         if (P.write_p) tc::bulk_s2g(P.p + gb, sp, C::TILE_B);
-      }
+      }  // kModeKcl: the epilogue wrote global memory itself
       tc::bulk_commit();
     };
     if (n_my > 0) load_y(0);
