@@ -11,8 +11,10 @@ RHS stages) over the whole mesh; n_dof = 139,345,920, so every step streams
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 `--impl reference` times the CPU restatement of the reference's CPU path
-(oracle/, f64, all host threads) on a bounded sample of the same workload.
-Under torchrun each rank runs one replica of the workload (weak scaling).
+(oracle/, f64, all host threads) on the same workload within a time budget.
+Under torchrun (N > 1 ranks) the workload is partitioned across the ranks
+with a halo exchange per stage over NCCL (strong scaling); `--replicas` runs
+N independent replicas instead (weak scaling).
 """
 from __future__ import annotations
 
@@ -195,6 +197,134 @@ def run_reference(args):
                 f"({args.ref_budget:.0f} s).",
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_sharded(args):
+    """The 48^3 sphere_pulse workload partitioned across the N ranks (strong
+    scaling): a Morton element partition, one local operator per rank over its
+    owned elements and halo, LSERK4 stages with one halo exchange each over
+    NCCL point-to-point, the interior elements' update overlapping the
+    exchange (partition.ShardedLserk).  `value` counts the global DOFs."""
+    import datetime
+
+    import torch
+
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import operator as O
+    from rapidfem_b200 import partition as PT
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    if world == 1:  # a one-rank group outside torchrun
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(29400 + os.getpid() % 1000))
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    wl = W.sphere_pulse(args.cells, 4)
+    parts = PT.build_parts(wl.mesh, PT.morton_partition(wl.mesh, world), materials=wl.materials)
+    me = parts[rank]
+    op = O.MaxwellOperator(me.mesh, 4, 1.0, materials=me.materials)
+    ctx = G.GpuContext(local)
+    gop = G.GpuOperator(ctx, op)
+    gop.set_engine({"fp32": 0, "tf32x3": 1}[args.engine])
+    eng = PT.GpuEngine(gop, dev)
+    y_local = wl.y0(op).astype(np.float32)  # the pulse at this rank's nodes (owned and halo)
+    n_global = 6 * op.np * wl.mesh.n_tets
+
+    # spectral radius: power iteration on the local operator, max over ranks
+    with torch.cuda.stream(eng.stream):
+        g = torch.Generator(device=dev).manual_seed(rank)
+        v = torch.randn(op.n_dof, device=dev, dtype=torch.float32, generator=g)
+        v /= v.norm()
+        av = torch.empty_like(v)
+        rho = 1.0
+        for _ in range(args.power_iters):
+            gop.apply_device(v.data_ptr(), av.data_ptr())
+            rho = float(av.norm())
+            v = av / rho
+    t = torch.tensor([rho], device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    dt = 0.5 * 2.8 / float(t)
+
+    sharded = PT.ShardedLserk(me, eng, PT.TorchTransport(), overlap=True)
+    eng.load(y_local)
+    torch.distributed.barrier()
+    sharded.step(dt, args.warmup)
+    eng.sync()
+    torch.distributed.barrier()
+    gop.reset_launch_count()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    eng.sync()
+    torch.distributed.barrier()
+    t_start.record(eng.stream)
+    sharded.step(dt, args.steps)
+    t_end.record(eng.stream)
+    eng.sync()
+    torch.distributed.barrier()
+    ms = t_start.elapsed_time(t_end)
+    ck = clocks.stop()
+    launches = gop.launch_count()
+    finite = bool(np.isfinite(eng.state()).all())
+    t = torch.tensor([ms], device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t)
+    value = n_global * 5 * args.steps / (ms * 1e-3)
+    stage_ms = ms / (5 * args.steps)
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_DOF_STAGE[4] * n_global / world / (stage_ms * 1e-3) / 1e9  # per GPU
+
+    # end to end: this rank's part from page-locked host memory, the run, the part back
+    y_host = torch.from_numpy(y_local).pin_memory()
+    y_out = torch.empty(op.n_dof, dtype=torch.float32).pin_memory()
+    y_dev = torch.empty(op.n_dof, dtype=torch.float32, device=dev)
+    eng.sync()
+    torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(eng.stream)
+    with torch.cuda.stream(eng.stream):
+        y_dev.copy_(y_host, non_blocking=True)
+        gop.load_device(y_dev.data_ptr())
+        sharded.step(dt, args.steps)
+        gop.store_device(y_dev.data_ptr())
+        y_out.copy_(y_dev, non_blocking=True)
+    e1.record(eng.stream)
+    eng.sync()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(t)
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(sphere_pulse_config(args.cells, 4, n_global, world),
+                       parallelism=f"element partition x{world} (Morton), one halo exchange per stage over "
+                                   "NCCL point-to-point, the interior update overlapping it"),
+        "run": {"dt": dt, "engine": args.engine, "halo_elements_max": int(max(p.halo.size for p in parts)),
+                "interior_fraction_min": float(min(p.n_interior / p.n_owned for p in parts))},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "stage kernel, per GPU", "stage_ms": stage_ms, "peak_kind": peak_kind},
+        "clocks": ck,
+        "e2e": {"value": n_global * 5 * args.steps / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
+                "h2d_bytes_per_step": op.n_dof * 4 / args.steps, "d2h_bytes_per_step": op.n_dof * 4 / args.steps,
+                "steps": args.steps, "api": "load_device / ShardedLserk.step / store_device per rank"},
+        "finite": finite,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del sharded, eng, gop
+    torch.distributed.barrier()
+    torch.distributed.destroy_process_group()
     return 0
 
 
@@ -814,6 +944,10 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="seconds of timed steps of the reference arm (full workload)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 ranks: N independent replicas instead of the partitioned run")
+    ap.add_argument("--sharded", action="store_true",
+                    help="the partitioned run even on one rank (a one-part partition)")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t", "c2-accuracy"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
                          "c5: the waveguide post variants with port probes; "
@@ -843,6 +977,8 @@ def main():
         return run_c2_accuracy(args)
     if args.workload == "c5":
         return run_c5(args)
+    if (_rank()[1] > 1 and not args.replicas) or args.sharded:
+        return run_sharded(args)
     return run_b200(args)
 
 

@@ -171,6 +171,14 @@ int dgtd_transient_functionals(dgtd_op *op, const float *y0, float dt, int64_t s
  * register (a_0 = 0), stage 4 does not write it.  No reference counterpart:
  * the reference steps whole LSERK4 steps only (gpu/operator.rs:906). */
 int dgtd_lserk_stage(dgtd_op *op, float h, int32_t stage, int drive, int64_t src_dof, float g);
+/* dgtd_lserk_stage on the elements [e_begin, e_end) only, for a partitioned
+ * run that overlaps its halo exchange with the elements that do not need the
+ * halo: e_begin a multiple of 20 (the tensor-core tile), e_end a multiple of
+ * 20 or n_elem.  flip != 0 makes the stage's output the current state (the
+ * last range of a stage); the ranges of one stage read the same input.  No
+ * counterpart in the reference. */
+int dgtd_lserk_stage_range(dgtd_op *op, float h, int32_t stage, int64_t e_begin, int64_t e_end, int32_t flip,
+                           int drive, int64_t src_dof, float g);
 /* Copy element blocks (6*Np f32 each, element-major SoA) of the resident
  * state to / from a device buffer: buf[j*6*Np + r] <-> element d_elems[j].
  * d_elems and d_buf are device pointers.  No counterpart in the reference: the

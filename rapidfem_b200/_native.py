@@ -112,6 +112,7 @@ _sig("dgtd_mlp_gradient", C.c_int, _vp, _pf, _pf, _i64, _pf, C.POINTER(_f32))
 _sig("dgtd_mlp_train", C.c_int, _vp, _pf, _pf, _i64, _i32, _f32, _pf)
 _sig("dgtd_etd_step_est", C.c_int, _vp, _pd, _pd, _f64, _i32, _f64, _pd, C.POINTER(_i32), C.POINTER(_f64))
 _sig("dgtd_lserk_stage", C.c_int, _vp, _f32, _i32, C.c_int, _i64, _f32)
+_sig("dgtd_lserk_stage_range", C.c_int, _vp, _f32, _i32, _i64, _i64, _i32, C.c_int, _i64, _f32)
 _sig("dgtd_state_gather_elements", C.c_int, _vp, _vp, _i64, _vp)
 _sig("dgtd_state_scatter_elements", C.c_int, _vp, _vp, _i64, _vp)
 _sig("dgtd_kcl_step", C.c_int, _vp, _pd, _f64, _pd, _pd)

@@ -325,7 +325,7 @@ int launch_rhs_n(dgtd_op* op, const RhsParams& P) {
     if (bps < 1) return set_error(DGTD_ERR_CUDA, "rhs kernel does not fit on an SM");
   }
   OpTables T{op->dT.p, op->liftT.p, op->fnodes.p, op->gtab.p, op->n_gather};
-  const int64_t tiles = (op->n_elem + C::E - 1) / C::E;
+  const int64_t tiles = (P.n_elem - P.e_begin + C::E - 1) / C::E;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms * bps);
   kern<<<grid, C::THREADS, C::SMEM, op->stream()>>>(P, T);
   op->launches++;
@@ -345,7 +345,7 @@ int launch_rhs64_n(dgtd_op* op, const RhsParamsT<double>& P) {
     if (bps < 1) return set_error(DGTD_ERR_CUDA, "fp64 rhs kernel does not fit on an SM");
   }
   OpTablesT<double> T{op->dT64.p, op->liftT64.p, op->fnodes.p, op->gtab.p, op->n_gather};
-  const int64_t tiles = (op->n_elem + C::E - 1) / C::E;
+  const int64_t tiles = (P.n_elem - P.e_begin + C::E - 1) / C::E;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms * bps);
   kern<<<grid, C::THREADS, C::SMEM, op->stream()>>>(P, T);
   op->launches++;
@@ -376,7 +376,9 @@ int launch_rhs_tc_n(dgtd_op* op, const RhsParams& P) {
     attr[op->ctx->device & 7] = true;
   }
   TcTables T{op->tc_bvol.p, op->tc_blift.p, op->fnodes.p, op->gtab.p, op->n_gather};
-  const int64_t tiles = op->n_elem_pad / C::E;
+  // whole tiles: a range ending at the op's last element runs to the padded end
+  const int64_t end = P.n_elem >= op->n_elem ? op->n_elem_pad : P.n_elem;
+  const int64_t tiles = (end - P.e_begin) / C::E;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)op->ctx->num_sms);
   kern<<<grid, kTcThreadsAll, C::SMEM, op->stream()>>>(P, T, tiles, op->err.p);
   op->launches++;
@@ -900,12 +902,24 @@ extern "C" int dgtd_state_scatter_elements(dgtd_op* op, const int64_t* d_elems, 
 }
 
 extern "C" int dgtd_lserk_stage(dgtd_op* op, float h, int32_t stage, int drive, int64_t src_dof, float g) {
+  if (!op) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: null op");
+  return dgtd_lserk_stage_range(op, h, stage, 0, op->n_elem, 1, drive, src_dof, g);
+}
+
+extern "C" int dgtd_lserk_stage_range(dgtd_op* op, float h, int32_t stage, int64_t e_begin, int64_t e_end,
+                                      int32_t flip, int drive, int64_t src_dof, float g) {
   if (!op || stage < 0 || stage > 4) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: stage must be 0..4");
   if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: step must be positive");
+  if (e_begin < 0 || e_end > op->n_elem || e_begin >= e_end || (e_begin % kTcTileE) != 0 ||
+      ((e_end % kTcTileE) != 0 && e_end != op->n_elem))
+    return set_error(DGTD_ERR_BAD_ARG, "lserk_stage_range: need 0 <= e_begin < e_end <= n_elem, e_begin a "
+                                       "multiple of 20 and e_end a multiple of 20 or n_elem");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   int64_t src_idx;
   DGTD_TRY(check_drive(op, drive, src_dof, &g, 1, &src_idx));
   RhsParams P = base_params(op);
+  P.e_begin = e_begin;
+  P.n_elem = e_end;
   P.y_in = op->y[op->cur].p;
   P.out = op->y[op->cur ^ 1].p;
   P.p = op->p.p;
@@ -918,7 +932,7 @@ extern "C" int dgtd_lserk_stage(dgtd_op* op, float h, int32_t stage, int drive, 
   P.src_vec = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
   P.src_g = drive == DGTD_DRIVE_FREE ? 0.f : g;
   DGTD_TRY(launch_rhs<kModeLserk>(op, P));
-  op->cur ^= 1;
+  if (flip) op->cur ^= 1;
   return DGTD_OK;
 }
 

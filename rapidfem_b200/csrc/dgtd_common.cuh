@@ -78,7 +78,8 @@ struct RhsParamsT {
   const float* kcl_g;
   R kcl_b, kcl_ew, kcl_amb;
   int kcl_stage;
-  int64_t n_elem;
+  int64_t n_elem;          // elements [e_begin, n_elem) are computed
+  int64_t e_begin;         // first element (a multiple of the tensor-core tile, 20); 0 for the whole op
   int64_t src_idx;         // DRIVE_POINT (Lserk, Krylov): SoA index, or -1
   R src_g;                 // held waveform value of the step
   R a, b, dt;              // LSERK stage coefficients

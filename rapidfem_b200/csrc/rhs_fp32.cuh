@@ -97,13 +97,13 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
     kry_g = (R)P.kry[1];
   }
 
-  const int64_t n_tiles = (P.n_elem + E - 1) / E;
+  const int64_t n_tiles = (P.n_elem - P.e_begin + E - 1) / E;
   const int le_me = tid / NP;
   const int i_me = tid - le_me * NP;
   const bool owns = tid < E * NP;
 
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    const int64_t e0 = tile * E;
+    const int64_t e0 = P.e_begin + tile * E;
     const int ne = (int)((P.n_elem - e0) < E ? (P.n_elem - e0) : E);
     __syncthreads();  // previous tile fully consumed (and tables loaded on the first pass)
     // ---- 1. state tile and element records -> shared memory

@@ -221,6 +221,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   uint8_t* const sFn = tsm + C::O_TAB;
   uint8_t* const sG = sFn + 4 * NFP;
   const bool use_p = MODE == kModeLserk && P.read_p;
+  const int64_t tile0 = P.e_begin / E;  // the launch covers tiles [tile0, tile0 + n_tiles)
   const int64_t n_my =
       n_tiles > (int64_t)blockIdx.x ? (n_tiles - (int64_t)blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
@@ -347,7 +348,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     int ys = 0;
     uint32_t ld_par = 0u;  // bit s: parity of the next wait on bar_ld[s]
     for (int64_t it = 0; it < n_my; ++it) {
-      const int64_t tile = blockIdx.x + it * gridDim.x;
+      const int64_t tile = tile0 + blockIdx.x + it * gridDim.x;
       const int64_t e0 = tile * E;
       const float* const sY = sY0 + ys * kYStride;
       const float* const sM = sM0 + ys * kMStride;
@@ -502,7 +503,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     int ys = 0;
     uint32_t ld_par = 0u;
     for (int64_t it = 0; it < n_my; ++it) {
-      const int64_t tile = blockIdx.x + it * gridDim.x;
+      const int64_t tile = tile0 + blockIdx.x + it * gridDim.x;
       const int ps = (int)(it & 1);
       const uint32_t ppar = (uint32_t)((it >> 1) & 1);
       bool ok = tc_waitw(&bar_mma[ps], ppar, abort_flag);
@@ -619,7 +620,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     const uint64_t dal = tc::tf32_step_desc(tc::smem_u32(all), M, 0);
     auto load_y = [&](int64_t j) {  // tile j of this CTA -> slot j % 3
       const int s = (int)(j % 3);
-      const int64_t tile = blockIdx.x + j * gridDim.x;
+      const int64_t tile = tile0 + blockIdx.x + j * gridDim.x;
       tc::mbar_expect_tx(&bar_ld[s], C::TILE_B + C::META_B);
       tc::bulk_g2s(sY0 + s * kYStride, P.y_in + tile * C::TILE_F, C::TILE_B, &bar_ld[s]);
       tc::bulk_g2s(sM0 + s * kMStride, P.meta + tile * E * kMetaWords, C::META_B, &bar_ld[s]);
@@ -627,13 +628,13 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     };
     auto load_p = [&](int64_t j) {  // residual register of tile j -> slot j & 1
       const int s = (int)(j & 1);
-      const int64_t tile = blockIdx.x + j * gridDim.x;
+      const int64_t tile = tile0 + blockIdx.x + j * gridDim.x;
       tc::mbar_expect_tx(&bar_p[s], C::TILE_B);
       tc::bulk_g2s(sP0 + s * kYStride, P.p + tile * C::TILE_F, C::TILE_B, &bar_p[s]);
       ++n_p[s];
     };
     auto store = [&](int64_t j) {
-      const int64_t gb = ((int64_t)blockIdx.x + j * gridDim.x) * C::TILE_F;
+      const int64_t gb = (tile0 + (int64_t)blockIdx.x + j * gridDim.x) * C::TILE_F;
       const float* sy = sY0 + (int)(j % 3) * kYStride;
       const float* sp = sP0 + (int)(j & 1) * kYStride;
       if (MODE == kModeApply || MODE == kModeKrylov) {

@@ -312,6 +312,15 @@ class GpuOperator:
             raise ValueError("set a vector drive with set_source_vector first and pass ('vector', None)")
         check(lib.dgtd_lserk_stage(self._h, float(h), int(stage), kind, dof, float(g)))
 
+    def lserk_stage_range(self, h, stage, e_begin, e_end, flip, drive=None, g=0.0):
+        """One fused LSERK4 stage on elements [e_begin, e_end) of the resident
+        state (dgtd_lserk_stage_range); `flip` on the last range of a stage."""
+        kind, dof, vec = self._drive(drive)
+        if vec is not None:
+            raise ValueError("set a vector drive with set_source_vector first and pass ('vector', None)")
+        check(lib.dgtd_lserk_stage_range(self._h, float(h), int(stage), int(e_begin), int(e_end),
+                                         1 if flip else 0, kind, dof, float(g)))
+
     def gather_elements(self, d_elems: int, n: int, d_buf: int) -> None:
         """Element blocks (6*Np f32) of the resident state into a device buffer."""
         check(lib.dgtd_state_gather_elements(self._h, d_elems, int(n), d_buf))

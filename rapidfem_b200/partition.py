@@ -72,10 +72,17 @@ def morton_partition(mesh: Mesh, n_parts: int) -> np.ndarray:
     return part
 
 
+TILE = 20  # elements per tensor-core tile: stage ranges start on a tile
+
+
 @dataclass
 class Part:
     """One rank's piece: local element k < n_owned is owned[k], local element
-    n_owned + j is halo[j] (global ids)."""
+    n_owned + j is halo[j] (global ids).  The owned elements come in two runs:
+    the first n_interior (a multiple of TILE) have no face neighbour in the
+    halo, so their stage update needs no exchange and can overlap it; the
+    rest (and the halo rows, whose updates are discarded) follow once the
+    halo has arrived."""
 
     rank: int
     owned: np.ndarray
@@ -85,6 +92,7 @@ class Part:
     materials: np.ndarray | None
     send: dict = field(default_factory=dict)  # peer -> local ids of owned elements to send
     recv: dict = field(default_factory=dict)  # peer -> local ids of halo slots to fill
+    n_interior: int = 0
 
     @property
     def n_owned(self) -> int:
@@ -100,9 +108,12 @@ class Part:
 
 
 def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None) -> list[Part]:
-    """The per-rank pieces of a partition `part[K]` (rank ids 0..R-1).  Send and
-    receive lists of a pair of ranks list the same global elements in the same
-    (ascending global id) order."""
+    """The per-rank pieces of a partition `part[K]` (rank ids 0..R-1).  Owned
+    elements are ordered interior first (no face neighbour owned elsewhere;
+    the interior run is cut to a multiple of TILE, the cut-off interior
+    elements join the boundary run), each run in ascending global id.  Send
+    and receive lists of a pair of ranks list the same global elements in the
+    same (ascending global id) order."""
     part = np.asarray(part, dtype=np.int64)
     K = mesh.n_tets
     if part.shape != (K,):
@@ -112,9 +123,15 @@ def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None) ->
     tets = np.asarray(mesh.tets, dtype=np.int64)
     fp = None if face_port is None else np.asarray(face_port, dtype=np.int32).reshape(K, 4)
     mat = None if materials is None else np.asarray(materials, dtype=np.float64).reshape(K, -1)
+    # an element is on the cut if a face neighbour belongs to another rank
+    nbr_part = np.where(nbr >= 0, part[np.maximum(nbr, 0)], -1)
+    on_cut = np.any((nbr >= 0) & (nbr_part != part[:, None]), axis=1)
     parts = []
     for r in range(R):
-        owned = np.flatnonzero(part == r)
+        mine = np.flatnonzero(part == r)
+        inner = mine[~on_cut[mine]]
+        n_int = (inner.size // TILE) * TILE
+        owned = np.concatenate([inner[:n_int], np.sort(np.concatenate([inner[n_int:], mine[on_cut[mine]]]))])
         nb = nbr[owned].ravel()
         nb = nb[nb >= 0]
         halo = np.unique(nb[part[nb] != r])
@@ -122,19 +139,26 @@ def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None) ->
         verts, inv = np.unique(tets[elems].ravel(), return_inverse=True)
         local = Mesh(np.ascontiguousarray(mesh.nodes[verts]), inv.reshape(-1, 4).astype(np.int32))
         parts.append(Part(r, owned, halo, local, None if fp is None else np.ascontiguousarray(fp[elems]),
-                          None if mat is None else np.ascontiguousarray(mat[elems])))
+                          None if mat is None else np.ascontiguousarray(mat[elems]), n_interior=n_int))
     for r, pr in enumerate(parts):
+        elems = pr.elements
+        order = np.argsort(elems, kind="stable")
+        srt = elems[order]
+
+        def local_ids(glob):  # local index of each global id (all present)
+            return order[np.searchsorted(srt, glob)].astype(np.int64)
+
         for q in range(R):
             if q == r:
                 continue
             # elements r owns that q keeps as halo: what r sends to q
             s_glob = parts[q].halo[part[parts[q].halo] == r]
             if s_glob.size:
-                pr.send[q] = np.searchsorted(pr.owned, s_glob).astype(np.int64)
+                pr.send[q] = local_ids(s_glob)
             # elements q owns that r keeps as halo: what r receives from q
             r_glob = pr.halo[part[pr.halo] == q]
             if r_glob.size:
-                pr.recv[q] = (pr.n_owned + np.searchsorted(pr.halo, r_glob)).astype(np.int64)
+                pr.recv[q] = local_ids(r_glob)
     return parts
 
 
@@ -158,14 +182,17 @@ def join_state(parts: list[Part], locals_: list[np.ndarray], np_: int) -> np.nda
 class GpuEngine:
     """The device operator of one part, for ShardedLserk / LoopbackLserk.
 
-    Every kernel of the operator, the exchange buffers and the transport's
-    collectives run on ONE torch CUDA stream, which the operator's context is
-    bound to.  NCCL point-to-point operations issued under `comm()` wait for
-    the gathers queued before them on that stream, and their completion is
-    waited for on that stream before the scatters that follow, so an exchange
-    needs no host synchronisation.  Engines whose operators share a context
-    (all parts on one device) share its stream: the first engine of a context
-    binds it (`stream`, or a new torch stream), the others reuse it."""
+    The operator's kernels run on one torch CUDA stream (`stream`) that the
+    operator's context is bound to; the transport's collectives and the halo
+    scatter run on a second stream (`comm_stream`).  The ordering is by
+    stream waits, so an exchange needs no host synchronisation:
+    `begin_exchange` makes the communication stream wait for the gathers
+    queued on the compute stream, and `end_exchange` makes the compute stream
+    wait for the scatters.  NCCL point-to-point operations issued under
+    `comm()` wait for the work queued on the communication stream, and
+    `req.wait()` makes that stream wait for their completion.  Engines whose
+    operators share a context (all parts on one device) share its streams:
+    the first engine of a context binds them, the others reuse them."""
 
     def __init__(self, gop, device, stream=None):
         import torch
@@ -178,9 +205,11 @@ class GpuEngine:
             bound = stream if stream is not None else torch.cuda.Stream(device=device)
             gop.ctx.set_stream(bound.cuda_stream)
             gop.ctx._engine_stream = bound
+            gop.ctx._engine_comm_stream = torch.cuda.Stream(device=device)
         elif stream is not None and stream is not bound:
             raise ValueError("engines of one context must share its stream")
         self.stream = bound
+        self.comm_stream = gop.ctx._engine_comm_stream
         self.bs = 6 * gop.host_op.np
         self._idx = {}
 
@@ -199,20 +228,38 @@ class GpuEngine:
             return self.torch.empty(n_elem * self.bs, dtype=self.torch.float32, device=self.device)
 
     def comm(self):
-        """Context in which the transport issues its operations (this engine's stream)."""
-        return self.torch.cuda.stream(self.stream)
+        """Context in which the transport issues its operations (the communication stream)."""
+        return self.torch.cuda.stream(self.comm_stream)
+
+    def begin_exchange(self) -> None:
+        """The communication stream waits for what the compute stream queued (the gathers)."""
+        self.comm_stream.wait_stream(self.stream)
+
+    def end_exchange(self) -> None:
+        """The compute stream waits for the communication stream (received and scattered halo)."""
+        self.stream.wait_stream(self.comm_stream)
 
     def gather(self, ids: np.ndarray, buf) -> None:
         self.gop.gather_elements(self._index(ids).data_ptr(), ids.size, buf.data_ptr())
 
     def scatter(self, ids: np.ndarray, buf) -> None:
-        self.gop.scatter_elements(self._index(ids).data_ptr(), ids.size, buf.data_ptr())
+        """Received blocks into the halo rows, on the communication stream."""
+        ctx = self.gop.ctx
+        ctx.set_stream(self.comm_stream.cuda_stream)
+        try:
+            self.gop.scatter_elements(self._index(ids).data_ptr(), ids.size, buf.data_ptr())
+        finally:
+            ctx.set_stream(self.stream.cuda_stream)
 
     def stage(self, h: float, s: int) -> None:
         self.gop.lserk_stage(h, s)
 
+    def stage_range(self, h: float, s: int, e_begin: int, e_end: int, flip: bool) -> None:
+        self.gop.lserk_stage_range(h, s, e_begin, e_end, flip)
+
     def sync(self) -> None:
         self.stream.synchronize()
+        self.comm_stream.synchronize()
 
     def load(self, y_local) -> None:
         self.gop.upload(np.asarray(y_local, dtype=np.float32))
@@ -243,45 +290,71 @@ class TorchTransport:
 
 
 class ShardedLserk:
-    """LSERK4 on one part: per stage, the halo exchange, then one fused stage of
-    the local operator (explicit.rs:100-135 with the exchange before each RHS)."""
+    """LSERK4 on one part (explicit.rs:100-135 with a halo exchange before each
+    RHS).  With `overlap` (and an engine with stage ranges) a stage is
+    [gather | exchange + scatter on the communication stream | the interior
+    elements' update on the compute stream | wait | the boundary and halo
+    elements' update], so the exchange runs under the interior update;
+    otherwise [exchange, fused stage]."""
 
-    def __init__(self, part: Part, engine, transport):
+    def __init__(self, part: Part, engine, transport, overlap: bool = True):
         self.part = part
         self.engine = engine
         self.transport = transport
         self.sbuf = {q: engine.new_buffer(ids.size) for q, ids in part.send.items()}
         self.rbuf = {q: engine.new_buffer(ids.size) for q, ids in part.recv.items()}
+        self.overlap = bool(overlap) and hasattr(engine, "stage_range") and part.n_interior > 0
 
-    def exchange(self) -> None:
+    def begin_exchange(self) -> None:
         """Gather the blocks peers need, move them, scatter the received ones.
-        A device engine orders the three on its stream (no host wait); an
-        engine without `comm()` works synchronously on the host."""
+        A device engine queues the gathers on its compute stream and the rest
+        on its communication stream (no host wait); an engine without `comm()`
+        works synchronously on the host."""
         for q, ids in self.part.send.items():
             self.engine.gather(ids, self.sbuf[q])
         comm = getattr(self.engine, "comm", None)
         if comm is None:
             self.transport.exchange(self.sbuf, self.rbuf)
         else:
+            self.engine.begin_exchange()
             with comm():
                 self.transport.exchange(self.sbuf, self.rbuf)
         for q, ids in self.part.recv.items():
             self.engine.scatter(ids, self.rbuf[q])
 
+    def end_exchange(self) -> None:
+        if hasattr(self.engine, "end_exchange"):
+            self.engine.end_exchange()
+
+    def exchange(self) -> None:
+        self.begin_exchange()
+        self.end_exchange()
+
     def step(self, h: float, steps: int = 1) -> None:
+        n_int, n_loc = self.part.n_interior, self.part.n_local
         for _ in range(int(steps)):
             for s in range(5):
-                self.exchange()
-                self.engine.stage(h, s)
+                if self.overlap:
+                    self.begin_exchange()
+                    self.engine.stage_range(h, s, 0, n_int, False)
+                    self.end_exchange()
+                    self.engine.stage_range(h, s, n_int, n_loc, True)
+                else:
+                    self.exchange()
+                    self.engine.stage(h, s)
 
 
 class LoopbackLserk:
     """All parts of a partition in one process (one device or the CPU): the
-    exchange copies each pair's blocks through a buffer of the sender."""
+    exchange copies each pair's blocks through a buffer of the sender.  With
+    `split` (and engines with stage ranges) each stage updates the interior
+    elements before the scatter and the rest after it, as an overlapped
+    sharded run does."""
 
-    def __init__(self, parts: list[Part], engines: list):
+    def __init__(self, parts: list[Part], engines: list, split: bool = False):
         self.parts = parts
         self.engines = engines
+        self.split = bool(split)
         self.bufs = {(r, q): engines[r].new_buffer(ids.size) for r, p in enumerate(parts) for q, ids in p.send.items()}
 
     def exchange(self) -> None:
@@ -299,6 +372,23 @@ class LoopbackLserk:
     def step(self, h: float, steps: int = 1) -> None:
         for _ in range(int(steps)):
             for s in range(5):
-                self.exchange()
+                if not self.split:
+                    self.exchange()
+                    for e in self.engines:
+                        e.stage(h, s)
+                    continue
+                for r, p in enumerate(self.parts):
+                    for q, ids in p.send.items():
+                        self.engines[r].gather(ids, self.bufs[(r, q)])
                 for e in self.engines:
-                    e.stage(h, s)
+                    e.sync()
+                for e, p in zip(self.engines, self.parts):
+                    if p.n_interior > 0:
+                        e.stage_range(h, s, 0, p.n_interior, False)
+                for r, p in enumerate(self.parts):
+                    for q, ids in p.recv.items():
+                        self.engines[r].scatter(ids, self.bufs[(q, r)])
+                for e in self.engines:
+                    e.sync()
+                for e, p in zip(self.engines, self.parts):
+                    e.stage_range(h, s, p.n_interior, p.n_local, True)

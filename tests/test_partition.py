@@ -27,6 +27,7 @@ class OracleEngine:
         self.a, self.b = R.lserk_coeffs()
         self.y = None
         self.p = None
+        self._out = None
 
     def new_buffer(self, n_elem):
         return torch.empty(n_elem * self.bs, dtype=torch.float64)
@@ -41,6 +42,20 @@ class OracleEngine:
         k = self.orc.apply(self.y)
         self.p = h * k if s == 0 else self.a[s] * self.p + h * k
         self.y = self.y + self.b[s] * self.p
+
+    def stage_range(self, h, s, e_begin, e_end, flip):
+        """The stage on elements [e_begin, e_end) only; the ranges of a stage
+        read the same input, the last one (flip) makes the output current."""
+        if self._out is None:
+            self._out = (self.y.copy(), np.zeros_like(self.y) if self.p is None else self.p.copy())
+        y_out, p_out = self._out
+        k = self.orc.apply(self.y)
+        r = slice(e_begin * self.bs, e_end * self.bs)
+        p_out[r] = h * k[r] if s == 0 else self.a[s] * self.p[r] + h * k[r]
+        y_out[r] = self.y[r] + self.b[s] * p_out[r]
+        if flip:
+            self.y, self.p = y_out, p_out
+            self._out = None
 
     def sync(self):
         pass
@@ -76,6 +91,10 @@ def test_parts_are_consistent():
             r_ids = parts[q].recv[p.rank]
             assert np.array_equal(p.owned[ids], parts[q].elements[r_ids])
         assert set(p.recv) == {q for q in range(3) if p.rank in parts[q].send}
+        # the interior run: whole tiles of elements with no face neighbour elsewhere
+        assert p.n_interior % PT.TILE == 0
+        inner = nbr[p.owned[:p.n_interior]].ravel()
+        assert np.all(np.isin(inner[inner >= 0], p.owned))
 
 
 def _global_run(mesh, port, mat, order, y0, h, steps):
@@ -130,6 +149,25 @@ def test_gloo_world2_matches_single_domain():
         mp.spawn(_rank_main, args=(2, port_no, tmp), nprocs=2, join=True)
         parts = PT.build_parts(mesh, PT.morton_partition(mesh, 2), face_port=port, materials=mat)
         got = PT.join_state(parts, [np.load(os.path.join(tmp, f"y{r}.npy")) for r in range(2)], orc.np)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+def test_loopback_split_stages_match_single_domain():
+    """Each stage as [interior elements | halo scatter | boundary and halo
+    elements], the order of an overlapped sharded run."""
+    mesh = O.structured_box_jittered(6, 5, 4, 1.0, 0.8, 0.9, 0.1, 9)
+    order = 2
+    orc = R.Operator(mesh.nodes, mesh.tets, order, 1.0)
+    y0 = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    h = 0.5 / orc.power_rho(30)[0]
+    want = orc.lserk(y0, h, 3)
+    parts = PT.build_parts(mesh, PT.morton_partition(mesh, 2))
+    assert all(p.n_interior >= 2 * PT.TILE for p in parts)
+    engines = [OracleEngine(p, order) for p in parts]
+    for e, yl in zip(engines, PT.split_state(parts, y0, orc.np)):
+        e.load(yl)
+    PT.LoopbackLserk(parts, engines, split=True).step(h, 3)
+    got = PT.join_state(parts, [e.state() for e in engines], orc.np)
     assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
 
 
