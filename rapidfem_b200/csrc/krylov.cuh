@@ -172,19 +172,6 @@ template <> struct KryVec<double> {
   }
 };
 
-// 8-byte vectors (2 floats), for the sweep that also writes w: half the
-// registers per column, so two CTAs fit on an SM.
-template <class B> struct KryVecHalf;
-template <> struct KryVecHalf<float> {
-  using T = float2;
-  static constexpr int W = 2;
-  __device__ static double at(const float2& v, int q) { return q == 0 ? v.x : v.y; }
-  __device__ static void set(float2& v, int q, double x) {
-    if (q == 0) v.x = (float)x; else v.y = (float)x;
-  }
-};
-template <> struct KryVecHalf<double> : KryVec<double> {};
-
 // partials[b*kKryRow + i] = sum over this block's k of V_i[k] * w[k], i < cols,
 // and w . w in the norm column.
 template <class B>
@@ -255,12 +242,12 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* sums, int 
 
 // First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads, 2)
+__global__ void __launch_bounds__(kKrylovThreads, 1)
 k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
   if (*skip) return;
-  using KV = KryVecHalf<B>;
+  using KV = KryVec<B>;
   using T = typename KV::T;
   __shared__ double u[kKryCols];
   __shared__ double sums[kKryRow];
