@@ -325,6 +325,63 @@ class TdSession:
         return np.array(rows), None
 
 
+class TdTrajectory(np.ndarray):
+    """A field trajectory [n_snapshot, n_dofs] (problem/td.py:170-192): an
+    ndarray that also carries the problem and the frame step."""
+
+    def __new__(cls, data, *, problem=None, dt=None):
+        obj = np.ascontiguousarray(data, dtype=np.float64).view(cls)
+        obj._problem = problem
+        obj._dt = dt
+        return obj
+
+    def __array_finalize__(self, obj):
+        if obj is None:
+            return
+        self._problem = getattr(obj, "_problem", None)
+        self._dt = getattr(obj, "_dt", None)
+
+
+class TdODE:
+    """The problem as the linear ODE dy/dt = A y for an external integrator
+    (problem/td.py:47-72): `rhs(t, y)` has scipy's solve_ivp signature and
+    runs on the device.  The assembled sparse A (`jacobian`) is not built on
+    this path."""
+
+    def __init__(self, problem):
+        self._p = problem
+        self.n_dofs = problem.n_dofs
+
+    def rhs(self, t, y):
+        return self._p._op.apply(y)
+
+    def jacobian(self, t=None, y=None):
+        raise NotImplementedError("the assembled sparse operator (state_space) is not built on the B200 path; "
+                                  "use rhs(t, y), which applies it on the device")
+
+    def __repr__(self):
+        return f"TdODE(n_dofs={self.n_dofs})"
+
+
+class TdStepper:
+    """A one-step propagator bound to a fixed dt (problem/td.py:75-98): the
+    exponential step, or LSERK4 sub-stepped to its stability limit."""
+
+    def __init__(self, problem, dt, krylov_dim, method="exponential"):
+        self._p = problem
+        self.dt = float(dt)
+        self.krylov_dim = int(krylov_dim)
+        self.method = method
+
+    def __call__(self, y):
+        frames, _ = self._p._op.transient(np.asarray(y, dtype=np.float64), dt=self.dt, steps=1,
+                                          method=self.method, krylov_dim=self.krylov_dim, verbose=False)
+        return frames[-1]
+
+    def __repr__(self):
+        return f"TdStepper(dt={self.dt:g}, method={self.method!r})"
+
+
 class ProblemTD:
     """problem/td.py:195-750 on the B200 path (box cavities and tet meshes)."""
 
@@ -381,6 +438,16 @@ class ProblemTD:
     def cfl_dt(self, *, recompute=False):
         return self._op.cfl_dt(recompute)
 
+    def ode(self):
+        """The problem as dy/dt = A y for an external integrator (problem/td.py:381)."""
+        return TdODE(self)
+
+    def stepper(self, dt, *, krylov_dim=40, method="exponential"):
+        """A reusable one-step propagator bound to `dt` (problem/td.py:487)."""
+        if method not in ("exponential", "explicit"):
+            raise ValueError("method must be 'exponential' or 'explicit'")
+        return TdStepper(self, dt, krylov_dim, method)
+
     def probe_dof(self, point, *, field="E", component="z"):
         return self._op.nearest_node_dof(tuple(float(x) for x in point), field, component)
 
@@ -400,7 +467,7 @@ class ProblemTD:
                                        waveform=waveform, method=method, device=device,
                                        krylov_dim=int(krylov_dim), warmup=int(warmup), verbose=verbose,
                                        port_probes=port_probes)
-        return frames
+        return TdTrajectory(frames, problem=self, dt=float(dt))
 
     def port_signals(self, traj, ports, *, dt=None):
         """Modal amplitude P_e(t) of each port over a trajectory (problem/td.py:612):

@@ -52,3 +52,30 @@ def test_problem_driven_transient_shapes():
                                    steps=20, verbose=False)
     assert t.shape == (21,) and series.shape == (2, 21)
     assert np.all(np.isfinite(series)) and np.abs(series).max() > 0
+
+
+def test_stepper_ode_and_trajectory():
+    """ProblemTD.stepper / ode and the TdTrajectory return type
+    (problem/td.py:47-98, :170-192, :381, :487)."""
+    from rapidfem_b200 import td as TD
+
+    p = TD.ProblemTD.box(size=(1, 1, 1), cells=(2, 2, 2), order=2)
+    n = p.n_dofs
+    y0 = np.sin(0.3 + 0.017 * np.arange(n))
+    dt = 0.5 * p.cfl_dt()
+    traj = p.transient(y0, dt=dt, steps=3, method="explicit", verbose=False)
+    assert isinstance(traj, TD.TdTrajectory) and traj.shape == (4, n) and traj._dt == dt
+    st = p.stepper(dt, method="explicit")
+    y = y0
+    for _ in range(3):
+        y = st(y)
+    assert np.allclose(y, traj[-1], rtol=0, atol=1e-6 * np.max(np.abs(traj[-1])))
+    ode = p.ode()
+    assert ode.n_dofs == n
+    assert np.array_equal(ode.rhs(0.0, y0), p.rhs(y0))
+    with pytest.raises(NotImplementedError):
+        ode.jacobian()
+    with pytest.raises(ValueError):
+        p.stepper(dt, method="adaptive")
+    ex = p.stepper(2 * dt, krylov_dim=24)(y0)
+    assert np.linalg.norm(ex - p.step(y0, 2 * dt, krylov_dim=24)) <= 1e-5 * np.linalg.norm(ex)
