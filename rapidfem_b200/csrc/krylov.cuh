@@ -242,7 +242,7 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* sums, int 
 
 // First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
 template <class B>
-__global__ void __launch_bounds__(kKrylovThreads, 2)
+__global__ void __launch_bounds__(kKrylovThreads, 1)
 k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
@@ -263,35 +263,27 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
-    // pass-1 update with each column streamed once, then the pass-2 dots with
-    // the columns read again (from L1: this thread just read the same 16-byte
-    // vectors), so that no column is held in registers across the two
     T wk = reinterpret_cast<const T*>(w)[k];
-    double x[KV::W];
-#pragma unroll
-    for (int q = 0; q < KV::W; ++q) x[q] = KV::at(wk, q);
+    T vk[kKryCols];
 #pragma unroll
     for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) {
-        const T vi = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
-#pragma unroll
-        for (int q = 0; q < KV::W; ++q) x[q] = fma(-u[i], KV::at(vi, q), x[q]);
-      }
+      if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
+    // per lane: the update, then the second pass's products with the stored
+    // (rounded) value, so that only one lane's converted values are live
 #pragma unroll
     for (int q = 0; q < KV::W; ++q) {
-      KV::set(wk, q, x[q]);
-      const double xs = KV::at(wk, q);  // the stored (rounded) value
-      x[q] = xs;
+      double x = KV::at(wk, q);
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
+      KV::set(wk, q, x);
+      const double xs = KV::at(wk, q);
       wn[0] = fma(xs, xs, wn[0]);
+#pragma unroll
+      for (int i = 0; i < kKryCols; ++i)
+        if (i < cols) acc[i] = fma(KV::at(vk[i], q), xs, acc[i]);
     }
     reinterpret_cast<T*>(w)[k] = wk;
-#pragma unroll
-    for (int i = 0; i < kKryCols; ++i)
-      if (i < cols) {
-        const T vi = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
-#pragma unroll
-        for (int q = 0; q < KV::W; ++q) acc[i] = fma(KV::at(vi, q), x[q], acc[i]);
-      }
   }
   double* row = partials_out + (int64_t)blockIdx.x * kKryRow;
   block_sums<kKryCols>(acc, cols, red, row);
