@@ -9,6 +9,7 @@
  *   crates/rapidfem-td/src/geom_factors.rs    (all_geometric_factors)
  *   crates/rapidfem-core/src/topology.rs      (FaceTopology::build)
  *   crates/rapidfem-td/src/rhs.rs:805-1000    (MaxwellOperator::new)
+ *   crates/rapidfem-td/src/rhs.rs:546-770     (periodic face pairs)
  *   crates/rapidfem-td/src/rhs.rs:1157-1242   (port_source, port projections)
  *   crates/rapidfem-td/src/waveguide.rs:90-152 (RectPort TE_mn profiles)
  * All arithmetic here is f64, as in the reference.
@@ -50,6 +51,18 @@ int dgtd_mesh_box_graded_z(int32_t nx, int32_t ny, int32_t nz, double lx, double
 int dgtd_host_op_build(const double *nodes, int64_t n_nodes, const int32_t *tets, int64_t n_elem,
                        int32_t order, double flux_alpha, const int32_t *face_port,
                        const double *materials, dgtd_host_op **out);
+/* A periodic face pair (PeriodicSpec, rhs.rs:253-270; link_periodic_faces,
+ * rhs.rs:616-770): the domain-boundary faces faces_a[n_a] and faces_b[n_b]
+ * (face ids e*4 + local face) are wired to one another as interior faces
+ * across the translation between the two sides' area-weighted centroids.
+ * Each side-A face takes the side-B face whose centroid is nearest its own
+ * translated centroid (within max(1e-9 |T|, 1e-12)), the pairing must be a
+ * bijection, and the face-node permutations are nearest-node matches in the
+ * translated frame (both directions).  Port faces and faces that already have
+ * a neighbour are rejected; on any error the operator is left unchanged.
+ * Call once per pair, after dgtd_host_op_build and before dgtd_host_op_desc. */
+int dgtd_host_op_link_periodic(dgtd_host_op *op, const int64_t *faces_a, int64_t n_a,
+                               const int64_t *faces_b, int64_t n_b);
 /* Releases the host operator (MaxwellOperator is dropped in the reference). */
 int dgtd_host_op_destroy(dgtd_host_op *op);
 /* Fill a dgtd_op_desc whose pointers stay valid while `op` lives: the arrays

@@ -594,6 +594,115 @@ int orc_op_get(const orc_op *op, const char *which, double *out) {
 void orc_op_set_port(orc_op *op, int ef, int port) { op->port[ef] = port; }
 
 /* ------------------------------------------------------------------------
+ * Periodic face pairs.  rhs.rs:546-568 (`match_face_nodes`), rhs.rs:588-614
+ * (`periodic_face_centroid`), rhs.rs:616-770 (`link_periodic_faces`), with
+ * PERIODIC_MATCH_REL_TOL = 1e-9 and PERIODIC_MATCH_ABS_FLOOR = 1e-12
+ * (constants.rs:216-222).  Faces are ids e*4+lf; triangle coordinates come
+ * from the mesh nodes, as in the reference.  Returns 0, or: 1 counts differ,
+ * 2 a port face, 3 a face with a neighbour, 4 zero area, 5 a side-A face
+ * without partner, 6 not a bijection, 7 an unmatched face node.  Matching is
+ * the reference's all-pairs nearest search; the operator changes only when
+ * every check passed.
+ * --------------------------------------------------------------------- */
+
+static void tri_xyz(const double *nodes, const int *tets, int ef, double v[3][3]) {
+    for (int q = 0; q < 3; q++)
+        for (int k = 0; k < 3; k++)
+            v[q][k] = nodes[3 * (size_t)tets[4 * (ef / 4) + TET_FACE_LOCAL[ef % 4][q]] + k];
+}
+
+static int match_face_nodes(const orc_op *op, int here, int there, const double *shift, double tol2,
+                            int *perm) {
+    int nfp = op->re.nfp;
+    double ph[21 * 3], pt[21 * 3];
+    for (int m = 0; m < nfp; m++) {
+        map_point(op, here / 4, op->re.nodes + 3 * op->re.face_nodes[(here % 4) * nfp + m], ph + 3 * m);
+        map_point(op, there / 4, op->re.nodes + 3 * op->re.face_nodes[(there % 4) * nfp + m], pt + 3 * m);
+    }
+    for (int m = 0; m < nfp; m++) {
+        double t[3] = {ph[3 * m] + shift[0], ph[3 * m + 1] + shift[1], ph[3 * m + 2] + shift[2]};
+        double best = 1.79769313486231570e+308;
+        int bm = 0;
+        for (int m2 = 0; m2 < nfp; m2++) {
+            double d = powi_d(t[0] - pt[3 * m2], 2) + powi_d(t[1] - pt[3 * m2 + 1], 2) +
+                       powi_d(t[2] - pt[3 * m2 + 2], 2);
+            if (d < best) { best = d; bm = m2; }
+        }
+        if (!(best < tol2)) return 1;
+        perm[m] = bm;
+    }
+    return 0;
+}
+
+int orc_link_periodic(orc_op *op, const double *nodes, const int *tets, const long *faces_a, int n_a,
+                      const long *faces_b, int n_b) {
+    if (n_a != n_b) return 1;
+    int n = n_a, nfp = op->re.nfp;
+    for (int i = 0; i < 2 * n; i++) {
+        long ef = i < n ? faces_a[i] : faces_b[i - n];
+        if (op->port[ef] != ORC_NONE) return 2;
+        if (op->nbr[ef] != ORC_NONE) return 3;
+    }
+    double *cen = malloc(sizeof(double) * 6 * (size_t)n);  /* A then B triangle centroids */
+    double side[2][3] = {{0, 0, 0}, {0, 0, 0}}, total[2] = {0, 0};
+    for (int i = 0; i < 2 * n; i++) {
+        int s = i >= n;
+        double v[3][3], e1[3], e2[3], nn[3];
+        tri_xyz(nodes, tets, (int)(s ? faces_b[i - n] : faces_a[i]), v);
+        for (int k = 0; k < 3; k++) { e1[k] = v[1][k] - v[0][k]; e2[k] = v[2][k] - v[0][k]; }
+        cross3(e1, e2, nn);
+        double area = 0.5 * sqrt(dot3(nn, nn));
+        for (int k = 0; k < 3; k++) {
+            side[s][k] += area * (v[0][k] + v[1][k] + v[2][k]) / 3.0;
+            cen[3 * (size_t)i + k] = (v[0][k] + v[1][k] + v[2][k]) / 3.0;
+        }
+        total[s] += area;
+    }
+    int rc = 0;
+    int *a2b = malloc(sizeof(int) * (size_t)n), *b2a = malloc(sizeof(int) * (size_t)n);
+    int *perm = malloc(sizeof(int) * 2 * (size_t)n * nfp);
+    if (!(total[0] > 0.0) || !(total[1] > 0.0)) { rc = 4; goto done; }
+    double trans[3], back[3];
+    for (int k = 0; k < 3; k++) {
+        trans[k] = side[1][k] / total[1] - side[0][k] / total[0];
+        back[k] = -trans[k];
+    }
+    double mag = sqrt(dot3(trans, trans));
+    double tol = 1e-9 * mag > 1e-12 ? 1e-9 * mag : 1e-12;
+    double tol2 = tol * tol;
+    for (int i = 0; i < n; i++) b2a[i] = -1;
+    for (int i = 0; i < n; i++) {
+        double t[3] = {cen[3 * i] + trans[0], cen[3 * i + 1] + trans[1], cen[3 * i + 2] + trans[2]};
+        double best = 1.79769313486231570e+308;
+        int bi = -1;
+        for (int j = 0; j < n; j++) {
+            const double *c = cen + 3 * ((size_t)n + j);
+            double d = powi_d(t[0] - c[0], 2) + powi_d(t[1] - c[1], 2) + powi_d(t[2] - c[2], 2);
+            if (d < best) { best = d; bi = j; }
+        }
+        if (!(best < tol2)) { rc = 5; goto done; }
+        if (b2a[bi] >= 0) { rc = 6; goto done; }
+        a2b[i] = bi;
+        b2a[bi] = i;
+    }
+    for (int i = 0; i < n; i++) {
+        int fa = (int)faces_a[i], fb = (int)faces_b[a2b[i]];
+        if (match_face_nodes(op, fa, fb, trans, tol2, perm + (size_t)(2 * i) * nfp) ||
+            match_face_nodes(op, fb, fa, back, tol2, perm + (size_t)(2 * i + 1) * nfp)) { rc = 7; goto done; }
+    }
+    for (int i = 0; i < n; i++) {
+        int fa = (int)faces_a[i], fb = (int)faces_b[a2b[i]];
+        op->nbr[fa] = fb / 4; op->nbr_lf[fa] = fb % 4;
+        op->nbr[fb] = fa / 4; op->nbr_lf[fb] = fa % 4;
+        memcpy(op->perm + (size_t)fa * nfp, perm + (size_t)(2 * i) * nfp, sizeof(int) * nfp);
+        memcpy(op->perm + (size_t)fb * nfp, perm + (size_t)(2 * i + 1) * nfp, sizeof(int) * nfp);
+    }
+done:
+    free(cen); free(a2b); free(b2a); free(perm);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------
  * The RHS.  rhs.rs:39-85 (`element_curl`), rhs.rs:1341-1473 (`apply_element`),
  * rhs.rs:1262-1325 (`apply_into`, contiguous element runs per task).
  * --------------------------------------------------------------------- */

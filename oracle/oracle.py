@@ -79,6 +79,9 @@ def lib():
     L.orc_set_threads.argtypes = [C.c_int]
     L.orc_get_threads.restype = C.c_int
     L.orc_lserk_coeffs.argtypes = [_dp, _dp]
+    _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+    L.orc_link_periodic.restype = C.c_int
+    L.orc_link_periodic.argtypes = [C.c_void_p, _dp, _ip, _lp, C.c_int, _lp, C.c_int]
     L.orc_kcl_coeffs.argtypes = [_dp, _dp, _dp]
     _lib = L
     return L
@@ -183,6 +186,19 @@ class Operator:
         self.n_dof = int(L.orc_op_n_dof(self.h))
         self.order = order
         self.flux_alpha = flux_alpha
+        self._nodes, self._tets = nodes, tets
+
+    _PERIODIC_ERRORS = {1: "different face counts on the two sides", 2: "a port face", 3: "a face with a neighbour",
+                        4: "zero total area", 5: "a side-A face without partner", 6: "not a bijection",
+                        7: "an unmatched face node"}
+
+    def link_periodic(self, faces_a, faces_b):
+        """link_periodic_faces (rhs.rs:616-770) on face ids e*4+lf."""
+        a = np.ascontiguousarray(faces_a, dtype=np.int64)
+        b = np.ascontiguousarray(faces_b, dtype=np.int64)
+        rc = self._L.orc_link_periodic(self.h, self._nodes.ravel(), self._tets.ravel(), a, a.size, b, b.size)
+        if rc:
+            raise ValueError(f"periodic pair: {self._PERIODIC_ERRORS.get(rc, rc)}")
 
     def __del__(self):
         try:

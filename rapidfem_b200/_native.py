@@ -153,6 +153,7 @@ _sig("dgtd_mesh_box_jittered", C.c_int, _i32, _i32, _i32, _f64, _f64, _f64, _f64
 _sig("dgtd_mesh_box_graded_z", C.c_int, _i32, _i32, _i32, _f64, _f64, _f64, _f64, _pd, _pi)
 _sig("dgtd_host_op_build", C.c_int, _pd, _i64, _pi, _i64, _i32, _f64, _vp, _vp, C.POINTER(_vp))
 _sig("dgtd_host_op_destroy", C.c_int, _vp)
+_sig("dgtd_host_op_link_periodic", C.c_int, _vp, _pl, _i64, _pl, _i64)
 _sig("dgtd_host_op_desc", C.c_int, _vp, C.POINTER(OpDesc))
 _sig("dgtd_host_op_info", C.c_int, _vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i64))
 _sig("dgtd_host_op_get", C.c_int, _vp, C.c_char_p, _pd)

@@ -6,12 +6,14 @@
 // Reference algorithms followed (paths relative to the rapidfem root):
 //   mesh_gen.rs:16-139, dg_basis.rs:61-385, geom_factors.rs:33-88,
 //   rapidfem-core topology.rs:50-91 + mesh.rs:45-50, rhs.rs:805-1000,
-//   rhs.rs:1030-1066, rhs.rs:1157-1199, waveguide.rs:39-145.
+//   rhs.rs:546-770 (periodic pairs), rhs.rs:1030-1066, rhs.rs:1157-1199,
+//   waveguide.rs:39-145.
 #include <algorithm>
 #include <parallel/algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -531,6 +533,168 @@ extern "C" int dgtd_host_op_build(const double* nodes, int64_t n_nodes, const in
 
 extern "C" int dgtd_host_op_destroy(dgtd_host_op* op) {
   delete op;
+  return DGTD_OK;
+}
+
+// ------------------------------------------------------- periodic face pairs
+
+namespace {
+
+const double kPeriodicRelTol = 1e-9;     // PERIODIC_MATCH_REL_TOL (constants.rs:216)
+const double kPeriodicAbsFloor = 1e-12;  // PERIODIC_MATCH_ABS_FLOOR (constants.rs:222)
+const V3 kRefVertex[4] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+
+struct FaceGeom {
+  V3 centroid;
+  double area;
+};
+
+FaceGeom face_geom(const dgtd::host::Operator& o, int64_t ef) {
+  const int64_t e = ef / 4;
+  const int lf = int(ef % 4);
+  V3 v[3];
+  for (int q = 0; q < 3; ++q) v[q] = o.map(e, kRefVertex[dgtd::host::kFaceLocal[lf][q]]);
+  const V3 n = cross({v[1][0] - v[0][0], v[1][1] - v[0][1], v[1][2] - v[0][2]},
+                     {v[2][0] - v[0][0], v[2][1] - v[0][1], v[2][2] - v[0][2]});
+  FaceGeom g;
+  g.area = 0.5 * std::sqrt(dot(n, n));
+  for (int k = 0; k < 3; ++k) g.centroid[k] = (v[0][k] + v[1][k] + v[2][k]) / 3.0;
+  return g;
+}
+
+std::string sci(double v) {
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "%.3e", v);
+  return buf;
+}
+
+double dist2(const V3& a, const V3& b) {
+  return dgtd::host::powi(a[0] - b[0], 2) + dgtd::host::powi(a[1] - b[1], 2) +
+         dgtd::host::powi(a[2] - b[2], 2);
+}
+
+// match_face_nodes (rhs.rs:546-568): perm[m] = the node of face `there`
+// nearest to node m of face `here` shifted by `shift`; false if one is
+// farther than sqrt(tol2).
+bool match_nodes(const dgtd::host::Operator& o, int64_t here, int64_t there, const V3& shift, double tol2,
+                 int32_t* perm, double* worst) {
+  const int nfp = o.re.nfp;
+  std::array<V3, 21> ph, pt;  // Nfp <= 21 (order 5)
+  for (int m = 0; m < nfp; ++m) {
+    ph[m] = o.map(here / 4, o.re.nodes[o.re.face_nodes[size_t(here % 4) * nfp + m]]);
+    pt[m] = o.map(there / 4, o.re.nodes[o.re.face_nodes[size_t(there % 4) * nfp + m]]);
+  }
+  bool ok = true;
+  for (int m = 0; m < nfp; ++m) {
+    const V3 target = {ph[m][0] + shift[0], ph[m][1] + shift[1], ph[m][2] + shift[2]};
+    double best = std::numeric_limits<double>::max();
+    int bm = 0;
+    for (int m2 = 0; m2 < nfp; ++m2) {
+      const double d = dist2(target, pt[m2]);
+      if (d < best) { best = d; bm = m2; }
+    }
+    if (!(best < tol2)) {
+      ok = false;
+      *worst = std::max(*worst, std::sqrt(best));
+    }
+    perm[m] = bm;
+  }
+  return ok;
+}
+
+}  // namespace
+
+// link_periodic_faces (rhs.rs:616-770) on face ids e*4+lf.  Everything is
+// checked before the operator changes, so a failed call leaves it as it was.
+extern "C" int dgtd_host_op_link_periodic(dgtd_host_op* h, const int64_t* faces_a, int64_t n_a,
+                                          const int64_t* faces_b, int64_t n_b) {
+  if (!h || !faces_a || !faces_b || n_a < 1 || n_b < 1)
+    return set_error(DGTD_ERR_BAD_ARG, "link_periodic: bad arguments");
+  auto& o = h->op;
+  if (n_a != n_b)
+    return set_error(DGTD_ERR_BAD_ARG, "link_periodic: periodic pair has different triangle counts on each side: A has " +
+                                           std::to_string(n_a) + ", B has " + std::to_string(n_b));
+  const int64_t n = n_a;
+  for (int side = 0; side < 2; ++side)
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t ef = (side ? faces_b : faces_a)[i];
+      if (ef < 0 || ef >= 4 * o.K) return set_error(DGTD_ERR_BAD_ARG, "link_periodic: face id out of range");
+      if (o.port[ef] >= 0)
+        return set_error(DGTD_ERR_BAD_ARG, "link_periodic: face " + std::to_string(ef) + " is marked both port and periodic");
+      if (o.nbr[ef] >= 0)
+        return set_error(DGTD_ERR_BAD_ARG, "link_periodic: face " + std::to_string(ef) + " is not on the domain boundary");
+    }
+  // Period translation from the area-weighted side centroids (rhs.rs:588-614).
+  std::vector<FaceGeom> ga(n), gb(n);
+  V3 ca = {0, 0, 0}, cb = {0, 0, 0};
+  double wa = 0.0, wb = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    ga[i] = face_geom(o, faces_a[i]);
+    gb[i] = face_geom(o, faces_b[i]);
+    for (int k = 0; k < 3; ++k) {
+      ca[k] += ga[i].area * ga[i].centroid[k];
+      cb[k] += gb[i].area * gb[i].centroid[k];
+    }
+    wa += ga[i].area;
+    wb += gb[i].area;
+  }
+  if (!(wa > 0.0) || !(wb > 0.0)) return set_error(DGTD_ERR_BAD_ARG, "link_periodic: periodic face has zero total area");
+  V3 trans;
+  for (int k = 0; k < 3; ++k) trans[k] = cb[k] / wb - ca[k] / wa;
+  const double mag = std::sqrt(dot(trans, trans));
+  const double tol = std::max(kPeriodicRelTol * mag, kPeriodicAbsFloor);
+  const double tol2 = tol * tol;
+  // Triangle partners: nearest translated centroid.  B's centroids are sorted
+  // by x, so each A triangle scans only the B triangles within tol in x; the
+  // nearest of those (lowest B index on a tie) is the nearest of all whenever
+  // one lies within tol.
+  std::vector<int64_t> bx(n);
+  for (int64_t i = 0; i < n; ++i) bx[i] = i;
+  std::sort(bx.begin(), bx.end(), [&](int64_t p, int64_t q) {
+    return gb[p].centroid[0] < gb[q].centroid[0] || (gb[p].centroid[0] == gb[q].centroid[0] && p < q);
+  });
+  std::vector<double> xs(n);
+  for (int64_t i = 0; i < n; ++i) xs[i] = gb[bx[i]].centroid[0];
+  std::vector<int64_t> a_to_b(n, -1), b_to_a(n, -1);
+  for (int64_t i = 0; i < n; ++i) {
+    const V3 t = {ga[i].centroid[0] + trans[0], ga[i].centroid[1] + trans[1], ga[i].centroid[2] + trans[2]};
+    auto lo = std::lower_bound(xs.begin(), xs.end(), t[0] - tol);
+    double best = std::numeric_limits<double>::max();
+    int64_t bi = -1;
+    for (auto it = lo; it != xs.end() && *it <= t[0] + tol; ++it) {
+      const int64_t j = bx[it - xs.begin()];
+      const double d = dist2(t, gb[j].centroid);
+      if (d < best || (d == best && j < bi)) { best = d; bi = j; }
+    }
+    if (bi < 0 || !(best < tol2))
+      return set_error(DGTD_ERR_BAD_ARG, "link_periodic: periodic face " + std::to_string(faces_a[i]) +
+                                             " on side A has no partner on side B within tolerance " + sci(tol));
+    if (b_to_a[bi] >= 0)
+      return set_error(DGTD_ERR_BAD_ARG, "link_periodic: periodic side-B face " + std::to_string(faces_b[bi]) +
+                                             " matched by two side-A faces; a periodic pair must be a bijection");
+    a_to_b[i] = bi;
+    b_to_a[bi] = i;
+  }
+  const int nfp = o.re.nfp;
+  const V3 back = {-trans[0], -trans[1], -trans[2]};
+  std::vector<int32_t> perm_a(size_t(n) * nfp), perm_b(size_t(n) * nfp);
+  double worst = 0.0;
+  bool ok = true;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t fa = faces_a[i], fb = faces_b[a_to_b[i]];
+    ok &= match_nodes(o, fa, fb, trans, tol2, &perm_a[size_t(i) * nfp], &worst);
+    ok &= match_nodes(o, fb, fa, back, tol2, &perm_b[size_t(i) * nfp], &worst);
+  }
+  if (!ok)
+    return set_error(DGTD_ERR_BAD_ARG, "link_periodic: periodic face node found no partner within tolerance " +
+                                           sci(tol) + " (best " + sci(worst) + ")");
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t fa = faces_a[i], fb = faces_b[a_to_b[i]];
+    o.nbr[fa] = int32_t(fb / 4); o.nbr_lf[fa] = int32_t(fb % 4);
+    o.nbr[fb] = int32_t(fa / 4); o.nbr_lf[fb] = int32_t(fa % 4);
+    std::memcpy(&o.perm[size_t(fa) * nfp], &perm_a[size_t(i) * nfp], sizeof(int32_t) * nfp);
+    std::memcpy(&o.perm[size_t(fb) * nfp], &perm_b[size_t(i) * nfp], sizeof(int32_t) * nfp);
+  }
   return DGTD_OK;
 }
 

@@ -15,13 +15,15 @@ rapidfem's meshes carry them) and attaches to them:
   characteristic (Silver-Mueller) boundary, and a rectangular port carries
   its TE_mn profile for injection and modal probes;
 * PEC plates (build.rs:244-247): interior faces severed from their neighbour,
-  each side a PEC wall; boundary faces are PEC anyway.
+  each side a PEC wall; boundary faces are PEC anyway;
+* periodic pairs (build.rs:235-240): two boundary face groups wired to one
+  another across the period translation (MaxwellOperator.link_periodic).
 
 Kinds the DG path of this library does not carry are rejected with the
 reference's wording where the reference rejects them (lumped ports) and with
 a clear error otherwise (Debye dispersion: the reference's GPU path excludes
 it too, gpu/operator.rs:211-215; coaxial, Floquet and numerical wave-port
-profiles; periodic pairs).  Frequency-domain-only face conditions are
+profiles).  Frequency-domain-only face conditions are
 ignored with a warning, as the reference does (build.rs:216-229).
 """
 from __future__ import annotations
@@ -233,8 +235,6 @@ def face_codes_of(tm: TaggedMesh, model: Model):
     if model.far_field_tag is not None:
         warnings.warn(f"TD: far-field surface tag {model.far_field_tag} ignored, the near-to-far-field "
                       "transform is frequency-domain only")
-    if model.periodic:
-        raise NotImplementedError("periodic face pairs are not carried by the device path")
     for tag in model.pec_tags:
         code[tm.faces_of(tag)] = PEC_PLATE
     return code, tags, modes
@@ -249,8 +249,23 @@ def operator_from_model(tm: TaggedMesh, model: Model, order: int, flux_alpha: fl
     del c
     mat = materials_of(tm, model)
     code, tags, modes = face_codes_of(tm, model)
+    pairs = periodic_faces_of(tm, model)
     op = MaxwellOperator(tm.mesh, order, flux_alpha, face_port=code, materials=mat)
+    for a, b in pairs:
+        op.link_periodic(a, b)
     return ModelOperator(op, tags, modes, mat, code)
+
+
+def periodic_faces_of(tm: TaggedMesh, model: Model) -> list:
+    """build.rs:235-240: per periodic pair (tag_a, tag_b), the face ids
+    (e*4 + local face) of each side's triangles."""
+    out = []
+    for a, b in model.periodic:
+        ta, tb = tm.face_tags.get(a), tm.face_tags.get(b)
+        if ta is None or tb is None or len(ta) == 0 or len(tb) == 0:
+            raise ValueError(f"periodic pair ({a}, {b}): a face tag has no triangles")
+        out.append((np.flatnonzero(tm.faces_of(a).ravel()), np.flatnonzero(tm.faces_of(b).ravel())))
+    return out
 
 
 def box_tagged(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0) -> TaggedMesh:

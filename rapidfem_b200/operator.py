@@ -134,6 +134,19 @@ class MaxwellOperator:
         check(lib.dgtd_host_op_get(self._h, name.encode(), out))
         return out
 
+    def link_periodic(self, faces_a, faces_b) -> None:
+        """Wire a periodic face pair (link_periodic_faces, rhs.rs:616-770):
+        the domain-boundary faces `faces_a` and `faces_b` (ids e*4 + local
+        face) become interior faces across the translation between the two
+        sides' centroids.  Raises (and leaves the operator unchanged) when a
+        face is a port or not on the boundary, the counts differ, or a face
+        or face node finds no partner."""
+        a = np.ascontiguousarray(faces_a, dtype=np.int64).ravel()
+        b = np.ascontiguousarray(faces_b, dtype=np.int64).ravel()
+        if a.size == 0 or b.size == 0:
+            raise ValueError("periodic pair: a side has no faces")
+        check(lib.dgtd_host_op_link_periodic(self._h, a, a.size, b, b.size))
+
     def desc(self) -> nat.OpDesc:
         d = nat.OpDesc()
         check(lib.dgtd_host_op_desc(self._h, C.byref(d)))

@@ -395,7 +395,7 @@ class ProblemTD:
     def from_model(cls, tagged_mesh, model, *, order=2, flux="upwind", c=C_LIGHT):
         """ProblemTD(g) of problem/td.py:256-283 for a model on a tagged mesh
         (this package has no geometry / meshing layer): materials, PML
-        absorbers, rectangular / ABC ports and PEC plates of `model`."""
+        absorbers, rectangular / ABC ports, PEC plates and periodic pairs of `model`."""
         obj = cls.__new__(cls)
         obj.c = float(c)
         obj._op = TdSession.from_model(tagged_mesh, model, order, flux, obj.c)

@@ -53,8 +53,8 @@ def test_port_order_codes_and_errors():
         M.face_codes_of(tm, M.Model(faces=[M.OtherFace(5, "lumped")]))
     with pytest.raises(NotImplementedError):
         M.face_codes_of(tm, M.Model(faces=[M.OtherFace(5, "coax")]))
-    with pytest.raises(NotImplementedError):
-        M.face_codes_of(tm, M.Model(periodic=[(1, 2)]))
+    with pytest.raises(ValueError, match="periodic pair \\(1, 99\\): a face tag has no triangles"):
+        M.periodic_faces_of(tm, M.Model(periodic=[(1, 99)]))
     with pytest.raises(NotImplementedError):
         M.materials_of(tm, M.Model(materials=[M.Material(1, debye=(2.0, 4.0, 1e-3))]))
     with warnings.catch_warnings(record=True) as w:
