@@ -814,14 +814,9 @@ def run_time_to_t(args):
     return 0
 
 
-def run_c5(args):
-    """The waveguide study: a 22.86 x 10.16 x 60 mm guide (39 x 17 x 101 hex x 6
-    tets), N = 3, a centred dielectric post (r = 1.5 mm) with eps_r spread over
-    2-10 in `--c5-variants` variants, a TE10 Gaussian-modulated pulse (10 GHz,
-    4 GHz FWHM bandwidth) injected by incident-field flux at z = 0, an absorbing
-    port at z = 60 mm, PEC walls; LSERK4 on the tensor-core stage kernel with
-    the modal amplitudes P_e of both ports recorded per step on the device, and
-    the first and last variants' series checked against the FP32 stage kernel."""
+def _c5_setup(args, local):
+    """The waveguide-post study's operator, port source and probes, step and
+    variants (shared by the LSERK4 and the ETD runs)."""
     import ctypes as C
 
     import torch
@@ -831,10 +826,6 @@ def run_c5(args):
     from rapidfem_b200 import td as T
     from rapidfem_b200 import workloads as W
 
-    rank, world, local = _rank()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local)
     c_light = 299792458.0
     a, b_w, L = 22.86e-3, 10.16e-3, 60e-3
     cells = tuple(args.c5_cells)
@@ -858,9 +849,147 @@ def run_c5(args):
     t0 = 3.0 * tau
     t_end = t0 + 3.0 * tau + L / 0.7
     steps = int(np.ceil(t_end / dt)) if args.c5_steps <= 0 else args.c5_steps
-    g = T.GaussianPulse(t0, tau, 10e9 / c_light)(np.arange(steps) * dt).astype(np.float32)
     V = args.c5_variants
-    eps_list = [2.0 + 8.0 * k / max(V - 1, 1) for k in range(V)]
+    return {"op": op, "post": post, "src": src, "funcs": funcs, "ctx": ctx, "stream": stream, "rho": rho.value,
+            "dt": dt, "steps": steps, "cells": cells, "V": V, "t0": t0, "tau": tau,
+            "wave": T.GaussianPulse(t0, tau, 10e9 / c_light),
+            "eps_list": [2.0 + 8.0 * k / max(V - 1, 1) for k in range(V)]}
+
+
+def run_c5_etd(args):
+    """The waveguide study under the exponential integrator: the first and last
+    post variants (eps_r 2 and 10) run by ETD with the learned step controller
+    (tensor-core Krylov matvec, m <= 60, the port source as a polynomial over
+    each step), the transmitted and reflected modal amplitudes recorded on the
+    device at every accepted step, against plain FP32 LSERK4 (CUDA-core stage
+    kernel, the source sampled at the stage times, amplitudes every step).  The
+    controller is trained on the plain controller's traces of the middle
+    variant (eps_r 6), which is not one of the two checked."""
+    import torch
+
+    from rapidfem_b200 import _native as nat
+    from rapidfem_b200 import etd as E
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import sources as S
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    cfg = _c5_setup(args, local)
+    op, post, src, funcs, ctx, stream = cfg["op"], cfg["post"], cfg["src"], cfg["funcs"], cfg["ctx"], cfg["stream"]
+    dt, steps, wave = cfg["dt"], cfg["steps"], cfg["wave"]
+    t_end = steps * dt
+    eps_checked = [2.0, 10.0]
+    plain = E.PlainEtd(tol=args.ttt_tol, m_max=60)
+    h0 = 8 * dt
+
+    def operator(eps):
+        gop = G.GpuOperator(ctx, op, inv_eps=np.repeat(np.where(post, 1.0 / eps, 1.0), 3))
+        gop.set_source_vector(src)
+        return gop
+
+    # training traces: the plain controller on the middle variant
+    logs = []
+    gop = operator(6.0)
+    gop.set_engine(nat.ENGINE_TF32X3)
+    _, st_tr = E.run_etd(gop, np.zeros(op.n_dof), src, wave, t_end, h0, plain, log=logs)
+    trace = {"eps_r": 6.0, "seconds": st_tr.seconds, "steps": st_tr.accepted, "rejected": st_tr.rejected,
+             "matvecs": st_tr.matvecs, "traces": len(logs)}
+    del gop
+    mlp = E.Mlp(ctx, seed=1)
+    w = time.perf_counter()
+    losses = E.train_controller(mlp, logs, epochs=3000, lr=3e-3)
+    train_s = time.perf_counter() - w
+    learned = E.LearnedEtd(mlp, plain)
+    g_st = S.stage_samples(wave, 0.0, dt, steps).astype(np.float32)
+    variants = []
+    for eps in eps_checked:
+        gop = operator(eps)
+        # plain FP32 LSERK4: amplitudes after every step, recorded on the device
+        gop.set_engine(nat.ENGINE_FP32)
+        gop.upload(np.zeros(op.n_dof, dtype=np.float32))
+        gop.set_functionals(funcs, steps + 1)
+        gop.record_functionals(0)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(steps):
+            gop.run_lserk_stages(dt, 1, ("vector", None), g_st[5 * k:5 * k + 5])
+            gop.record_functionals(k + 1)
+        e1.record(stream)
+        stream.synchronize()
+        lserk_s = e0.elapsed_time(e1) * 1e-3
+        ref = gop.functional_series(steps + 1)
+        t_ref = np.arange(steps + 1) * dt
+        # learned ETD on the tensor-core matvec
+        gop.set_engine(nat.ENGINE_TF32X3)
+        _, st = E.run_etd(gop, np.zeros(op.n_dof), src, wave, t_end, h0, plain, learned=learned,
+                          functionals=funcs)
+
+        def rel_series(run):
+            at = np.stack([np.interp(run.times, t_ref, ref[:, q]) for q in range(ref.shape[1])], axis=1)
+            return [float(np.linalg.norm(run.series[:, q] - at[:, q]) / np.linalg.norm(at[:, q]))
+                    for q in range(ref.shape[1])]
+
+        rel = rel_series(st)
+        plain_run = None
+        if eps == eps_checked[0]:
+            # the plain controller alone on the same variant
+            _, sp = E.run_etd(gop, np.zeros(op.n_dof), src, wave, t_end, h0, plain, functionals=funcs)
+            rp = rel_series(sp)
+            plain_run = {"seconds": sp.seconds, "steps": sp.accepted, "rejected": sp.rejected,
+                         "matvecs": sp.matvecs, "rel_l2_transmitted_Pe": rp[0], "rel_l2_reflected_Pe": rp[1]}
+        variants.append({"eps_r": eps, "lserk4_fp32_seconds": lserk_s, "lserk4_steps": steps,
+                         "etd_plain": plain_run,
+                         "etd_learned_seconds": st.seconds, "etd_steps": st.accepted, "etd_rejected": st.rejected,
+                         "etd_matvecs": st.matvecs, "proposals_kept": st.proposals_kept,
+                         "proposals_failed": st.proposals_failed,
+                         "rel_l2_transmitted_Pe": rel[0], "rel_l2_reflected_Pe": rel[1],
+                         "peak_transmitted_Pe": {"lserk4": float(np.max(np.abs(ref[:, 0]))),
+                                                 "etd": float(np.max(np.abs(st.series[:, 0])))},
+                         "speedup_vs_lserk4_fp32": lserk_s / st.seconds})
+        del gop
+    line = {
+        "metric": "seconds per waveguide variant (learned ETD) with port probes vs plain FP32 LSERK4",
+        "value": float(np.mean([v["etd_learned_seconds"] for v in variants])), "unit": "s", "n_gpus": 1,
+        "steps": int(np.mean([v["etd_steps"] for v in variants])), "warmup": 0, "higher_is_better": False,
+        "scaling": "none", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"WR-90 post variants eps_r {eps_checked} ({op.n_elem} tets, N=3, "
+                               f"{op.n_dof} DOFs), TE10 pulse injected at z=0, T={t_end:.5g} (operator time)",
+                   "etd": {"tol": plain.tol, "m_max": plain.m_max, "source_terms": 8, "engine": "tf32x3"},
+                   "lserk4": {"engine": "fp32", "dt": dt, "source": "sampled at the stage times"},
+                   "controller_training": dict(trace, train_seconds=train_s, epochs=3000,
+                                               loss_first=float(losses[0]), loss_last=float(losses[-1])),
+                   "variants": variants},
+        "e2e": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_c5(args):
+    """The waveguide study: a 22.86 x 10.16 x 60 mm guide (39 x 17 x 101 hex x 6
+    tets), N = 3, a centred dielectric post (r = 1.5 mm) with eps_r spread over
+    2-10 in `--c5-variants` variants, a TE10 Gaussian-modulated pulse (10 GHz,
+    4 GHz FWHM bandwidth) injected by incident-field flux at z = 0, an absorbing
+    port at z = 60 mm, PEC walls; LSERK4 on the tensor-core stage kernel with
+    the modal amplitudes P_e of both ports recorded per step on the device, and
+    the first and last variants' series checked against the FP32 stage kernel."""
+    import torch
+
+    from rapidfem_b200 import _native as nat
+    from rapidfem_b200 import gpu as G
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    cfg = _c5_setup(args, local)
+    op, post, src, funcs, ctx, stream = cfg["op"], cfg["post"], cfg["src"], cfg["funcs"], cfg["ctx"], cfg["stream"]
+    dt, steps, cells, V, eps_list = cfg["dt"], cfg["steps"], cfg["cells"], cfg["V"], cfg["eps_list"]
+    g = cfg["wave"](np.arange(steps) * dt).astype(np.float32)
 
     def run(eps, engine):
         ie = np.repeat(np.where(post, 1.0 / eps, 1.0), 3)
@@ -948,9 +1077,11 @@ def main():
                     help="with N > 1 ranks: N independent replicas instead of the partitioned run")
     ap.add_argument("--sharded", action="store_true",
                     help="the partitioned run even on one rank (a one-part partition)")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "c4", "c5", "time-to-t", "c2-accuracy"],
+    ap.add_argument("--workload", default="sphere",
+                    choices=["sphere", "c4", "c5", "c5-etd", "time-to-t", "c2-accuracy"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
                          "c5: the waveguide post variants with port probes; "
+                         "c5-etd: two of those variants under the learned ETD controller against FP32 LSERK4; "
                          "time-to-t: LSERK4 vs adaptive / learned ETD to a final time against the oracle")
     ap.add_argument("--c5-variants", type=int, default=32)
     ap.add_argument("--c5-cells", type=int, nargs=3, default=[39, 17, 101])
@@ -977,6 +1108,8 @@ def main():
         return run_c2_accuracy(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "c5-etd":
+        return run_c5_etd(args)
     if (_rank()[1] > 1 and not args.replicas) or args.sharded:
         return run_sharded(args)
     return run_b200(args)

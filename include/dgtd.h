@@ -165,6 +165,20 @@ int dgtd_transient_functionals(dgtd_op *op, const float *y0, float dt, int64_t s
                                const int64_t *fun_idx, const double *fun_w, double *out,
                                float *y_final);
 
+/* Linear functionals of the resident state recorded on the device, for
+ * drivers that step the state themselves (ETD tries, stage-level LSERK4).
+ * dgtd_op_set_functionals stores n_fun functionals (fun_ptr / fun_idx /
+ * fun_w as for dgtd_transient_functionals) and room for max_rows rows;
+ * dgtd_record_functionals writes the functionals of the current state into
+ * row `row` (stream-ordered, no host synchronisation); dgtd_functional_series
+ * copies rows [0, n_rows) to out[n_rows*n_fun] and synchronises.  The
+ * reference evaluates port amplitudes on the host from recorded trajectories
+ * (session.rs:1041-1054). */
+int dgtd_op_set_functionals(dgtd_op *op, int64_t n_fun, const int64_t *fun_ptr, const int64_t *fun_idx,
+                            const double *fun_w, int64_t max_rows);
+int dgtd_record_functionals(dgtd_op *op, int64_t row);
+int dgtd_functional_series(dgtd_op *op, int64_t n_rows, double *out);
+
 /* ---- stage-level stepping for drivers that act between stages
  * (a partitioned run's halo exchange).  One fused LSERK4 stage (0..4) of h on
  * the resident state (explicit.rs:122-133); stage 0 restarts the residual

@@ -192,6 +192,10 @@ struct dgtd_op {
   int64_t kcl_log_n = 0;  // accepted substeps of the last adaptive run
   DevBuf<float> kcl_bak, kcl_e, kcl_stage, kcl_k, kcl_g;
   DevBuf<double> kcl_part;
+  // functionals recorded on the resident state (dgtd_op_set_functionals)
+  DevBuf<int64_t> fn_ptr, fn_idx;
+  DevBuf<double> fn_w, fn_out;
+  int64_t fn_n = 0, fn_rows = 0;
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
@@ -205,6 +209,7 @@ struct dgtd_op {
     kst.free(); skip.free(); mass.free(); absdet.free();
     tc_bvol.free(); tc_blift.free(); err.free();
     kcl_ctl.free(); kcl_log.free(); kcl_bak.free(); kcl_e.free(); kcl_stage.free(); kcl_k.free(); kcl_g.free(); kcl_part.free();
+    fn_ptr.free(); fn_idx.free(); fn_w.free(); fn_out.free();
   }
 };
 
@@ -1094,6 +1099,60 @@ extern "C" int dgtd_transient_functionals(dgtd_op* op, const float* y0, float dt
   d_ptr.free(); d_idx.free(); d_w.free(); d_out.free();
   if (st != DGTD_OK) return st;
   CUDA_TRY(e);
+  return check_kernel_flag(op);
+}
+
+extern "C" int dgtd_op_set_functionals(dgtd_op* op, int64_t n_fun, const int64_t* fun_ptr, const int64_t* fun_idx,
+                                       const double* fun_w, int64_t max_rows) {
+  if (!op || n_fun < 1 || !fun_ptr || max_rows < 1) return set_error(DGTD_ERR_BAD_ARG, "set_functionals: bad argument");
+  if (fun_ptr[0] != 0) return set_error(DGTD_ERR_BAD_ARG, "set_functionals: fun_ptr[0] must be 0");
+  for (int64_t q = 0; q < n_fun; ++q)
+    if (fun_ptr[q + 1] < fun_ptr[q]) return set_error(DGTD_ERR_BAD_ARG, "set_functionals: fun_ptr must not decrease");
+  const int64_t n_terms = fun_ptr[n_fun];
+  if (n_terms > 0 && (!fun_idx || !fun_w)) return set_error(DGTD_ERR_BAD_ARG, "set_functionals: terms missing");
+  std::vector<int64_t> sidx((size_t)n_terms);
+  for (int64_t k = 0; k < n_terms; ++k) {
+    if (fun_idx[k] < 0 || fun_idx[k] >= op->n_dof)
+      return set_error(DGTD_ERR_BAD_ARG, "set_functionals: DOF " + std::to_string(fun_idx[k]) + " out of range");
+    sidx[k] = aos_to_soa_index(fun_idx[k], op->np);
+  }
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));  // the old buffers may still be read
+  op->fn_ptr.free(); op->fn_idx.free(); op->fn_w.free(); op->fn_out.free();
+  op->fn_n = op->fn_rows = 0;
+  DGTD_TRY(op->fn_ptr.alloc(n_fun + 1));
+  DGTD_TRY(op->fn_idx.alloc(std::max<int64_t>(n_terms, 1)));
+  DGTD_TRY(op->fn_w.alloc(std::max<int64_t>(n_terms, 1)));
+  DGTD_TRY(op->fn_out.alloc((size_t)max_rows * n_fun));
+  CUDA_TRY(cudaMemcpyAsync(op->fn_ptr.p, fun_ptr, (n_fun + 1) * 8, cudaMemcpyHostToDevice, op->stream()));
+  if (n_terms > 0) {
+    CUDA_TRY(cudaMemcpyAsync(op->fn_idx.p, sidx.data(), n_terms * 8, cudaMemcpyHostToDevice, op->stream()));
+    CUDA_TRY(cudaMemcpyAsync(op->fn_w.p, fun_w, n_terms * 8, cudaMemcpyHostToDevice, op->stream()));
+  }
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));  // sidx leaves scope
+  op->fn_n = n_fun;
+  op->fn_rows = max_rows;
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_record_functionals(dgtd_op* op, int64_t row) {
+  if (!op || op->fn_n < 1) return set_error(DGTD_ERR_BAD_ARG, "record_functionals: no functionals set");
+  if (row < 0 || row >= op->fn_rows) return set_error(DGTD_ERR_BAD_ARG, "record_functionals: row out of range");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  k_functionals<<<(unsigned)op->fn_n, 256, 0, op->stream()>>>(op->y[op->cur].p, op->fn_ptr.p, op->fn_idx.p,
+                                                              op->fn_w.p, op->fn_out.p + row * op->fn_n);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_functional_series(dgtd_op* op, int64_t n_rows, double* out) {
+  if (!op || !out || op->fn_n < 1 || n_rows < 0 || n_rows > op->fn_rows)
+    return set_error(DGTD_ERR_BAD_ARG, "functional_series: bad argument");
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  if (n_rows > 0)
+    CUDA_TRY(cudaMemcpyAsync(out, op->fn_out.p, (size_t)n_rows * op->fn_n * 8, cudaMemcpyDeviceToHost, op->stream()));
+  CUDA_TRY(cudaStreamSynchronize(op->stream()));
   return check_kernel_flag(op);
 }
 

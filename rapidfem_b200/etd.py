@@ -18,8 +18,9 @@ controller logged) for the next step size and Krylov cap from the history of
 the last four accepted steps; the proposed step is never below the plain
 controller's own next step, it is tried and kept only if its estimate passes,
 otherwise the plain controller decides the step (and its estimate alone decides
-acceptance).  A proposal within 5 % of the plain step is not tried on its own,
-and after a failed proposal the next attempt is the plain controller's.  The training target of a logged step is what its
+acceptance).  A proposal within 5 % of the plain step is not tried on its own;
+after a failed proposal the next attempt is the plain controller's, and after
+k failed proposals in a row the next 2^(k-1) (at most 32) are.  The training target of a logged step is what its
 run says in hindsight: the largest step the plain controller itself took
 within the next LOOKAHEAD accepted steps (a step size it reached and passed
 from a similar state), relative to the previous step, and that step's Krylov
@@ -116,6 +117,8 @@ class EtdStats:
     matvecs: int = 0
     seconds: float = 0.0
     history: list = field(default_factory=list)
+    times: np.ndarray | None = None   # t of each recorded row (0 and every accepted step)
+    series: np.ndarray | None = None  # [rows, n_fun] functionals of the state at `times`
 
 
 def features(hist: list, tol: float, m_max: int, h_ref: float) -> np.ndarray:
@@ -174,7 +177,8 @@ class LearnedEtd:
 
 
 def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEtd | None = None,
-            log: list | None = None, max_attempts=100000, point_dof=None, n_coef=8, src_tol=None):
+            log: list | None = None, max_attempts=100000, point_dof=None, n_coef=8, src_tol=None,
+            functionals=None, max_rows=1 << 16):
     """ETD from t = 0 to t_end on the device-resident state; returns (y, EtdStats).
 
     The source is b*g(t) (b a vector, or the unit vector of `point_dof`), g =
@@ -188,7 +192,9 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
     device: each try reads back only the Krylov dimension and estimate.
     `log`, if given, gets a (features, target) pair per accepted step of the
     plain controller for training (the look-ahead target of the module
-    docstring)."""
+    docstring).  `functionals` [(idx, w), ...] (F(y) = sum w[k] y[idx[k]],
+    e.g. port modal amplitudes) are recorded on the device at t = 0 and after
+    every accepted step, into EtdStats.times / series (at most max_rows rows)."""
     from . import sources as S
 
     driven = waveform is not None and (b is not None or point_dof is not None)
@@ -202,13 +208,24 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
     src_tol = plain.tol if src_tol is None else float(src_tol)
     gop.upload(np.asarray(y0, dtype=np.float32))
     st = EtdStats()
+    times = [0.0]
+    if functionals:
+        gop.set_functionals(functionals, max_rows)
+        gop.record_functionals(0)
+
+    def recorded(t_now):
+        if functionals:
+            if len(times) >= max_rows:
+                raise RuntimeError("ETD run exceeded the functional rows")
+            gop.record_functionals(len(times))
+            times.append(t_now)
     pending = []  # (features, index of the accepted step, previous step) awaiting look-ahead targets
     hist: list[StepRecord] = []
     t, h, m = 0.0, float(h0), plain.m_max
     rejects = 0
     w0 = time.perf_counter()
     attempts = 0
-    failed_last = False
+    skip, streak = 0, 0  # proposals still to skip; consecutive failed proposals
 
     def coef_for(t0, hh):
         """(coef, hh): the step's source polynomial, hh shortened until it fits."""
@@ -236,7 +253,9 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
         feat = features(hist, plain.tol, plain.m_max, h0)
         tried_learned = False
         hp = mp = None
-        if learned is not None and not failed_last:
+        if learned is not None and skip > 0:
+            skip -= 1
+        elif learned is not None:
             hp, mp = learned.propose(hist, h0)
             # never below the plain controller's own next step: the network
             # can only skip ahead of it; a proposal no longer than that step
@@ -244,21 +263,25 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             hp = min(max(hp, h), t_end - t)
             if hp <= 1.05 * min(h, t_end - t):
                 hp = None
-        failed_last = False
         if hp is not None:
             hp, dim, est = attempt(hp, mp)
             tried_learned = True
             if est <= plain.tol:
                 gop.etd_commit()
+                streak = 0
                 st.proposals_kept += 1
                 st.accepted += 1
                 t += hp
+                recorded(t)
                 hist.append(StepRecord(hp, dim, est, rejects))
                 rejects = 0
                 h, m = plain.next_after(hp, est, dim, mp, True)
                 continue
             st.proposals_failed += 1
-            failed_last = True  # the next attempt is the plain controller's alone
+            # the next attempts are the plain controller's alone: one after an
+            # isolated failure, doubling with each further failure in a row
+            streak += 1
+            skip = min(1 << (streak - 1), 32)
         h_try = min(h, t_end - t)
         h_try, dim, est = attempt(h_try, m)
         if est <= plain.tol:
@@ -267,6 +290,7 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             if log is not None and not tried_learned:
                 pending.append((feat, len(hist), hist[-1].h if hist else h0))
             t += h_try
+            recorded(t)
             hist.append(StepRecord(h_try, dim, est, rejects))
             rejects = 0
             h, m = plain.next_after(h_try, est, dim, m, True)
@@ -276,6 +300,9 @@ def run_etd(gop, y0, b, waveform, t_end, h0, plain: PlainEtd, learned: LearnedEt
             h, m = plain.next_after(h_try, est, dim, m, False)
     y = gop.download().astype(np.float64)
     st.seconds = time.perf_counter() - w0
+    if functionals:
+        st.times = np.array(times)
+        st.series = gop.functional_series(len(times))
     st.history = [(r.h, r.dim, r.est) for r in hist]
     if log is not None:
         for feat, k, prev in pending:

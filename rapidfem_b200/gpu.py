@@ -516,5 +516,31 @@ class GpuOperator:
                 raise ValueError("need 5 waveform samples per step")
         check(lib.dgtd_run_lserk_stages(self._h, float(h), int(steps), kind, dof, nat.ptr(gs)))
 
+    def set_functionals(self, functionals, max_rows: int) -> None:
+        """Functionals [(idx, w), ...] (F(y) = sum w[k] y[idx[k]], AoS DOF
+        indices) to record on the resident state, with room for max_rows rows."""
+        idx = [np.ascontiguousarray(i, dtype=np.int64).ravel() for i, _ in functionals]
+        wts = [np.ascontiguousarray(w, dtype=np.float64).ravel() for _, w in functionals]
+        if not idx:
+            raise ValueError("no functionals")
+        for i, w in zip(idx, wts):
+            if i.size != w.size:
+                raise ValueError("functional index and weight arrays differ in length")
+        ptr = np.zeros(len(idx) + 1, dtype=np.int64)
+        ptr[1:] = np.cumsum([i.size for i in idx])
+        self._fn_keep = (np.concatenate(idx), np.concatenate(wts))
+        self._n_fun = len(idx)
+        check(lib.dgtd_op_set_functionals(self._h, len(idx), ptr, nat.ptr(self._fn_keep[0]),
+                                          nat.ptr(self._fn_keep[1]), int(max_rows)))
+
+    def record_functionals(self, row: int) -> None:
+        """The functionals of the current state into row `row` (no synchronisation)."""
+        check(lib.dgtd_record_functionals(self._h, int(row)))
+
+    def functional_series(self, n_rows: int) -> np.ndarray:
+        out = np.empty(int(n_rows) * self._n_fun, dtype=np.float64)
+        check(lib.dgtd_functional_series(self._h, int(n_rows), out))
+        return out.reshape(int(n_rows), self._n_fun)
+
     def apply_device(self, d_y: int, d_dy: int) -> None:
         check(lib.dgtd_apply_device(self._h, C.c_void_p(d_y), C.c_void_p(d_dy)))

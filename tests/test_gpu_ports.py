@@ -99,3 +99,40 @@ def test_session_port_probes_match_port_signals(ctx):
     assert np.max(np.abs(rows[:, 1:] - sig.T)) <= 1e-12 * np.max(np.abs(sig))
     with pytest.raises(ValueError):
         s.port_signals(traj[:, :-1], ["in"])
+
+
+def test_recorded_functionals_on_resident_state(ctx):
+    """dgtd_record_functionals between stage-level LSERK4 calls equals the
+    per-step series of dgtd_transient_functionals, and an ETD run records the
+    same functionals at each accepted step (its last row equals the host
+    projection of its final state)."""
+    from rapidfem_b200 import etd as ETD
+
+    _, _, prod, orc = _guide()
+    steps = 40
+    prof0, prof1, b, dt, g = _drive(prod, orc, steps)
+    gop = G.GpuOperator(ctx, prod)
+    n = gop.n_dof()
+    funcs = [prod.port_modal_weights(0, prof0, "E"), prod.port_modal_weights(1, prof1, "E")]
+    want, _ = gop.transient_functionals(np.zeros(n), dt, steps, 1, drive=("vector", b), g=g, functionals=funcs)
+    gop.upload(np.zeros(n, dtype=np.float32))
+    gop.set_source_vector(b)
+    gop.set_functionals(funcs, steps + 1)
+    gop.record_functionals(0)
+    for k in range(steps):
+        # a held sample per step: the 5 stage values all equal g[k]
+        gop.run_lserk_stages(dt, 1, drive=("vector", None), g_stages=np.full(5, g[k], dtype=np.float32))
+        gop.record_functionals(k + 1)
+    got = gop.functional_series(steps + 1)
+    assert np.array_equal(got, want)
+    with pytest.raises(Exception):
+        gop.record_functionals(steps + 1)  # past the rows set aside
+
+    t0, tau = 30 * dt, 10 * dt
+    wave = lambda t: np.exp(-((np.asarray(t) - t0) / tau) ** 2) * np.cos(2 * np.pi * 1.5 * np.asarray(t))
+    y, st = ETD.run_etd(gop, np.zeros(n), b, wave, steps * dt, 4 * dt, ETD.PlainEtd(1e-7, 24),
+                        functionals=funcs)
+    assert st.series.shape == (st.accepted + 1, 2) and st.times[0] == 0.0
+    assert abs(st.times[-1] - steps * dt) < 1e-9 * steps * dt
+    host = np.array([np.dot(y[i], w) for i, w in funcs])
+    assert np.allclose(st.series[-1], host, rtol=1e-5, atol=1e-9 * np.max(np.abs(want)))
