@@ -199,6 +199,31 @@ int dgtd_lserk_stage_range(dgtd_op *op, float h, int32_t stage, int64_t e_begin,
  * halo exchange of a partitioned (multi-GPU) run. */
 int dgtd_state_gather_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, float *d_buf);
 int dgtd_state_scatter_elements(dgtd_op *op, const int64_t *d_elems, int64_t n, const float *d_buf);
+/* The same for any f32 device vector in the state layout (a Krylov basis
+ * vector), d_vec a device pointer of at least the state's length. */
+int dgtd_vec_gather_elements(dgtd_op *op, const float *d_vec, const int64_t *d_elems, int64_t n, float *d_buf);
+int dgtd_vec_scatter_elements(dgtd_op *op, float *d_vec, const int64_t *d_elems, int64_t n, const float *d_buf);
+
+/* ---- partitioned Krylov / ETD (one part of an element partition per rank).
+ * The part's operator holds its n_owned owned elements first, then its halo
+ * elements.  With the hooks set, every Arnoldi process of the op (dgtd_expmv,
+ * dgtd_etd_step*, dgtd_etd_try) reduces its dot products and norms over the
+ * owned elements only and calls, on the op's stream order:
+ *   halo(user, d_vec)              before each matvec: refresh the halo blocks
+ *                                  of the f32 vector d_vec from the peers;
+ *   sum(user, d_partials, count)   after each partial-sum kernel: replace the
+ *                                  count f64 values at d_partials by their sum
+ *                                  over all parts (an allreduce);
+ * so that every part forms the same Hessenberg matrix, estimate and step
+ * decision.  A hook returns 0, or a nonzero value that the entry point returns
+ * as DGTD_ERR_CUDA.  With hooks set, a point drive may name src_dof = -1 (the
+ * source lies on another part).  n_owned = 0 and null hooks restore the
+ * unpartitioned op.  Requires the f32 Krylov basis and n_owned*6*Np a
+ * multiple of 4 (the sweeps read 16-byte vectors).  The reference has no
+ * partitioned path; its Arnoldi is propagator.rs:186-326. */
+typedef int (*dgtd_halo_hook)(void *user, float *d_vec);
+typedef int (*dgtd_sum_hook)(void *user, double *d_partials, int64_t count);
+int dgtd_op_set_partition(dgtd_op *op, int64_t n_owned, dgtd_halo_hook halo, dgtd_sum_hook sum, void *user);
 
 /* ---- FP64 path ---------------------------------------------------------
  * The same RHS and LSERK4 stage in f64 on the CUDA cores (f64 operators,

@@ -130,6 +130,11 @@ _sig("dgtd_etd_step_poly", C.c_int, _vp, _pd, _pd, _i32, _pd, _f64, _i32, _f64, 
 _sig("dgtd_op_set_krylov_precision", C.c_int, _vp, C.c_int)
 _sig("dgtd_etd_try", C.c_int, _vp, _f64, _i32, _f64, _i32, _vp, C.c_int, _i64, C.POINTER(_i32), C.POINTER(_f64))
 _sig("dgtd_etd_commit", C.c_int, _vp)
+HALO_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p)
+SUM_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64)
+_sig("dgtd_op_set_partition", C.c_int, _vp, _i64, _vp, _vp, _vp)
+_sig("dgtd_vec_gather_elements", C.c_int, _vp, _vp, _vp, _i64, _vp)
+_sig("dgtd_vec_scatter_elements", C.c_int, _vp, _vp, _vp, _i64, _vp)
 _sig("dgtd_op_set_functionals", C.c_int, _vp, _i64, _pl, _vp, _vp, _i64)
 _sig("dgtd_record_functionals", C.c_int, _vp, _i64)
 _sig("dgtd_functional_series", C.c_int, _vp, _i64, _pd)

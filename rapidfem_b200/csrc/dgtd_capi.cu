@@ -196,6 +196,11 @@ struct dgtd_op {
   DevBuf<int64_t> fn_ptr, fn_idx;
   DevBuf<double> fn_w, fn_out;
   int64_t fn_n = 0, fn_rows = 0;
+  // partitioned Krylov (dgtd_op_set_partition): owned elements and the hooks
+  int64_t part_owned = 0;
+  dgtd_halo_hook part_halo = nullptr;
+  dgtd_sum_hook part_sum = nullptr;
+  void* part_user = nullptr;
 
   cudaStream_t stream() const { return ctx->stream; }
   ~dgtd_op() {
@@ -903,6 +908,48 @@ extern "C" int dgtd_state_scatter_elements(dgtd_op* op, const int64_t* d_elems, 
                                                                                        bs, d_buf);
   op->launches++;
   CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_vec_gather_elements(dgtd_op* op, const float* d_vec, const int64_t* d_elems, int64_t n,
+                                        float* d_buf) {
+  if (!op || !d_vec || n < 0 || (n > 0 && (!d_elems || !d_buf)))
+    return set_error(DGTD_ERR_BAD_ARG, "vec_gather_elements: bad argument");
+  if (n == 0) return DGTD_OK;
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  const int bs = 6 * op->np;
+  k_gather_blocks<<<grid_for(n * bs, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(d_vec, d_elems, n, bs, d_buf);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_vec_scatter_elements(dgtd_op* op, float* d_vec, const int64_t* d_elems, int64_t n,
+                                         const float* d_buf) {
+  if (!op || !d_vec || n < 0 || (n > 0 && (!d_elems || !d_buf)))
+    return set_error(DGTD_ERR_BAD_ARG, "vec_scatter_elements: bad argument");
+  if (n == 0) return DGTD_OK;
+  CUDA_TRY(cudaSetDevice(op->ctx->device));
+  const int bs = 6 * op->np;
+  k_scatter_blocks<<<grid_for(n * bs, 256, op->ctx->num_sms), 256, 0, op->stream()>>>(d_vec, d_elems, n, bs, d_buf);
+  op->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return DGTD_OK;
+}
+
+extern "C" int dgtd_op_set_partition(dgtd_op* op, int64_t n_owned, dgtd_halo_hook halo, dgtd_sum_hook sum,
+                                     void* user) {
+  if (!op || n_owned < 0 || n_owned > op->n_elem) return set_error(DGTD_ERR_BAD_ARG, "set_partition: bad argument");
+  if ((n_owned > 0) != (halo != nullptr && sum != nullptr))
+    return set_error(DGTD_ERR_BAD_ARG, "set_partition: give n_owned > 0 with both hooks, or 0 without");
+  // the Krylov sweeps read whole 16-byte vectors: the owned prefix must end on one
+  if ((n_owned * 6 * op->np) % 4 != 0)
+    return set_error(DGTD_ERR_BAD_ARG, "set_partition: the owned DOFs must be a multiple of 4 "
+                                       "(an even number of owned elements at order 4)");
+  op->part_owned = n_owned;
+  op->part_halo = halo;
+  op->part_sum = sum;
+  op->part_user = user;
   return DGTD_OK;
 }
 
@@ -1900,7 +1947,11 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
                  int64_t src_idx, B* out, bool first, int abort_chunks) {
   using namespace dgtd;
   cudaStream_t s = op->stream();
-  const int64_t n = op->n_dof;
+  // a part of a partition reduces over its owned elements (the prefix of the
+  // element-major layout) and sums its partials with the other parts
+  const bool parted = op->part_owned > 0;
+  if (parted && sizeof(B) != 4) return set_error(DGTD_ERR_UNSUPPORTED, "partitioned Krylov needs the f32 basis");
+  const int64_t n = parted ? op->part_owned * 6 * op->np : op->n_dof;
   const int64_t len = (int64_t)state_len(op);
   const int nb = kKrylovBlocks, nt = kKrylovThreads;
   const int gs = grid_for(n, 256, op->ctx->num_sms);
@@ -1908,6 +1959,17 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
   B* vb = kry_bufs<B>(op).basis->p;
   double* pa = op->partials.p;
   double* pb = pa + (size_t)kKrylovBlocks * kKryRow;
+  const int64_t n_part = (int64_t)kKrylovBlocks * kKryRow;
+  auto psum = [&](double* buf) -> int {
+    if (parted && op->part_sum(op->part_user, buf, n_part) != 0)
+      return set_error(DGTD_ERR_CUDA, "partitioned Krylov: the sum hook failed");
+    return DGTD_OK;
+  };
+  auto phalo = [&](const B* vec) -> int {
+    if (parted && op->part_halo(op->part_user, (float*)const_cast<B*>(vec)) != 0)
+      return set_error(DGTD_ERR_CUDA, "partitioned Krylov: the halo hook failed");
+    return DGTD_OK;
+  };
   if (first) {
     struct {
       int dim_total, est_none;
@@ -1921,6 +1983,7 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
   }
   k_kry_norm_partials<B><<<nb, nt, 0, s>>>(v, n, pa);
   KRY_TRACE("norm_partials", -1);
+  DGTD_TRY(psum(pa));
   k_kry_start<<<1, kExpmThreads, 0, s>>>(st, pa, nb, t, tol, P, op->kpoly.p, delta, m, op->skip.p);
   KRY_TRACE("start", -1);
   op->launches += 2;
@@ -1928,14 +1991,18 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
   for (int j = 0; j < m; ++j) {
     B* w = vb + (int64_t)j * len;  // slot j + 1
     const B* vj = kry_col(v, (const B*)vb, len, j);
+    DGTD_TRY(phalo(vj));
     DGTD_TRY(kry_matvec<B>(op, vj, w, bvec, src_idx, st->mv, op->skip.p));
     KRY_TRACE("matvec", j);
     k_kry_dots<B><<<nb, nt, 0, s>>>(v, vb, len, n, j + 1, w, pa, op->skip.p);
     KRY_TRACE("dots", j);
+    DGTD_TRY(psum(pa));
     k_kry_update_dots<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
     KRY_TRACE("update_dots", j);
+    DGTD_TRY(psum(pb));
     k_kry_update_norm<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
     KRY_TRACE("update_norm", j);
+    DGTD_TRY(psum(pa));
     k_kry_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, pa, nb, j, op->skip.p);
     KRY_TRACE("finish_norm", j);
     op->launches += 4;
@@ -2108,8 +2175,11 @@ extern "C" int dgtd_etd_try(dgtd_op* op, double h, int32_t m, double tol, int32_
   const float* bvec = nullptr;
   int P = n_coef;
   if (drive == DGTD_DRIVE_POINT) {
-    if (src_dof < 0 || src_dof >= op->n_dof) return set_error(DGTD_ERR_BAD_ARG, "etd_try: source DOF out of range");
-    src_idx = aos_to_soa_index(src_dof, op->np);
+    // a part of a partition without the source DOF drives nothing locally
+    const bool elsewhere = src_dof == -1 && op->part_owned > 0;
+    if (!elsewhere && (src_dof < 0 || src_dof >= op->n_dof))
+      return set_error(DGTD_ERR_BAD_ARG, "etd_try: source DOF out of range");
+    src_idx = elsewhere ? -1 : aos_to_soa_index(src_dof, op->np);
   } else if (drive == DGTD_DRIVE_VECTOR) {
     if (!op->src_vec_set) return set_error(DGTD_ERR_BAD_ARG, "etd_try: vector drive without a source vector");
     bvec = op->src_vec.p;

@@ -329,6 +329,57 @@ class GpuOperator:
         """A device buffer of element blocks into the resident state."""
         check(lib.dgtd_state_scatter_elements(self._h, d_elems, int(n), d_buf))
 
+    def gather_vec_elements(self, d_vec: int, d_elems: int, n: int, d_buf: int) -> None:
+        """Element blocks of a device vector in the state layout into a device buffer."""
+        check(lib.dgtd_vec_gather_elements(self._h, d_vec, d_elems, int(n), d_buf))
+
+    def scatter_vec_elements(self, d_vec: int, d_elems: int, n: int, d_buf: int) -> None:
+        """A device buffer of element blocks into a device vector in the state layout."""
+        check(lib.dgtd_vec_scatter_elements(self._h, d_vec, d_elems, int(n), d_buf))
+
+    def set_partition(self, n_owned: int, halo=None, reduce=None) -> None:
+        """Make the op one part of an element partition for its Krylov / ETD
+        entry points (dgtd_op_set_partition): dots and norms over the first
+        n_owned elements, `halo(d_vec)` refreshing a device vector's halo blocks
+        before each matvec and `reduce(d_partials, count)` summing f64 partials
+        over all parts in place.  n_owned = 0 restores the undivided op.  An
+        exception in a hook fails the entry point that called it and is
+        re-raised there."""
+        if int(n_owned) == 0:
+            check(lib.dgtd_op_set_partition(self._h, 0, None, None, None))
+            self._part_hooks = None
+            return
+        errors = []
+
+        def on_halo(_user, d_vec):
+            try:
+                halo(int(d_vec))
+                return 0
+            except BaseException as e:  # noqa: BLE001 - carried to the caller
+                errors.append(e)
+                return 1
+
+        def on_sum(_user, d_buf, count):
+            try:
+                reduce(int(d_buf), int(count))
+                return 0
+            except BaseException as e:  # noqa: BLE001
+                errors.append(e)
+                return 1
+
+        hooks = (nat.HALO_HOOK(on_halo), nat.SUM_HOOK(on_sum), errors)
+        check(lib.dgtd_op_set_partition(self._h, int(n_owned), C.cast(hooks[0], C.c_void_p),
+                                        C.cast(hooks[1], C.c_void_p), None))
+        self._part_hooks = hooks  # the C side keeps the function pointers
+
+    def _hook_check(self, status: int) -> None:
+        hooks = getattr(self, "_part_hooks", None)
+        if status != nat.DGTD_OK and hooks is not None and hooks[2]:
+            err = hooks[2].pop(0)
+            hooks[2].clear()
+            raise RuntimeError("a partition hook failed") from err
+        check(status)
+
     def kcl_step(self, y, h):
         """One KCL RK4(3)5 step (explicit_adaptive.rs:84-152): (y_new, err)."""
         y = _f64(y)
@@ -463,8 +514,8 @@ class GpuOperator:
         a = None if coef is None else _f64(coef)
         dim = C.c_int32()
         est = C.c_double()
-        check(lib.dgtd_etd_try(self._h, float(h), int(m), float(tol), 0 if a is None else a.size, nat.ptr(a),
-                               kind, dof, C.byref(dim), C.byref(est)))
+        self._hook_check(lib.dgtd_etd_try(self._h, float(h), int(m), float(tol), 0 if a is None else a.size,
+                                          nat.ptr(a), kind, dof, C.byref(dim), C.byref(est)))
         return dim.value, est.value
 
     def etd_commit(self) -> None:

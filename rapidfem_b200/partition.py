@@ -251,6 +251,27 @@ class GpuEngine:
         finally:
             ctx.set_stream(self.stream.cuda_stream)
 
+    def gather_vec(self, d_vec: int, ids: np.ndarray, buf) -> None:
+        """Element blocks of a device vector (a Krylov basis vector) into `buf`."""
+        self.gop.gather_vec_elements(d_vec, self._index(ids).data_ptr(), ids.size, buf.data_ptr())
+
+    def scatter_vec(self, d_vec: int, ids: np.ndarray, buf) -> None:
+        """Received blocks into a device vector's halo rows, on the communication stream."""
+        ctx = self.gop.ctx
+        ctx.set_stream(self.comm_stream.cuda_stream)
+        try:
+            self.gop.scatter_vec_elements(d_vec, self._index(ids).data_ptr(), ids.size, buf.data_ptr())
+        finally:
+            ctx.set_stream(self.stream.cuda_stream)
+
+    def view_f64(self, d_buf: int, count: int):
+        """A torch view of `count` f64 values of device memory at `d_buf`."""
+        return device_view(self.torch, d_buf, count, "<f8", self.device)
+
+    def reduce_context(self):
+        """Context in which a collective on the partial sums is issued (the compute stream)."""
+        return self.torch.cuda.stream(self.stream)
+
     def stage(self, h: float, s: int) -> None:
         self.gop.lserk_stage(h, s)
 
@@ -392,3 +413,160 @@ class LoopbackLserk:
                     e.sync()
                 for e, p in zip(self.engines, self.parts):
                     e.stage_range(h, s, p.n_interior, p.n_local, True)
+
+
+# --------------------------------------------------------------- Krylov / ETD
+
+class _CudaBuffer:
+    """Device memory described by the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def device_view(torch, ptr: int, n: int, typestr: str, device):
+    """A torch tensor over `n` values of device memory at `ptr` (no copy)."""
+    return torch.as_tensor(_CudaBuffer(ptr, n, typestr), device=device)
+
+
+def local_dof(part: Part, np_: int, dof: int) -> int:
+    """The local AoS DOF of the global AoS DOF `dof` ((e*Np + node)*6 + c) on
+    this part, or -1 when another part owns element e."""
+    bs = 6 * np_
+    e, r = divmod(int(dof), bs)
+    k = np.flatnonzero(part.owned == e)
+    return int(k[0]) * bs + r if k.size else -1
+
+
+class ShardedKrylov:
+    """The Arnoldi process of one part's device operator over a partition
+    (dgtd_op_set_partition): before each matvec the Krylov vector's halo blocks
+    are exchanged with the peers over the transport (as ShardedLserk exchanges
+    the state), and after each partial-sum kernel the f64 partials (the CGS
+    dots and norms, at most (m+1) per pass and one norm) are all-reduced, so
+    every part forms the same Hessenberg matrix, estimate and step decision.
+    The engine's gop then runs dgtd_expmv / dgtd_etd_try (etd.run_etd) as on
+    one domain, with the part's local state and source."""
+
+    def __init__(self, part: Part, engine, transport, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+        self.part = part
+        self.engine = engine
+        self.transport = transport
+        self.sbuf = {q: engine.new_buffer(ids.size) for q, ids in part.send.items()}
+        self.rbuf = {q: engine.new_buffer(ids.size) for q, ids in part.recv.items()}
+        engine.gop.set_partition(part.n_owned, self.halo, self.reduce)
+
+    def halo(self, d_vec: int) -> None:
+        for q, ids in self.part.send.items():
+            self.engine.gather_vec(d_vec, ids, self.sbuf[q])
+        comm = getattr(self.engine, "comm", None)
+        if comm is None:
+            self.transport.exchange(self.sbuf, self.rbuf)
+        else:
+            self.engine.begin_exchange()
+            with comm():
+                self.transport.exchange(self.sbuf, self.rbuf)
+        for q, ids in self.part.recv.items():
+            self.engine.scatter_vec(d_vec, ids, self.rbuf[q])
+        if hasattr(self.engine, "end_exchange"):
+            self.engine.end_exchange()
+
+    def reduce(self, d_buf: int, count: int) -> None:
+        t = self.engine.view_f64(d_buf, count)
+        with self.engine.reduce_context():
+            self.dist.all_reduce(t, group=self.group)
+
+    def close(self) -> None:
+        self.engine.gop.set_partition(0)
+
+
+class LoopbackKrylov:
+    """All parts of a partition on one device, each part's Krylov / ETD run in
+    its own host thread (`run`): the hooks of the parts meet at a barrier, the
+    halo blocks of each Krylov vector are copied from the peers' vectors, and
+    part 0 sums the parts' partials in a fixed order (all on the shared stream
+    of the parts' context, so no host wait is needed between the copies and
+    the kernels).  A part whose thread fails breaks the barrier (and every
+    wait on it ends after `timeout` seconds), so the other parts fail too."""
+
+    def __init__(self, parts: list[Part], engines: list, timeout: float = 120.0):
+        import threading
+
+        self.torch = engines[0].torch
+        self.parts = parts
+        self.engines = engines
+        self.stream = engines[0].stream
+        if any(e.stream is not self.stream for e in engines):
+            raise ValueError("the parts' operators must share one context (one stream)")
+        self.barrier = threading.Barrier(len(parts), timeout=timeout)
+        self.slot = [0] * len(parts)
+        self.bufs = {(q, r): engines[q].new_buffer(ids.size) for r, p in enumerate(parts) for q, ids in p.recv.items()}
+        # index lists on the device before any thread runs
+        self.ids = {}
+        for r, p in enumerate(parts):
+            for q, ids in p.recv.items():
+                self.ids[("recv", r, q)] = engines[r]._index(ids)
+                self.ids[("send", q, r)] = engines[q]._index(parts[q].send[r])
+        for r, (p, e) in enumerate(zip(parts, engines)):
+            e.gop.set_partition(p.n_owned, lambda d, r=r: self._halo(r, d),
+                                lambda d, c, r=r: self._reduce(r, d, c))
+
+    def _halo(self, r: int, d_vec: int) -> None:
+        self.slot[r] = d_vec
+        self.barrier.wait()
+        for q, ids in self.parts[r].recv.items():
+            buf = self.bufs[(q, r)]
+            src = self.ids[("send", q, r)]
+            self.engines[q].gop.gather_vec_elements(self.slot[q], src.data_ptr(), src.numel(), buf.data_ptr())
+            dst = self.ids[("recv", r, q)]
+            self.engines[r].gop.scatter_vec_elements(d_vec, dst.data_ptr(), dst.numel(), buf.data_ptr())
+        self.barrier.wait()
+
+    def _reduce(self, r: int, d_buf: int, count: int) -> None:
+        self.slot[r] = d_buf
+        self.barrier.wait()
+        if r == 0:
+            dev = self.engines[0].device
+            with self.torch.cuda.stream(self.stream):
+                views = [device_view(self.torch, p, count, "<f8", dev) for p in self.slot]
+                total = views[0].clone()
+                for v in views[1:]:
+                    total += v
+                for v in views:
+                    v.copy_(total)
+        self.barrier.wait()
+
+    def run(self, fn) -> list:
+        """fn(r) for every part r, each in its own thread; returns the results
+        in part order and re-raises the first failure."""
+        import threading
+
+        out, err = [None] * len(self.parts), [None] * len(self.parts)
+
+        def body(r):
+            try:
+                out[r] = fn(r)
+            except BaseException as e:  # noqa: BLE001 - re-raised below
+                err[r] = e
+                self.barrier.abort()
+
+        ts = [threading.Thread(target=body, args=(r,)) for r in range(len(self.parts))]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        first = next((e for e in err if e is not None and not isinstance(e, RuntimeError)), None)
+        first = first or next((e for e in err if e is not None), None)
+        if first is not None:
+            raise first
+        return out
+
+    def close(self) -> None:
+        for e in self.engines:
+            e.gop.set_partition(0)
+

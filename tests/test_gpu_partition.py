@@ -100,3 +100,79 @@ def test_stage_range_arguments(ctx):
             gop.lserk_stage_range(1e-3, 0, b, e, False)
     gop.lserk_stage_range(1e-3, 0, 0, 160, False)
     gop.lserk_stage_range(1e-3, 0, 160, 162, True)
+
+
+def _krylov_setup(ctx, n_parts=2):
+    mesh = O.structured_box_jittered(6, 5, 4, 1.0, 0.8, 0.7, 0.1, 3)
+    order = 3  # 120 DOFs per element: every owned prefix ends on a 16-byte vector
+    full = O.MaxwellOperator(mesh, order, 1.0)
+    g_full = G.GpuOperator(ctx, full)
+    parts = PT.build_parts(mesh, PT.morton_partition(mesh, n_parts))
+    dev = torch.device("cuda", 0)
+    ctx2 = G.GpuContext(0)  # the parts share this context's stream
+    engines = [PT.GpuEngine(G.GpuOperator(ctx2, O.MaxwellOperator(p.mesh, order, 1.0)), dev) for p in parts]
+    y0 = np.sin(0.3 + 0.017 * np.arange(full.n_dof))
+    dof = full.nearest_node_dof([0.5, 0.4, 0.35], 0, 2)
+    return mesh, full, g_full, parts, engines, y0, dof
+
+
+def test_loopback_krylov_etd_tries_match_single_domain(ctx):
+    """dgtd_etd_try over a 2-part partition (one host thread per part, halo
+    hooks and all-reduced partial sums) against the undivided op: the same
+    Krylov dimensions, the state to f32 rounding of the reordered sums."""
+    mesh, full, g_full, parts, engines, y0, dof = _krylov_setup(ctx)
+    coef = np.array([1.0, 0.5, -0.2])
+    h, m = 0.02, 24
+    g_full.upload(y0.astype(np.float32))
+    want_dims = []
+    for _ in range(3):
+        d, _ = g_full.etd_try(h, m, 0.0, coef=coef, drive=("point", dof))
+        g_full.etd_commit()
+        want_dims.append(d)
+    want = g_full.download()
+    lk = PT.LoopbackKrylov(parts, engines)
+    locs = PT.split_state(parts, y0, full.np)
+
+    def body(r):
+        gop = engines[r].gop
+        gop.upload(locs[r].astype(np.float32))
+        dims = []
+        ldof = PT.local_dof(parts[r], full.np, dof)
+        for _ in range(3):
+            d, _ = gop.etd_try(h, m, 0.0, coef=coef, drive=("point", ldof))
+            gop.etd_commit()
+            dims.append(d)
+        return gop.download(), dims
+
+    res = lk.run(body)
+    lk.close()
+    assert sum(PT.local_dof(p, full.np, dof) >= 0 for p in parts) == 1
+    assert all(dims == want_dims for _, dims in res)
+    got = PT.join_state(parts, [y for y, _ in res], full.np)
+    assert rel_l2(got, want) < 1e-5
+
+
+def test_loopback_krylov_etd_run_matches_single_domain(ctx):
+    """etd.run_etd with the plain controller on every part (one thread each):
+    the parts take the same steps, and the joined state matches the
+    undivided run."""
+    from rapidfem_b200 import etd as E
+
+    mesh, full, g_full, parts, engines, y0, dof = _krylov_setup(ctx)
+    wave = lambda t: np.sin(2 * np.pi * 1.5 * np.asarray(t)) * np.exp(-((np.asarray(t) - 0.3) / 0.15) ** 2)
+    plain = E.PlainEtd(tol=1e-7, m_max=36)
+    want, st = E.run_etd(g_full, y0, None, wave, 0.3, 0.01, plain, point_dof=dof)
+    lk = PT.LoopbackKrylov(parts, engines)
+    locs = PT.split_state(parts, y0, full.np)
+
+    def body(r):
+        ldof = PT.local_dof(parts[r], full.np, dof)
+        return E.run_etd(engines[r].gop, locs[r], None, wave, 0.3, 0.01, plain, point_dof=ldof)
+
+    res = lk.run(body)
+    lk.close()
+    steps = [s.accepted for _, s in res]
+    assert len(set(steps)) == 1 and len({s.matvecs for _, s in res}) == 1
+    assert abs(steps[0] - st.accepted) <= 1
+    got = PT.join_state(parts, [y for y, _ in res], full.np)
+    assert rel_l2(got, want) < 1e-4

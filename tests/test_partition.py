@@ -199,3 +199,98 @@ def test_partition_rejects_bad_part_count():
     mesh, _, _ = _problem()
     with pytest.raises(ValueError):
         PT.morton_partition(mesh, 0)
+
+
+class CpuVecEngine:
+    """Vectors and partial sums of a partitioned Krylov run as CPU tensors,
+    addressed by their data pointers as the device hooks address device
+    memory: the host side of ShardedKrylov without a device."""
+
+    class _Gop:
+        def __init__(self):
+            self.n_owned, self.hooks = 0, None
+
+        def set_partition(self, n_owned, halo=None, reduce=None):
+            self.n_owned, self.hooks = n_owned, (halo, reduce)
+
+    def __init__(self, bs):
+        self.bs = bs
+        self.reg = {}
+        self.gop = self._Gop()
+
+    def register(self, t):
+        self.reg[t.data_ptr()] = t
+        return t.data_ptr()
+
+    def new_buffer(self, n_elem):
+        return torch.empty(n_elem * self.bs, dtype=torch.float64)
+
+    def gather_vec(self, d_vec, ids, buf):
+        buf.copy_(self.reg[d_vec].view(-1, self.bs)[torch.from_numpy(ids)].reshape(-1))
+
+    def scatter_vec(self, d_vec, ids, buf):
+        self.reg[d_vec].view(-1, self.bs)[torch.from_numpy(ids)] = buf.view(-1, self.bs)
+
+    def view_f64(self, d_buf, count):
+        return self.reg[d_buf][:count]
+
+    def reduce_context(self):
+        import contextlib
+
+        return contextlib.nullcontext()
+
+
+def _krylov_rank_main(rank, world, port_no, tmp):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port_no}", rank=rank, world_size=world)
+    try:
+        mesh, port, mat = _problem()
+        parts = PT.build_parts(mesh, PT.morton_partition(mesh, world), face_port=port, materials=mat)
+        me = parts[rank]
+        bs = 6 * 10  # order 2
+        eng = CpuVecEngine(bs)
+        sk = PT.ShardedKrylov(me, eng, PT.TorchTransport())
+        assert eng.gop.n_owned == me.n_owned
+        # a Krylov vector: owned blocks hold the global vector, halo blocks are stale
+        g = np.sin(0.3 + 0.017 * np.arange(mesh.n_tets * bs))
+        v = torch.from_numpy(PT.split_state(parts, g, 10)[rank].copy())
+        v.view(-1, bs)[me.n_owned:] = float("nan")
+        halo, reduce = eng.gop.hooks
+        halo(eng.register(v))
+        # partial sums: each part's own, summed over the parts in place
+        part_sums = torch.arange(16, dtype=torch.float64) * (rank + 1)
+        reduce(eng.register(part_sums), 12)
+        np.save(os.path.join(tmp, f"v{rank}.npy"), v.numpy())
+        np.save(os.path.join(tmp, f"s{rank}.npy"), part_sums.numpy())
+        sk.close()
+        assert eng.gop.n_owned == 0
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_krylov_hooks():
+    """The host side of the partitioned Krylov path on two gloo ranks: the halo
+    hook refreshes a vector's halo blocks from the peer's owned blocks, the
+    sum hook all-reduces the partial sums in place (only `count` values)."""
+    mesh, port, mat = _problem()
+    bs = 60
+    g = np.sin(0.3 + 0.017 * np.arange(mesh.n_tets * bs))
+    with tempfile.TemporaryDirectory() as tmp:
+        port_no = 29500 + ((os.getpid() + 7) % 2000)
+        mp.spawn(_krylov_rank_main, args=(2, port_no, tmp), nprocs=2, join=True)
+        parts = PT.build_parts(mesh, PT.morton_partition(mesh, 2), face_port=port, materials=mat)
+        for r, p in enumerate(parts):
+            v = np.load(os.path.join(tmp, f"v{r}.npy")).reshape(-1, bs)
+            assert np.array_equal(v, g.reshape(-1, bs)[p.elements])
+            s = np.load(os.path.join(tmp, f"s{r}.npy"))
+            assert np.array_equal(s[:12], np.arange(12) * 3.0) and np.array_equal(s[12:], np.arange(12, 16) * (r + 1))
+
+
+def test_local_dof():
+    mesh, port, mat = _problem()
+    parts = PT.build_parts(mesh, PT.morton_partition(mesh, 3))
+    bs = 6 * 4  # order 1
+    for dof in (0, 7 * bs + 5, (mesh.n_tets - 1) * bs + 23):
+        hits = [PT.local_dof(p, 4, dof) for p in parts]
+        assert sum(h >= 0 for h in hits) == 1
+        r = next(i for i, h in enumerate(hits) if h >= 0)
+        assert parts[r].elements[hits[r] // bs] == dof // bs and hits[r] % bs == dof % bs
