@@ -1997,10 +1997,23 @@ int krylov_chunk(dgtd_op* op, const B* v, double t, int m, double tol, int P, do
     k_kry_dots<B><<<nb, nt, 0, s>>>(v, vb, len, n, j + 1, w, pa, op->skip.p);
     KRY_TRACE("dots", j);
     DGTD_TRY(psum(pa));
-    k_kry_update_dots<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    // the sweeps' register-held columns: the smallest of 4, 8, 12 covering j + 1
+    if (j < 4) {
+      k_kry_update_dots<B, 4><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    } else if (j < 8) {
+      k_kry_update_dots<B, 8><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    } else {
+      k_kry_update_dots<B, kKryCols><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pa, nb, pb, op->skip.p);
+    }
     KRY_TRACE("update_dots", j);
     DGTD_TRY(psum(pb));
-    k_kry_update_norm<B><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    if (j < 4) {
+      k_kry_update_norm<B, 4><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    } else if (j < 8) {
+      k_kry_update_norm<B, 8><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    } else {
+      k_kry_update_norm<B, kKryCols><<<nb, nt, 0, s>>>(st, v, vb, len, n, j, w, pb, nb, pa, op->skip.p);
+    }
     KRY_TRACE("update_norm", j);
     DGTD_TRY(psum(pa));
     k_kry_finish_norm<<<1, kExpmThreads, kExpmSmem, s>>>(st, pa, nb, j, op->skip.p);

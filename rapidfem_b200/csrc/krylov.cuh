@@ -241,11 +241,14 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* sums, int 
 }
 
 // First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
-template <class B>
-__global__ void __launch_bounds__(kKrylovThreads, 1)
+// NC (4, 8 or 12) bounds the columns held in registers: the launch picks the
+// smallest NC >= j + 1, so the early steps of a chunk run two blocks per SM.
+template <class B, int NC>
+__global__ void __launch_bounds__(kKrylovThreads, NC <= 8 ? 2 : 1)
 k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
+  static_assert(NC <= kKryCols, "columns");
   if (*skip) return;
   using KV = KryVec<B>;
   using T = typename KV::T;
@@ -256,17 +259,17 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   sum_partials(partials_in, nb_in, cols, sums);
   kry_proj(st, sums, j, 0, u);
   __syncthreads();
-  double acc[kKryCols];
+  double acc[NC];
 #pragma unroll
-  for (int i = 0; i < kKryCols; ++i) acc[i] = 0.0;
+  for (int i = 0; i < NC; ++i) acc[i] = 0.0;
   double wn[1] = {0.0};
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
     T wk = reinterpret_cast<const T*>(w)[k];
-    T vk[kKryCols];
+    T vk[NC];
 #pragma unroll
-    for (int i = 0; i < kKryCols; ++i)
+    for (int i = 0; i < NC; ++i)
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
     // per lane: the update, then the second pass's products with the stored
     // (rounded) value, so that only one lane's converted values are live
@@ -274,19 +277,19 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
     for (int q = 0; q < KV::W; ++q) {
       double x = KV::at(wk, q);
 #pragma unroll
-      for (int i = 0; i < kKryCols; ++i)
+      for (int i = 0; i < NC; ++i)
         if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
       KV::set(wk, q, x);
       const double xs = KV::at(wk, q);
       wn[0] = fma(xs, xs, wn[0]);
 #pragma unroll
-      for (int i = 0; i < kKryCols; ++i)
+      for (int i = 0; i < NC; ++i)
         if (i < cols) acc[i] = fma(KV::at(vk[i], q), xs, acc[i]);
     }
     reinterpret_cast<T*>(w)[k] = wk;
   }
   double* row = partials_out + (int64_t)blockIdx.x * kKryRow;
-  block_sums<kKryCols>(acc, cols, red, row);
+  block_sums<NC>(acc, cols, red, row);
   __syncthreads();
   block_sums<1>(wn, 1, red, row + kKryNormCol);
 }
@@ -295,11 +298,12 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
 // partials of pass 1 (|w'|^2 < kReorth2 |w|^2); without it block 0 records
 // |[w'; wa]|^2 for the norm finisher and the sweep is skipped.  With it, the
 // second-pass update and the partial sums of |w|^2 (the norm column).
-template <class B>
+template <class B, int NC>
 __global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
+  static_assert(NC <= kKryCols, "columns");
   if (*skip) return;
   using KV = KryVec<B>;
   using T = typename KV::T;
@@ -328,15 +332,15 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
     T wk = reinterpret_cast<const T*>(w)[k];
-    T vk[kKryCols];
+    T vk[NC];
 #pragma unroll
-    for (int i = 0; i < kKryCols; ++i)
+    for (int i = 0; i < NC; ++i)
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
 #pragma unroll
     for (int q = 0; q < KV::W; ++q) {
       double x = KV::at(wk, q);
 #pragma unroll
-      for (int i = 0; i < kKryCols; ++i)
+      for (int i = 0; i < NC; ++i)
         if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
       KV::set(wk, q, x);
       const double xs = KV::at(wk, q);  // the stored (rounded) value

@@ -93,6 +93,17 @@ class Part:
     send: dict = field(default_factory=dict)  # peer -> local ids of owned elements to send
     recv: dict = field(default_factory=dict)  # peer -> local ids of halo slots to fill
     n_interior: int = 0
+    links: list = field(default_factory=list)  # periodic face pairs between local elements, local face ids
+
+    def operator(self, order: int, flux_alpha: float = 1.0):
+        """The part's host operator (MaxwellOperator over the local mesh, face
+        codes and materials) with its periodic links applied."""
+        from .operator import MaxwellOperator
+
+        op = MaxwellOperator(self.mesh, order, flux_alpha, face_port=self.face_port, materials=self.materials)
+        for a, b in self.links:
+            op.link_periodic(a, b)
+        return op
 
     @property
     def n_owned(self) -> int:
@@ -107,19 +118,45 @@ class Part:
         return np.concatenate([self.owned, self.halo])
 
 
-def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None) -> list[Part]:
+def periodic_links(op, pairs) -> list:
+    """The face pairs of periodic links as linked in a global host operator:
+    for each (faces_a, faces_b) of `pairs` (face ids e*4 + local face, as
+    model.periodic_faces_of gives them), (faces_a, the partner of each)."""
+    nbr = op.get("nbr").astype(np.int64)
+    lf = op.get("nbr_lf").astype(np.int64)
+    out = []
+    for a, _ in pairs:
+        a = np.asarray(a, dtype=np.int64)
+        if np.any(nbr[a] < 0):
+            raise ValueError("a periodic face of the pair is not linked in the operator")
+        out.append((a, nbr[a] * 4 + lf[a]))
+    return out
+
+
+def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None, links=None) -> list[Part]:
     """The per-rank pieces of a partition `part[K]` (rank ids 0..R-1).  Owned
     elements are ordered interior first (no face neighbour owned elsewhere;
     the interior run is cut to a multiple of TILE, the cut-off interior
     elements join the boundary run), each run in ascending global id.  Send
     and receive lists of a pair of ranks list the same global elements in the
-    same (ascending global id) order."""
+    same (ascending global id) order.  `links` (periodic_links) adds the
+    periodic face pairs to the neighbour relation; each part keeps, in
+    Part.links, the pairs whose two elements are both local, in local face
+    ids (Part.operator applies them).  A halo element's link to an element
+    that is not local stays a boundary face, which only changes halo rows."""
     part = np.asarray(part, dtype=np.int64)
     K = mesh.n_tets
     if part.shape != (K,):
         raise ValueError("part must have one rank id per element")
     R = int(part.max()) + 1
     nbr = face_neighbours(mesh.tets)
+    links = [(np.asarray(a, dtype=np.int64), np.asarray(b, dtype=np.int64)) for a, b in (links or [])]
+    for a, b in links:
+        if a.shape != b.shape:
+            raise ValueError("periodic link sides differ in length")
+        flat = nbr.reshape(-1)
+        flat[a] = b // 4
+        flat[b] = a // 4
     tets = np.asarray(mesh.tets, dtype=np.int64)
     fp = None if face_port is None else np.asarray(face_port, dtype=np.int32).reshape(K, 4)
     mat = None if materials is None else np.asarray(materials, dtype=np.float64).reshape(K, -1)
@@ -138,8 +175,16 @@ def build_parts(mesh: Mesh, part: np.ndarray, face_port=None, materials=None) ->
         elems = np.concatenate([owned, halo])
         verts, inv = np.unique(tets[elems].ravel(), return_inverse=True)
         local = Mesh(np.ascontiguousarray(mesh.nodes[verts]), inv.reshape(-1, 4).astype(np.int32))
+        loc = -np.ones(K, dtype=np.int64)
+        loc[elems] = np.arange(elems.size)
+        plinks = []
+        for a, b in links:
+            both = (loc[a // 4] >= 0) & (loc[b // 4] >= 0)
+            if np.any(both):
+                plinks.append((loc[a[both] // 4] * 4 + a[both] % 4, loc[b[both] // 4] * 4 + b[both] % 4))
         parts.append(Part(r, owned, halo, local, None if fp is None else np.ascontiguousarray(fp[elems]),
-                          None if mat is None else np.ascontiguousarray(mat[elems]), n_interior=n_int))
+                          None if mat is None else np.ascontiguousarray(mat[elems]), n_interior=n_int,
+                          links=plinks))
     for r, pr in enumerate(parts):
         elems = pr.elements
         order = np.argsort(elems, kind="stable")

@@ -23,6 +23,8 @@ class OracleEngine:
     def __init__(self, part: PT.Part, order: int):
         self.orc = R.Operator(part.mesh.nodes, part.mesh.tets, order, 1.0, face_port=part.face_port,
                               materials=part.materials)
+        for a, b in part.links:
+            self.orc.link_periodic(a, b)
         self.bs = 6 * self.orc.np
         self.a, self.b = R.lserk_coeffs()
         self.y = None
@@ -294,3 +296,43 @@ def test_local_dof():
         assert sum(h >= 0 for h in hits) == 1
         r = next(i for i, h in enumerate(hits) if h >= 0)
         assert parts[r].elements[hits[r] // bs] == dof // bs and hits[r] % bs == dof % bs
+
+
+def test_loopback_periodic_partition_matches_single_domain():
+    """A box periodic in x and z, split in three: the periodic links join the
+    neighbour relation (halo elements across the period), each part links the
+    pairs it holds both sides of, and the run matches the undivided one."""
+    from rapidfem_b200 import model as M
+
+    tm = M.box_tagged(6, 2, 4, 1.0, 0.5, 0.8)
+    pairs = M.periodic_faces_of(tm, M.Model(periodic=[(1, 2), (5, 6)]))
+    order = 2
+    glob = M.operator_from_model(tm, M.Model(periodic=[(1, 2), (5, 6)]), order).op
+    links = PT.periodic_links(glob, pairs)
+    orc = R.Operator(tm.mesh.nodes, tm.mesh.tets, order, 1.0)
+    for a, b in links:
+        orc.link_periodic(a, b)
+    y0 = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    h = 0.5 / orc.power_rho(30)[0]
+    want = orc.lserk(y0, h, 3)
+    parts = PT.build_parts(tm.mesh, PT.morton_partition(tm.mesh, 3), links=links)
+    assert any(p.links for p in parts)
+    for p in parts:
+        # halo: every face neighbour, across the period too
+        nbr = PT.face_neighbours(tm.mesh.tets).reshape(-1)
+        for a, b in links:
+            nbr[a], nbr[b] = b // 4, a // 4
+        need = nbr.reshape(-1, 4)[p.owned].ravel()
+        assert np.array_equal(np.setdiff1d(np.unique(need[need >= 0]), p.owned), p.halo)
+        # the host build links what the oracle links
+        eng_nbr = p.operator(order).get("nbr")
+        loc = R.Operator(p.mesh.nodes, p.mesh.tets, order, 1.0)
+        for a, b in p.links:
+            loc.link_periodic(a, b)
+        assert np.array_equal(eng_nbr, loc.get("nbr"))
+    engines = [OracleEngine(p, order) for p in parts]
+    for e, yl in zip(engines, PT.split_state(parts, y0, orc.np)):
+        e.load(yl)
+    PT.LoopbackLserk(parts, engines).step(h, 3)
+    got = PT.join_state(parts, [e.state() for e in engines], orc.np)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
