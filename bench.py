@@ -969,6 +969,59 @@ def run_c5_etd(args):
     return 0
 
 
+def run_etd_try(args):
+    """One exponential step of the stiff driven configuration timed alone: the
+    graded slab (--ttt-cells), N = 3, a soft E_z point source at the centre
+    whose Gaussian-modulated sine (f = 2, sigma_t = 0.5, t0 = 2.5) enters as an
+    8-term polynomial over the step, h = 0.01, Krylov cap 48 (4 sub-steps of
+    12), tol 1e-6, tensor-core matvec.  `--warmup` committed steps from rest,
+    then the next step's candidate tried `--steps` times (not committed, so
+    every timed try does the same work); reports ms per try and per Arnoldi
+    step."""
+    import torch
+
+    from rapidfem_b200 import gpu as G
+    from rapidfem_b200 import sources as S
+    from rapidfem_b200 import workloads as W
+
+    rank, world, local = _rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    ctx = G.GpuContext(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    op = W.graded_slab(args.ttt_cells, 3).build()
+    gop = G.GpuOperator(ctx, op)
+    dof = op.nearest_node_dof([0.5, 0.5, 0.5], 0, 2)
+    coef, _ = S.step_polynomial(lambda t: S.gaussian_sine(t, 2.5, 0.5, 2.0), 2.0, 0.01, 8)
+    gop.upload(np.zeros(op.n_dof, dtype=np.float32))
+    for _ in range(args.warmup):  # committed: the timed tries start from a driven field
+        gop.etd_try(0.01, 48, args.ttt_tol, coef=coef, drive=("point", dof))
+        gop.etd_commit()
+    stream.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dims = []
+    for _ in range(args.steps):
+        d, est = gop.etd_try(0.01, 48, args.ttt_tol, coef=coef, drive=("point", dof))
+        dims.append(d)
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {"metric": "ms per ETD try", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"graded slab {args.ttt_cells}^3 x 6, N=3, point source, h=0.01, m<=48, "
+                                   f"tol {args.ttt_tol}, tensor-core matvec", "n_dof": op.n_dof,
+                       "arnoldi_steps_per_try": dims[-1], "est": est,
+                       "ms_per_arnoldi_step": ms / max(dims[-1], 1)},
+            "e2e": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_c5(args):
     """The waveguide study: a 22.86 x 10.16 x 60 mm guide (39 x 17 x 101 hex x 6
     tets), N = 3, a centred dielectric post (r = 1.5 mm) with eps_r spread over
@@ -1078,10 +1131,11 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="the partitioned run even on one rank (a one-part partition)")
     ap.add_argument("--workload", default="sphere",
-                    choices=["sphere", "c4", "c5", "c5-etd", "time-to-t", "c2-accuracy"],
+                    choices=["sphere", "c4", "c5", "c5-etd", "time-to-t", "c2-accuracy", "etd-try"],
                     help="sphere: the 48^3 N=4 single-instance workload; c4: the batched cavities; "
                          "c5: the waveguide post variants with port probes; "
                          "c5-etd: two of those variants under the learned ETD controller against FP32 LSERK4; "
+                         "etd-try: one exponential step of the time-to-t configuration timed alone; "
                          "time-to-t: LSERK4 vs adaptive / learned ETD to a final time against the oracle")
     ap.add_argument("--c5-variants", type=int, default=32)
     ap.add_argument("--c5-cells", type=int, nargs=3, default=[39, 17, 101])
@@ -1110,6 +1164,8 @@ def main():
         return run_c5(args)
     if args.workload == "c5-etd":
         return run_c5_etd(args)
+    if args.workload == "etd-try":
+        return run_etd_try(args)
     if (_rank()[1] > 1 and not args.replicas) or args.sharded:
         return run_sharded(args)
     return run_b200(args)
