@@ -605,7 +605,11 @@ class LoopbackKrylov:
             t.start()
         for t in ts:
             t.join()
-        first = next((e for e in err if e is not None and not isinstance(e, RuntimeError)), None)
+        def from_barrier(e):  # a part stopped because another part failed
+            return isinstance(e, threading.BrokenBarrierError) or \
+                isinstance(getattr(e, "__cause__", None), threading.BrokenBarrierError)
+
+        first = next((e for e in err if e is not None and not from_barrier(e)), None)
         first = first or next((e for e in err if e is not None), None)
         if first is not None:
             raise first
