@@ -301,7 +301,8 @@ class GpuOperator:
         out = np.empty_like(y)
         dim = C.c_int32()
         est = C.c_double()
-        check(lib.dgtd_etd_step_est(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim), C.byref(est)))
+        self._hook_check(lib.dgtd_etd_step_est(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim),
+                                               C.byref(est)))
         return out, dim.value, est.value
 
     def lserk_stage(self, h, stage, drive=None, g=0.0):
@@ -470,7 +471,7 @@ class GpuOperator:
             raise ValueError("Krylov dimension must be >= 1")
         out = np.empty_like(v)
         dim = C.c_int32()
-        check(lib.dgtd_expmv(self._h, v, float(t), int(m), float(tol), out, C.byref(dim)))
+        self._hook_check(lib.dgtd_expmv(self._h, v, float(t), int(m), float(tol), out, C.byref(dim)))
         return out, dim.value
 
     def etd_step(self, y, b, h, m, tol=0.0):
@@ -483,7 +484,7 @@ class GpuOperator:
             raise ValueError("Krylov dimension must be >= 1")
         out = np.empty_like(y)
         dim = C.c_int32()
-        check(lib.dgtd_etd_step(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim)))
+        self._hook_check(lib.dgtd_etd_step(self._h, y, b, float(h), int(m), float(tol), out, C.byref(dim)))
         return out, dim.value
 
     def etd_step_poly(self, y, b, coef, h, m, tol=0.0):
@@ -497,8 +498,8 @@ class GpuOperator:
         out = np.empty_like(y)
         dim = C.c_int32()
         est = C.c_double()
-        check(lib.dgtd_etd_step_poly(self._h, y, b, a.size, a, float(h), int(m), float(tol), out, C.byref(dim),
-                                     C.byref(est)))
+        self._hook_check(lib.dgtd_etd_step_poly(self._h, y, b, a.size, a, float(h), int(m), float(tol), out,
+                                                C.byref(dim), C.byref(est)))
         return out, dim.value, est.value
 
     def set_krylov_precision(self, bits: int) -> None:
