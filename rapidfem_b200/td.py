@@ -22,6 +22,8 @@ from . import gpu as G
 from . import operator as O
 
 C_LIGHT = 299_792_458.0
+RESONANCE_STATIC_FRACTION = 1e-3  # constants.rs:305: modes below this share of max |Im| are static
+RESONANCE_MERGE_REL = 1e-3        # constants.rs:308: resonances this close (relative) are one
 KRYLOV_TOL = 1e-10
 _CTX = {}
 
@@ -70,6 +72,25 @@ def _sample(waveform, t):
     except Exception:
         pass
     return np.array([float(waveform(float(x))) for x in np.ravel(t)])
+
+
+def _distance2_colors(nbr: np.ndarray) -> np.ndarray:
+    """Greedy colouring of the elements such that two elements that are face
+    neighbours, or share a face neighbour, differ in colour."""
+    K = nbr.shape[0]
+    adj = [[int(x) for x in row if x >= 0] for row in nbr]
+    color = -np.ones(K, dtype=np.int64)
+    for e in range(K):
+        used = set()
+        for a in adj[e]:
+            used.add(int(color[a]))
+            for b in adj[a]:
+                used.add(int(color[b]))
+        k = 0
+        while k in used:
+            k += 1
+        color[e] = k
+    return color
 
 
 class TdSession:
@@ -150,6 +171,68 @@ class TdSession:
         e = C.c_double()
         check(lib.dgtd_field_energy(self.gop.handle, self._check("y", y), C.byref(e)))
         return e.value
+
+    # ---- the assembled operator and its spectrum
+    def state_space(self):
+        """A as CSR (n, row_ptr, col_idx, values), td.rs:382 over
+        assemble_sparse (rhs.rs:1621-1700): the operator couples an element
+        only to itself and its face neighbours, so its columns are probed
+        with unit vectors, the same local column of every element of one
+        distance-2 colour at once (no two elements of one colour share a
+        neighbour, so each output block comes from one probe), each probe one
+        FP64 RHS on the device (dgtd_apply_f64); exact zeros are dropped and
+        each row's columns ascend.  Memory O(nnz); n_colours * 6 Np probes."""
+        nbr = self.op.get("nbr").astype(np.int64).reshape(-1, 4)
+        K, bs, n = nbr.shape[0], 6 * self.op.np, self.n_dofs()
+        color = _distance2_colors(nbr)
+        rows, cols, vals = [], [], []
+        il = np.arange(bs, dtype=np.int64)
+        for col_id in range(int(color.max()) + 1):
+            src = np.flatnonzero(color == col_id)
+            # (output element, probed element) pairs of this colour's stencils
+            sten = np.concatenate([src[:, None], nbr[src]], axis=1)
+            dst = sten.ravel()
+            owner = np.repeat(src, 5)
+            keep = dst >= 0
+            dst, owner = dst[keep], owner[keep]
+            for jl in range(bs):
+                probe = np.zeros(n)
+                probe[src * bs + jl] = 1.0
+                blk = self.gop.apply_f64(probe).reshape(K, bs)[dst]
+                nz = blk != 0.0
+                rows.append((dst[:, None] * bs + il[None, :])[nz])
+                cols.append(np.broadcast_to((owner * bs + jl)[:, None], blk.shape)[nz])
+                vals.append(blk[nz])
+        r = np.concatenate(rows)
+        c = np.concatenate(cols)
+        v = np.concatenate(vals)
+        order = np.lexsort((c, r))
+        r, c, v = r[order], c[order], v[order]
+        row_ptr = np.zeros(n + 1, dtype=np.int64)
+        np.add.at(row_ptr, r + 1, 1)
+        return n, np.cumsum(row_ptr), c.astype(np.int64), v
+
+    def resonances(self, n: int = 8) -> np.ndarray:
+        """The n lowest distinct resonances (session.rs:1007-1031): the dense
+        spectrum of A, near-static modes (|Im| <= 1e-3 max |Im|) dropped, the
+        least damped first, f = c |Im lambda| / 2 pi, values within 1e-3 of a
+        kept one merged, returned ascending.  Dense, so for modest meshes."""
+        m, row_ptr, col_idx, vals = self.state_space()
+        a = np.zeros((m, m))
+        a[np.repeat(np.arange(m), np.diff(row_ptr)), col_idx] = vals
+        ev = np.linalg.eigvals(a)
+        w_max = float(np.max(np.abs(ev.imag))) if ev.size else 0.0
+        phys = ev[np.abs(ev.imag) > RESONANCE_STATIC_FRACTION * w_max]
+        phys = phys[np.argsort(-phys.real, kind="stable")]
+        out = []
+        for z in phys:
+            f = abs(z.imag) * self.c / (2.0 * math.pi)
+            if any(abs(f - g) <= RESONANCE_MERGE_REL * g for g in out):
+                continue
+            out.append(f)
+            if len(out) >= n:
+                break
+        return np.sort(np.array(out))
 
     # ---- steps
     def step(self, y, h, krylov_dim=40, tol=None):
@@ -345,8 +428,7 @@ class TdTrajectory(np.ndarray):
 class TdODE:
     """The problem as the linear ODE dy/dt = A y for an external integrator
     (problem/td.py:47-72): `rhs(t, y)` has scipy's solve_ivp signature and
-    runs on the device.  The assembled sparse A (`jacobian`) is not built on
-    this path."""
+    runs on the device; `jacobian()` is the assembled sparse A."""
 
     def __init__(self, problem):
         self._p = problem
@@ -356,8 +438,7 @@ class TdODE:
         return self._p._op.apply(y)
 
     def jacobian(self, t=None, y=None):
-        raise NotImplementedError("the assembled sparse operator (state_space) is not built on the B200 path; "
-                                  "use rhs(t, y), which applies it on the device")
+        return self._p.state_space()
 
     def __repr__(self):
         return f"TdODE(n_dofs={self.n_dofs})"
@@ -437,6 +518,20 @@ class ProblemTD:
 
     def cfl_dt(self, *, recompute=False):
         return self._op.cfl_dt(recompute)
+
+    def state_space(self):
+        """The operator A as a scipy.sparse.csr_matrix (problem/td.py:367-379)."""
+        try:
+            from scipy.sparse import csr_matrix
+        except ImportError as e:
+            raise ImportError("scipy is required for state_space() and jacobian()") from e
+        n, row_ptr, col_idx, values = self._op.state_space()
+        return csr_matrix((values, col_idx, row_ptr), shape=(n, n))
+
+    def resonances(self, *, n=8):
+        """Cavity resonant frequencies from the operator's spectrum
+        (problem/td.py:391-399; session.rs:1007-1031).  Dense: modest meshes only."""
+        return np.asarray(self._op.resonances(n))
 
     def ode(self):
         """The problem as dy/dt = A y for an external integrator (problem/td.py:381)."""

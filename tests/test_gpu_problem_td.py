@@ -73,9 +73,49 @@ def test_stepper_ode_and_trajectory():
     ode = p.ode()
     assert ode.n_dofs == n
     assert np.array_equal(ode.rhs(0.0, y0), p.rhs(y0))
-    with pytest.raises(NotImplementedError):
-        ode.jacobian()
+    jac = ode.jacobian()
+    assert jac.shape == (n, n)
+    assert np.linalg.norm(jac @ y0 - p.rhs(y0)) <= 1e-5 * np.linalg.norm(p.rhs(y0))
     with pytest.raises(ValueError):
         p.stepper(dt, method="adaptive")
     ex = p.stepper(2 * dt, krylov_dim=24)(y0)
     assert np.linalg.norm(ex - p.step(y0, 2 * dt, krylov_dim=24)) <= 1e-5 * np.linalg.norm(ex)
+
+
+def test_state_space_matches_the_oracle():
+    """assemble_sparse (rhs.rs:1621-1700, its tests :2260-2330): the probed CSR
+    against the f64 oracle's matrix-free apply, within the stencil bound and
+    genuinely sparse, on an operator with a port face and materials."""
+    from rapidfem_b200 import td as TD
+
+    m = O.structured_box(3, 3, 3)
+    nodes, tets = R.box_mesh(3, 3, 3, 1.0, 1.0, 1.0)
+    port = np.where(O.boundary_faces_on_plane(m, 2, 0.0), 0, -1)
+    eps = np.where(m.nodes[m.tets].mean(axis=1)[:, 0] > 0.5, 4.0, 1.0)
+    mat = O.isotropic_materials(eps, sigma=np.where(eps > 1, 0.3, 0.0))
+    sess = TD.TdSession(O.MaxwellOperator(m, 2, 1.0, face_port=port, materials=mat))
+    orc = R.Operator(nodes, tets, 2, 1.0, face_port=port, materials=mat)
+    n, row_ptr, col_idx, vals = sess.state_space()
+    assert n == orc.n_dof and row_ptr[-1] == vals.size
+    assert np.all(np.diff(row_ptr) >= 0)
+    for r in range(0, n, 97):  # columns ascend within a row
+        assert np.all(np.diff(col_idx[row_ptr[r]:row_ptr[r + 1]]) > 0)
+    stride = 6 * 10
+    assert vals.size <= 5 * stride * n and vals.size < n * n // 4
+    from scipy.sparse import csr_matrix
+    a = csr_matrix((vals, col_idx, row_ptr), shape=(n, n))
+    v = np.cos(1.0 + 0.07 * np.arange(n))
+    want = orc.apply(v)
+    assert np.linalg.norm(a @ v - want) <= 1e-12 * np.linalg.norm(want)
+
+
+def test_resonance_of_the_unit_cube():
+    """session.rs:1373-1382: TE/TM 110 of the unit PEC cube (2x2x2, N = 2,
+    c = 1) at sqrt(2)/2 within 2 %, three ascending values."""
+    from rapidfem_b200 import td as TD
+
+    p = TD.ProblemTD.box(size=(1, 1, 1), cells=(2, 2, 2), order=2, c=1.0)
+    f = p.resonances(n=3)
+    want = np.sqrt(2.0) / 2.0
+    assert f.size == 3 and abs(f[0] - want) / want < 0.02
+    assert np.all(np.diff(f) > 0)
