@@ -259,6 +259,9 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   sum_partials(partials_in, nb_in, cols, sums);
   kry_proj(st, sums, j, 0, u);
   __syncthreads();
+  float uf[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) uf[i] = i < cols ? (float)u[i] : 0.f;
   double acc[NC];
 #pragma unroll
   for (int i = 0; i < NC; ++i) acc[i] = 0.0;
@@ -272,14 +275,24 @@ k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
     for (int i = 0; i < NC; ++i)
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
     // per lane: the update, then the second pass's products with the stored
-    // (rounded) value, so that only one lane's converted values are live
+    // (rounded) value, so that only one lane's converted values are live.
+    // An f32 basis takes the update in f32 (the stored vector is f32; the
+    // dots that build H stay f64); an f64 basis keeps f64 throughout.
 #pragma unroll
     for (int q = 0; q < KV::W; ++q) {
-      double x = KV::at(wk, q);
+      if constexpr (sizeof(B) == 4) {
+        float x = (float)KV::at(wk, q);
 #pragma unroll
-      for (int i = 0; i < NC; ++i)
-        if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
-      KV::set(wk, q, x);
+        for (int i = 0; i < NC; ++i)
+          if (i < cols) x = fmaf(-uf[i], (float)KV::at(vk[i], q), x);
+        KV::set(wk, q, x);
+      } else {
+        double x = KV::at(wk, q);
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+          if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
+        KV::set(wk, q, x);
+      }
       const double xs = KV::at(wk, q);
       wn[0] = fma(xs, xs, wn[0]);
 #pragma unroll
@@ -327,6 +340,9 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
   if (blockIdx.x == 0 && threadIdx.x == 0) st->reorth = 1;
   kry_proj(st, sums, j, 1, u);
   __syncthreads();
+  float uf[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) uf[i] = i < cols ? (float)u[i] : 0.f;
   double acc[1] = {0.0};
   const int64_t nv = (n + KV::W - 1) / KV::W;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -338,11 +354,19 @@ k_kry_update_norm(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__
       if (i < cols) vk[i] = reinterpret_cast<const T*>(kry_col(v0, vb, len, i))[k];
 #pragma unroll
     for (int q = 0; q < KV::W; ++q) {
-      double x = KV::at(wk, q);
+      if constexpr (sizeof(B) == 4) {  // f32 basis: the update in f32, as the first pass
+        float x = (float)KV::at(wk, q);
 #pragma unroll
-      for (int i = 0; i < NC; ++i)
-        if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
-      KV::set(wk, q, x);
+        for (int i = 0; i < NC; ++i)
+          if (i < cols) x = fmaf(-uf[i], (float)KV::at(vk[i], q), x);
+        KV::set(wk, q, x);
+      } else {
+        double x = KV::at(wk, q);
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+          if (i < cols) x = fma(-u[i], KV::at(vk[i], q), x);
+        KV::set(wk, q, x);
+      }
       const double xs = KV::at(wk, q);  // the stored (rounded) value
       acc[0] = fma(xs, xs, acc[0]);
     }
