@@ -242,9 +242,10 @@ __device__ __forceinline__ void kry_proj(KrylovDev* st, const double* sums, int 
 
 // First-pass update w -= sum u_i V_i and the second pass's dots in one sweep.
 // NC (4, 8 or 12) bounds the columns held in registers: the launch picks the
-// smallest NC >= j + 1, so the early steps of a chunk run two blocks per SM.
+// smallest NC >= j + 1.  Every instantiation fits 128 registers (two blocks
+// per SM) with the f32 update of an f32 basis.
 template <class B, int NC>
-__global__ void __launch_bounds__(kKrylovThreads, NC <= 8 ? 2 : 1)
+__global__ void __launch_bounds__(kKrylovThreads, 2)
 k_kry_update_dots(KrylovDev* st, const B* __restrict__ v0, const B* __restrict__ vb, int64_t len, int64_t n,
                   int j, B* __restrict__ w, const double* __restrict__ partials_in, int nb_in,
                   double* __restrict__ partials_out, const int* skip) {
