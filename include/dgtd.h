@@ -99,13 +99,16 @@ typedef struct {
                                       stepping with its own dt (no reference counterpart) */
 } dgtd_op_desc;
 
-/* Contraction engine of the stage / RHS kernels.  A new op uses TF32X3 for
- * orders 1-4 and FP32 for order 5; the Arnoldi matvec always runs on FP32.
+/* Contraction engine of the stage / RHS / Krylov-matvec kernels.  A new op
+ * uses TF32X3 for orders 1-4 and FP32 for order 5.  The two FP32 engines
+ * differ only in the elements per CTA tile (the same arithmetic, so the same
+ * results to the bit); batch autotuning picks per order group.
  * (Split-BF16 products were measured at 1-3e-5 relative error per RHS at
  * N = 4, above the 1e-5 bar, and are not offered.) */
 typedef enum {
     DGTD_ENGINE_FP32 = 0,      /* FP32 FMA on the CUDA cores, orders 1-5 */
-    DGTD_ENGINE_TF32X3 = 1     /* 3xTF32 split products on tcgen05 tensor cores, FP32 accumulate, orders 1-4 */
+    DGTD_ENGINE_TF32X3 = 1,    /* 3xTF32 split products on tcgen05 tensor cores, FP32 accumulate, orders 1-4 */
+    DGTD_ENGINE_FP32_SMALL_TILES = 2  /* DGTD_ENGINE_FP32 with half as many elements per tile */
 } dgtd_engine;
 
 /* GpuOperator::new (gpu/operator.rs:207). Uploads the operator once. */

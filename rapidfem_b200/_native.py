@@ -22,7 +22,7 @@ ERR_NAMES = {
 }
 
 DRIVE_FREE, DRIVE_POINT, DRIVE_VECTOR = 0, 1, 2
-ENGINE_FP32, ENGINE_TF32X3 = 0, 1
+ENGINE_FP32, ENGINE_TF32X3, ENGINE_FP32_SMALL_TILES = 0, 1, 2
 
 
 class DgtdError(RuntimeError):

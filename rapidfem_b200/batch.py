@@ -222,7 +222,7 @@ class BatchRunner:
         self.tuning = []
         self.stream.synchronize()
         for k, (g, gop) in enumerate(zip(self.groups, self.gops)):
-            cands = [nat.ENGINE_FP32] + ([nat.ENGINE_TF32X3] if g.order <= 4 else [])
+            cands = [nat.ENGINE_FP32, nat.ENGINE_FP32_SMALL_TILES] + ([nat.ENGINE_TF32X3] if g.order <= 4 else [])
             times = {}
             for eng in cands:
                 gop.set_engine(eng)
@@ -231,7 +231,8 @@ class BatchRunner:
                 times[eng] = self._time_steps(k, trial_steps)
             best = min(times, key=times.get)
             gop.set_engine(best)
-            name = {nat.ENGINE_FP32: "fp32", nat.ENGINE_TF32X3: "tf32x3"}
+            name = {nat.ENGINE_FP32: "fp32", nat.ENGINE_FP32_SMALL_TILES: "fp32_small_tiles",
+                    nat.ENGINE_TF32X3: "tf32x3"}
             self.tuning.append({"order": g.order, "instances": len(g.members), "n_dof": g.n_dof,
                                 "ms_per_step": {name[k]: round(v, 4) for k, v in times.items()},
                                 "engine": name[best]})

@@ -323,11 +323,11 @@ int to_aos(dgtd_op* op, const TI* soa, TO* aos) {
 }
 
 // ---- RHS kernel dispatch
-template <int N, int MODE>
+template <int N, int MODE, int TD>
 int launch_rhs_n(dgtd_op* op, const RhsParams& P) {
-  using C = Fp32Cfg<N>;
+  using C = Fp32Cfg<N, float, TD>;
   static int blocks_per_sm[8] = {0};
-  auto kern = rhs_fp32_kernel<N, MODE>;
+  auto kern = rhs_fp32_kernel<N, MODE, TD>;
   int& bps = blocks_per_sm[op->ctx->device & 7];
   if (bps == 0) {
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
@@ -409,12 +409,22 @@ int launch_rhs(dgtd_op* op, const RhsParams& P) {
       }
     }
   }
+  if (op->engine == DGTD_ENGINE_FP32_SMALL_TILES) {
+    switch (op->order) {
+      case 1: return launch_rhs_n<1, MODE, 2>(op, P);
+      case 2: return launch_rhs_n<2, MODE, 2>(op, P);
+      case 3: return launch_rhs_n<3, MODE, 2>(op, P);
+      case 4: return launch_rhs_n<4, MODE, 2>(op, P);
+      case 5: return launch_rhs_n<5, MODE, 2>(op, P);
+      default: return set_error(DGTD_ERR_UNSUPPORTED, "order outside 1..5");
+    }
+  }
   switch (op->order) {
-    case 1: return launch_rhs_n<1, MODE>(op, P);
-    case 2: return launch_rhs_n<2, MODE>(op, P);
-    case 3: return launch_rhs_n<3, MODE>(op, P);
-    case 4: return launch_rhs_n<4, MODE>(op, P);
-    case 5: return launch_rhs_n<5, MODE>(op, P);
+    case 1: return launch_rhs_n<1, MODE, 1>(op, P);
+    case 2: return launch_rhs_n<2, MODE, 1>(op, P);
+    case 3: return launch_rhs_n<3, MODE, 1>(op, P);
+    case 4: return launch_rhs_n<4, MODE, 1>(op, P);
+    case 5: return launch_rhs_n<5, MODE, 1>(op, P);
     default: return set_error(DGTD_ERR_UNSUPPORTED, "order outside 1..5");
   }
 }
@@ -728,7 +738,8 @@ extern "C" int dgtd_op_n_dof(const dgtd_op* op, int64_t* n) {
 
 extern "C" int dgtd_op_set_engine(dgtd_op* op, int engine) {
   if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_set_engine: null op");
-  if (engine == DGTD_ENGINE_FP32 || (engine == DGTD_ENGINE_TF32X3 && op->order <= 4)) {
+  if (engine == DGTD_ENGINE_FP32 || engine == DGTD_ENGINE_FP32_SMALL_TILES ||
+      (engine == DGTD_ENGINE_TF32X3 && op->order <= 4)) {
     op->engine = engine;
     return DGTD_OK;
   }

@@ -23,13 +23,15 @@
 
 namespace dgtd {
 
-template <int N, class R = float>
+template <int N, class R = float, int TD = 1>
 struct Fp32Cfg {
   static constexpr int NP = np_of(N);
   static constexpr int NFP = nfp_of(N);
   static constexpr int NF = 4 * NFP;
-  // Elements per tile: ~256 threads, E even so the tile start stays 16B aligned.
-  static constexpr int E = N == 1 ? 64 : N == 2 ? 24 : N == 3 ? 12 : N == 4 ? 8 : 4;
+  // Elements per tile: ~256 threads (TD = 1) or half as many (TD = 2, the
+  // small-tile engine), E even so the tile start stays 16B aligned.
+  static constexpr int E = (N == 1 ? 64 : N == 2 ? 24 : N == 3 ? 12 : N == 4 ? 8 : 4) / TD;
+  static_assert(TD == 1 || TD == 2, "tile divisor");
   static constexpr int THREADS = ((E * NP + 31) / 32) * 32;
   static constexpr int TILE = E * 6 * NP;  // values of state per tile
   // shared memory layout (in R); every region starts on a 16-byte boundary
@@ -68,9 +70,9 @@ __device__ __forceinline__ void cross3f(R ax, R ay, R az, R bx, R by, R bz, R& o
   oz = ax * by - ay * bx;
 }
 
-template <int N, int MODE, class R>
+template <int N, int MODE, class R, int TD = 1>
 __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTablesT<R>& T) {
-  using C = Fp32Cfg<N, R>;
+  using C = Fp32Cfg<N, R, TD>;
   using V = typename Vec16<R>::T;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, E = C::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -348,10 +350,11 @@ __device__ __forceinline__ void rhs_cc_body(const RhsParamsT<R>& P, const OpTabl
   }
 }
 
-// FP32 engine (stage, RHS and the Krylov matvec of an f32 basis).
-template <int N, int MODE>
-__global__ void __launch_bounds__(Fp32Cfg<N>::THREADS) rhs_fp32_kernel(RhsParams P, OpTables T) {
-  rhs_cc_body<N, MODE, float>(P, T);
+// FP32 engine (stage, RHS and the Krylov matvec of an f32 basis); TD = 2 is
+// the same engine with half-size element tiles (DGTD_ENGINE_FP32_SMALL_TILES).
+template <int N, int MODE, int TD = 1>
+__global__ void __launch_bounds__(Fp32Cfg<N, float, TD>::THREADS) rhs_fp32_kernel(RhsParams P, OpTables T) {
+  rhs_cc_body<N, MODE, float, TD>(P, T);
 }
 
 // FP64 path: the same algorithm with f64 operators, records and state (and
