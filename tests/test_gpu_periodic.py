@@ -58,3 +58,45 @@ def test_periodic_plane_wave_device(ctx):
     # the FP64 device path follows the oracle to rounding
     gop = G.GpuOperator(ctx, M.operator_from_model(tm, M.Model(periodic=pairs), 3).op)
     assert rel_l2(gop.transient_f64(y0, t_end / steps, steps), want) < 1e-10
+
+
+def test_periodic_column_passes_plane_wave_device(ctx):
+    """The reference's periodic plane-wave test (rhs.rs:3261-3436) with the
+    device ETD step (f32 basis, tensor-core matvec): energy within 5e-3,
+    forward coherence > 0.85, and > 0.3 above the PEC-walled column."""
+    from .test_periodic import _column, _packet, coherence
+
+    lz = 4.0
+    op_per, orc = _column(1, 1, 16, 0.5, 0.5, lz, [(1, 2), (3, 4), (5, 6)])
+    op_pec, _ = _column(1, 1, 16, 0.5, 0.5, lz, [(1, 2), (3, 4)])
+    g_per, g_pec = G.GpuOperator(ctx, op_per), G.GpuOperator(ctx, op_pec)
+    y0 = _packet(orc.node_coords(), lz)
+    zero = np.zeros_like(y0)
+    yp, yc = y0.copy(), y0.copy()
+    for _ in range(250):
+        yp, _ = g_per.etd_step(yp, zero, 0.04, 24)
+        yc, _ = g_pec.etd_step(yc, zero, 0.04, 24)
+    e0 = orc.field_energy(y0)
+    assert abs(orc.field_energy(yp) - e0) / e0 < 5e-3
+    assert coherence(yp) > 0.85 and coherence(yp) - coherence(yc) > 0.3
+
+
+def test_periodic_box_is_translation_invariant_device(ctx):
+    """The reference's translation-invariance test (rhs.rs:3437-3620) with the
+    device ETD step on the FP64 path (f64 basis and matvec)."""
+    from .test_periodic import _column
+
+    op_all, _ = _column(1, 1, 4, 0.5, 0.5, 1.5, [(1, 2), (3, 4), (5, 6)])
+    op_z, _ = _column(1, 1, 4, 0.5, 0.5, 1.5, [(1, 2), (3, 4)])
+    g_all, g_z = G.GpuOperator(ctx, op_all), G.GpuOperator(ctx, op_z)
+    for g in (g_all, g_z):
+        g.set_krylov_precision(64)
+    y0 = np.zeros(op_all.n_dof)
+    y0[0::6] = 1.0
+    zero = np.zeros_like(y0)
+    ya, yz = y0.copy(), y0.copy()
+    for _ in range(80):
+        ya, _ = g_all.etd_step(ya, zero, 0.05, 18)
+        yz, _ = g_z.etd_step(yz, zero, 0.05, 18)
+    s_all, s_z = float(np.std(ya[0::6])), float(np.std(yz[0::6]))
+    assert s_all < 1e-9 and s_z > 100.0 * s_all

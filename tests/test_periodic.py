@@ -170,3 +170,67 @@ def test_periodic_with_port_and_plate_matches_oracle():
     plain = R.Operator(tm.mesh.nodes, tm.mesh.tets, 2, 1.0, face_port=mo.face_port, materials=mo.materials)
     y = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
     assert rel_l2(plain.apply(y), orc.apply(y)) > 1e-2
+
+
+# The reference's periodic-boundary tests (rhs.rs:3261-3436 and :3437-3620),
+# run on the oracle here and on the device in tests/test_gpu_periodic.py.
+
+def _column(nx, ny, nz, lx, ly, lz, pairs, order=2):
+    """The Kuhn box with the given periodic pairs of its face groups 1..6,
+    central flux, as (host operator, oracle with the same links)."""
+    tm = M.box_tagged(nx, ny, nz, lx, ly, lz)
+    return _linked(tm, order, pairs, alpha=0.0)
+
+
+def _packet(xyz, lz):
+    """E_x = f(z), H_y = -f(z): a Gaussian TEM packet along the column, so the
+    forward coherence sum(E_x (-H_y)) / sum(E_x^2) starts at 1."""
+    f = np.exp(-((xyz[:, 2] - 0.5 * lz) / 0.40) ** 2)
+    y = np.zeros((xyz.shape[0], 6))
+    y[:, 0] = f
+    y[:, 4] = -f
+    return y.ravel()
+
+
+def coherence(y):
+    y = y.reshape(-1, 6)
+    return float(np.sum(y[:, 0] * -y[:, 4]) / np.sum(y[:, 0] ** 2))
+
+
+def test_periodic_column_passes_plane_wave_oracle():
+    """rhs.rs:3261-3436: the packet crosses the periodic z pair as a clean
+    forward wave (energy within 5e-3, coherence > 0.85 after 2.5 box
+    periods), while PEC z walls reflect it (coherence lower by > 0.3)."""
+    lz = 4.0
+    _, per = _column(1, 1, 16, 0.5, 0.5, lz, [(1, 2), (3, 4), (5, 6)])
+    _, pec = _column(1, 1, 16, 0.5, 0.5, lz, [(1, 2), (3, 4)])
+    y0 = _packet(per.node_coords(), lz)
+    assert abs(coherence(y0) - 1.0) < 1e-9
+    zero = np.zeros_like(y0)
+    yp, yc = y0.copy(), y0.copy()
+    for _ in range(250):
+        yp, _ = per.etd_step(yp, zero, 0.04, 24)
+        yc, _ = pec.etd_step(yc, zero, 0.04, 24)
+    assert np.all(np.isfinite(yp)) and np.all(np.isfinite(yc))
+    e0 = per.field_energy(y0)
+    assert abs(per.field_energy(yp) - e0) / e0 < 5e-3
+    assert coherence(yp) > 0.85
+    assert coherence(yp) - coherence(yc) > 0.3
+
+
+def test_periodic_box_is_translation_invariant_oracle():
+    """rhs.rs:3437-3620: a uniform E_x in a fully periodic box stays uniform
+    (std < 1e-9 after 80 ETD steps); with PEC z walls it develops structure
+    (std > 100x that)."""
+    _, per = _column(1, 1, 4, 0.5, 0.5, 1.5, [(1, 2), (3, 4), (5, 6)])
+    _, zpec = _column(1, 1, 4, 0.5, 0.5, 1.5, [(1, 2), (3, 4)])
+    y0 = np.zeros(per.n_dof)
+    y0[0::6] = 1.0
+    zero = np.zeros_like(y0)
+    ya, yz = y0.copy(), y0.copy()
+    for _ in range(80):
+        ya, _ = per.etd_step(ya, zero, 0.05, 18)
+        yz, _ = zpec.etd_step(yz, zero, 0.05, 18)
+    s_all, s_z = float(np.std(ya[0::6])), float(np.std(yz[0::6]))
+    assert s_all < 1e-9
+    assert s_z > 100.0 * s_all
