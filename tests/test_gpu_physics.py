@@ -1,0 +1,60 @@
+"""The reference's operator physics tests (rhs.rs:1995-2030, :2366-2520; see
+tests/test_physics.py for the oracle runs) on the device path: the operator
+assembled by TdSession.state_space (FP64 device RHS), the propagation by the
+device Krylov expmv."""
+import numpy as np
+import pytest
+
+from rapidfem_b200 import gpu as G
+from rapidfem_b200 import operator as O
+from rapidfem_b200 import td as TD
+
+from .test_physics import _port_column, energy_mass, least_damped_re
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(sess):
+    n, row_ptr, col_idx, vals = sess.state_space()
+    a = np.zeros((n, n))
+    a[np.repeat(np.arange(n), np.diff(row_ptr)), col_idx] = vals
+    return a
+
+
+def test_conductivity_damps_at_the_analytic_rate_device():
+    mesh = O.structured_box(1, 1, 1)
+    res = []
+    for sigma in (0.0, 0.2):
+        mat = O.isotropic_materials(np.ones(mesh.n_tets), sigma=np.full(mesh.n_tets, sigma))
+        sess = TD.TdSession(O.MaxwellOperator(mesh, 2, 1.0, materials=mat))
+        res.append(least_damped_re(_dense(sess)))
+    delta, want = res[1] - res[0], -0.2 / 2.0
+    assert abs(delta - want) / abs(want) < 0.1
+
+
+def test_port_operator_only_dissipates_device():
+    mesh, port = _port_column(2, 2.0, 1.0, True)
+    op = O.MaxwellOperator(mesh, 2, 0.0, face_port=port)
+    a = _dense(TD.TdSession(op))
+    ma = energy_mass(op) @ a  # the host operator carries the same arrays as the oracle
+    ev = np.linalg.eigvalsh(ma + ma.T)
+    scale = np.max(np.abs(ma))
+    assert ev.max() < 1e-7 * scale and ev.min() < -1e-3 * scale
+
+
+def test_port_face_drains_field_energy_device():
+    ctx = G.GpuContext(0)
+    kept = {}
+    for with_port in (False, True):
+        mesh, port = _port_column(10, 5.0, 0.5, with_port)
+        op = O.MaxwellOperator(mesh, 2, 0.0, face_port=port)
+        sess = TD.TdSession(op)
+        gop = G.GpuOperator(ctx, op)
+        xyz = op.node_coords()
+        y = np.zeros(op.n_dof)
+        y[0::6] = np.exp(-((xyz[:, 2] - 2.5) / 0.5) ** 2)
+        e0 = sess.field_energy(y)
+        for _ in range(900):
+            y, _ = gop.expmv(y, 0.06, 24)
+        kept[with_port] = sess.field_energy(y) / e0
+    assert kept[False] > 0.95 and kept[True] < 0.5
