@@ -58,3 +58,19 @@ def test_port_face_drains_field_energy_device():
             y, _ = gop.expmv(y, 0.06, 24)
         kept[with_port] = sess.field_energy(y) / e0
     assert kept[False] > 0.95 and kept[True] < 0.5
+
+
+def test_port_injects_a_mode_at_the_group_velocity_device():
+    from .test_physics import group_velocity_check, guide
+
+    _, _, op, _, _ = guide()
+    gop = G.GpuOperator(G.GpuContext(0), op)
+    group_velocity_check(lambda y, b, h, m: gop.etd_step(y, b, h, m)[0], op)
+
+
+def test_port_extracts_the_incident_amplitude_device():
+    from .test_physics import guide, incident_amplitude_check
+
+    _, _, op, _, funcs = guide()
+    gop = G.GpuOperator(G.GpuContext(0), op)
+    incident_amplitude_check(lambda y, b, h, m: gop.etd_step(y, b, h, m)[0], funcs)

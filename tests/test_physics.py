@@ -87,3 +87,79 @@ def test_port_face_drains_field_energy():
             y, _ = orc.expmv(y, 0.06, 24)
         kept[with_port] = orc.field_energy(y) / e0
     assert kept[False] > 0.95 and kept[True] < 0.5
+
+
+# ---- the rectangular waveguide port (rhs.rs:2522-2735): TE10 injected at
+# z = 0 of a 1 x 0.5 x 9 guide (N = 2, central flux), a Gaussian-modulated sine
+OMEGA0 = 1.6 * np.pi
+
+
+def guide():
+    """(mesh, host operator with the TE10 port at z = 0, port source b,
+    P_e / P_h functionals)."""
+    mesh = O.structured_box(2, 1, 18, 1.0, 0.5, 9.0)
+    port = np.where(O.boundary_faces_on_plane(mesh, 2, 0.0), 0, -1)
+    op = O.MaxwellOperator(mesh, 2, 0.0, face_port=port)
+    prof = op.rect_port_profiles(0, [0.0, 0.0, 1.0], (1, 0))
+    return mesh, port, op, op.port_source(0, prof), (op.port_modal_weights(0, prof, "E"),
+                                                     op.port_modal_weights(0, prof, "H"))
+
+
+def pulse(t):
+    return np.exp(-((t - 7.0) / 2.5) ** 2) * np.sin(OMEGA0 * (t - 7.0))
+
+
+def group_velocity_check(etd_step, op):
+    """rhs.rs:2522-2623: the packet's peaks at z = 3.5 and 6.5 (E_y at the
+    guide's centre) travel at the TE10 group velocity sqrt(1 - (pi/a/w0)^2)
+    within 15 %; 850 ETD steps of 0.02 with the source held per step."""
+    b = guide()[3]
+    p1 = op.nearest_node_dof([0.5, 0.25, 3.5], 0, 1)
+    p2 = op.nearest_node_dof([0.5, 0.25, 6.5], 0, 1)
+    y = np.zeros(op.n_dof)
+    pk = [[0.0, 0.0], [0.0, 0.0]]
+    for s in range(850):
+        t = s * 0.02
+        y = etd_step(y, b * pulse(t), 0.02, 20)
+        for k, p in enumerate((p1, p2)):
+            if abs(y[p]) > pk[k][0]:
+                pk[k] = [abs(y[p]), t]
+    assert np.all(np.isfinite(y)) and pk[0][0] > 1e-3 and pk[1][0] > 1e-3
+    v = 3.0 / (pk[1][1] - pk[0][1])
+    vg = np.sqrt(1.0 - (np.pi / OMEGA0) ** 2)
+    assert abs(v - vg) / vg < 0.15
+
+
+def incident_amplitude_check(etd_step, funcs):
+    """rhs.rs:2623-2735: from the port's P_e, P_h series the incident wave
+    A = (P_e + Z P_h) / 2 dominates the reflected B = (P_e - Z P_h) / 2
+    (|B/A| < 0.06, Z = w / sqrt(w^2 - (pi/a)^2) the TE10 impedance) at three
+    frequencies of the band; 700 steps."""
+    b = guide()[3]
+    (ie, we), (ih, wh) = funcs
+    y = np.zeros(b.size)
+    pe, ph = [], []
+    dt = 0.02
+    for s in range(700):
+        y = etd_step(y, b * pulse(s * dt), dt, 20)
+        pe.append(we @ y[ie])
+        ph.append(wh @ y[ih])
+    t = np.arange(700) * dt
+    for w in (1.45 * np.pi, 1.6 * np.pi, 1.75 * np.pi):
+        ker = np.exp(-1j * w * t) * dt
+        fe, fh = np.dot(pe, ker), np.dot(ph, ker)
+        z = w / np.sqrt(w * w - np.pi ** 2)
+        a_inc, b_ref = 0.5 * (fe + z * fh), 0.5 * (fe - z * fh)
+        assert abs(a_inc) > 1e-3 and abs(b_ref) / abs(a_inc) < 0.06
+
+
+def test_port_injects_a_mode_at_the_group_velocity():
+    mesh, port, op, _, _ = guide()
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, face_port=port)
+    group_velocity_check(lambda y, b, h, m: orc.etd_step(y, b, h, m)[0], op)
+
+
+def test_port_extracts_the_incident_amplitude():
+    mesh, port, op, _, funcs = guide()
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, face_port=port)
+    incident_amplitude_check(lambda y, b, h, m: orc.etd_step(y, b, h, m)[0], funcs)
