@@ -74,3 +74,29 @@ def test_port_extracts_the_incident_amplitude_device():
     _, _, op, _, funcs = guide()
     gop = G.GpuOperator(G.GpuContext(0), op)
     incident_amplitude_check(lambda y, b, h, m: gop.etd_step(y, b, h, m)[0], funcs)
+
+
+def test_cavity_fundamental_on_an_irregular_mesh_device():
+    from .test_physics import WANT_FUNDAMENTAL, fundamental
+
+    mesh = O.structured_box_jittered(2, 2, 2, 1.0, 1.0, 1.0, 0.25, 7)
+    re, im = fundamental(_dense(TD.TdSession(O.MaxwellOperator(mesh, 2, 1.0))))
+    assert re < 0.0 and abs(im - WANT_FUNDAMENTAL) / WANT_FUNDAMENTAL < 0.08
+
+
+def test_cavity_fundamental_converges_device():
+    from .test_physics import WANT_FUNDAMENTAL, fundamental
+
+    err = []
+    for cells in (1, 2):
+        sess = TD.TdSession(O.MaxwellOperator(O.structured_box(cells, cells, cells), 2, 1.0))
+        err.append(abs(fundamental(_dense(sess))[1] - WANT_FUNDAMENTAL) / WANT_FUNDAMENTAL)
+    assert err[1] < err[0] and err[1] < 1e-3
+
+
+def test_anisotropic_central_flux_conserves_energy_device():
+    from .test_physics import anisotropic_box, skew_defect
+
+    mesh, mat = anisotropic_box()
+    op = O.MaxwellOperator(mesh, 2, 0.0, materials=mat)
+    assert skew_defect(_dense(TD.TdSession(op)), energy_mass(op)) < 1e-12

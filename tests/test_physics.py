@@ -163,3 +163,59 @@ def test_port_extracts_the_incident_amplitude():
     mesh, port, op, _, funcs = guide()
     orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, face_port=port)
     incident_amplitude_check(lambda y, b, h, m: orc.etd_step(y, b, h, m)[0], funcs)
+
+
+# ---- cavity modes and energy conservation (rhs.rs:1830-1945, :2113-2222)
+WANT_FUNDAMENTAL = np.pi * np.sqrt(2.0)  # TE/TM110 of the unit PEC cube, c = 1
+
+
+def fundamental(a):
+    """(Re, |Im|) of the least-damped physical mode (|Im| > 1)."""
+    ev = np.linalg.eigvals(a)
+    ev = ev[np.abs(ev.imag) > 1.0]
+    z = ev[np.argmax(ev.real)]
+    return float(z.real), float(abs(z.imag))
+
+
+def anisotropic_box():
+    mesh = O.structured_box_jittered(2, 1, 1, 1.0, 0.6, 0.7, 0.2, 5)
+    K = mesh.n_tets
+    mat = np.zeros((K, 8))
+    i = np.arange(K)
+    mat[:, 0], mat[:, 1], mat[:, 2] = 2.0 + (i % 3), 3.0, 1.5
+    mat[:, 3], mat[:, 4], mat[:, 5] = 1.0, 1.2 + 0.3 * (i % 2), 2.0
+    return mesh, mat
+
+
+def skew_defect(a, m):
+    """|M~A + A'M~| / |M~A| (central flux, no loss, PEC: exactly skew)."""
+    ma = m @ a
+    return float(np.linalg.norm(ma + ma.T) / np.linalg.norm(ma))
+
+
+def test_cavity_fundamental_on_an_irregular_mesh():
+    """rhs.rs:2151-2185: jittered 2^3 cube (amplitude 0.25, seed 7), N = 2,
+    upwind: the fundamental is damped (Re < 0) and within 8 % of pi sqrt 2."""
+    mesh = O.structured_box_jittered(2, 2, 2, 1.0, 1.0, 1.0, 0.25, 7)
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 1.0)
+    re, im = fundamental(dense(orc.apply, orc.n_dof))
+    assert re < 0.0 and abs(im - WANT_FUNDAMENTAL) / WANT_FUNDAMENTAL < 0.08
+
+
+def test_cavity_fundamental_converges():
+    """rhs.rs:2187-2222: N = 2 on the 1^3 and 2^3 cubes: the error falls and is
+    below 1e-3 on the finer mesh."""
+    err = []
+    for cells in (1, 2):
+        mesh = O.structured_box(cells, cells, cells)
+        orc = R.Operator(mesh.nodes, mesh.tets, 2, 1.0)
+        err.append(abs(fundamental(dense(orc.apply, orc.n_dof))[1] - WANT_FUNDAMENTAL) / WANT_FUNDAMENTAL)
+    assert err[1] < err[0] and err[1] < 1e-3
+
+
+def test_anisotropic_central_flux_conserves_energy():
+    """rhs.rs:2031-2075: diagonal anisotropic eps and mu varying by element,
+    central flux, jittered mesh: M~A is skew to rounding."""
+    mesh, mat = anisotropic_box()
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, materials=mat)
+    assert skew_defect(dense(orc.apply, orc.n_dof), energy_mass(orc)) < 1e-12
