@@ -269,8 +269,16 @@ class TdSession:
             raise ValueError(f"component must be 'x', 'y' or 'z', got {component!r}")
         return self.op.nearest_node_dof(point, f, cpt)
 
+    def _port(self, name):
+        """(index, spec) of a port of this problem; a name that is not one is
+        refused (python/tests/test_td_model.py:72-78)."""
+        hit = self._ports.get(name)
+        if hit is None:
+            raise ValueError(f"{name!r} is not a port of this problem")
+        return hit
+
     def port_source(self, name):
-        k, spec = self._ports[name]
+        k, spec = self._port(name)
         if spec.get("mode") is None:
             return np.zeros(self.n_dofs())
         prof = self.op.rect_port_profiles(k, spec["inward_normal"], spec["mode"])
@@ -281,7 +289,7 @@ class TdSession:
         (rhs.rs:1211-1242)."""
         if name not in self._ports:
             raise ValueError(f"no port named {name!r}")
-        k, spec = self._ports[name]
+        k, spec = self._port(name)
         if spec.get("mode") is None:
             raise ValueError(f"port {name!r} is an absorbing boundary, not a modal port")
         prof = self.op.rect_port_profiles(k, spec["inward_normal"], spec["mode"])

@@ -119,3 +119,30 @@ def test_resonance_of_the_unit_cube():
     want = np.sqrt(2.0) / 2.0
     assert f.size == 3 and abs(f[0] - want) / want < 0.02
     assert np.all(np.diff(f) > 0)
+
+
+def test_driven_transient_from_a_model_port():
+    """python/tests/test_td_model.py:34-78 on a model-built guide: a port-driven
+    run starts at zero and injects the pulse, the GaussianPulse object and a
+    Python callable of it drive the same run to the bit, the port signal has a
+    row per frame, and a name that is not a port is refused."""
+    from rapidfem_b200 import model as M
+    from rapidfem_b200 import td as TD
+
+    tm = M.box_tagged(3, 2, 6, 22.86e-3, 10.16e-3, 60e-3)
+    p = TD.ProblemTD.from_model(tm, M.Model(faces=[M.RectangularPort(5, (1, 0)), M.AbcFace(6)]),
+                                order=1, flux="upwind")
+    pulse = TD.GaussianPulse(t0=90e-12, tau=22e-12, f0=10e9)
+    t = np.linspace(0.0, 200e-12, 9)
+    ref = np.exp(-((t - 90e-12) / 22e-12) ** 2) * np.cos(2 * np.pi * 10e9 * (t - 90e-12))
+    assert np.allclose(pulse(t), ref, rtol=0.0, atol=1e-15) and pulse(90e-12) == 1.0
+    run = dict(port=5, dt=3e-12, steps=20, method="explicit", verbose=False)
+    native = p.transient(waveform=pulse, **run)
+    python = p.transient(waveform=lambda s: pulse(s), **run)
+    amp = np.linalg.norm(np.asarray(native), axis=1)
+    assert np.all(np.isfinite(native)) and amp[0] == 0.0 and amp.max() > 0.0
+    assert np.array_equal(native, python)
+    _, rows = p.port_signals(native, [5])
+    assert rows.shape == (1, 21) and np.abs(rows).max() > 0.0
+    with pytest.raises(ValueError, match="not a port"):
+        p.transient(port=99, waveform=pulse, dt=3e-12, steps=1, verbose=False)
