@@ -146,6 +146,36 @@ def test_krylov_matches_lserk_on_the_dg_operator():
     assert dim < 40
 
 
+def test_kcl_matches_the_exponential_propagator_below_cfl():
+    # explicit_adaptive.rs:219-255: one KCL RK4(3)5 step of 1e-3 vs expmv, < 1e-9.
+    nodes, tets = R.box_mesh(2, 2, 2)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    y0 = np.sin(0.3 + 0.017 * np.arange(op.n_dof))
+    got, _ = op.kcl_step(y0, 1e-3)
+    want, _ = op.expmv(y0, 1e-3, 40, 0.0)
+    assert rel_l2(got, want) < 1e-9
+
+
+def test_kcl_and_lserk4_driven_match_etd_below_cfl():
+    # explicit.rs:265-313, explicit_adaptive.rs:257-300: one driven step of 1e-3
+    # (a point source of 0.7, a spread vector source) vs the ETD step, < 1e-9.
+    nodes, tets = R.box_mesh(2, 2, 2)
+    op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
+    n = op.n_dof
+    y0 = np.sin(0.2 + 0.019 * np.arange(n))
+    sdof = n // 3
+    point = np.zeros(n)
+    point[sdof] = 0.7
+    spread = 0.4 * np.cos(0.11 * np.arange(n))
+    for b, kw in ((point, dict(src_dof=sdof)), (spread, dict(src_vec=spread))):
+        g = 0.7 if "src_dof" in kw else 1.0
+        want, _ = op.etd_step(y0, b, 1e-3, 40)
+        kcl, _ = op.kcl_step(y0, 1e-3, g=g, **kw)
+        assert rel_l2(kcl, want) < 1e-9
+        rk = op.lserk(y0, 1e-3, 1, vals=np.array([g]), **kw)
+        assert rel_l2(rk, want) < 1e-9
+
+
 def test_etd_step_matches_augmented_dense():
     nodes, tets = R.box_mesh(1, 1, 1)
     op = R.Operator(nodes, tets, 2, flux_alpha=1.0)
