@@ -200,14 +200,36 @@ def run_reference(args):
     return 0
 
 
+def _init_nccl(local, seconds):
+    """The NCCL process group of this rank on cuda:`local`, its communicator
+    created at once (a barrier), with file descriptor 1 pointed at stderr
+    meanwhile: NCCL's version banner and init log lines go to stderr, so
+    stdout carries only the JSON line."""
+    import datetime
+
+    import torch
+
+    torch.cuda.set_device(local)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=seconds),
+                                             device_id=torch.device("cuda", local))
+        torch.distributed.barrier()
+        torch.cuda.synchronize()
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def run_sharded(args):
     """The 48^3 sphere_pulse workload partitioned across the N ranks (strong
     scaling): a Morton element partition, one local operator per rank over its
     owned elements and halo, LSERK4 stages with one halo exchange each over
     NCCL point-to-point, the interior elements' update overlapping the
     exchange (partition.ShardedLserk).  `value` counts the global DOFs."""
-    import datetime
-
     import torch
 
     from rapidfem_b200 import gpu as G
@@ -221,9 +243,8 @@ def run_sharded(args):
         os.environ.setdefault("MASTER_PORT", str(29400 + os.getpid() % 1000))
         os.environ.setdefault("RANK", "0")
         os.environ.setdefault("WORLD_SIZE", "1")
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    _init_nccl(local, 120)
     wl = W.sphere_pulse(args.cells, 4)
     parts = PT.build_parts(wl.mesh, PT.morton_partition(wl.mesh, world), materials=wl.materials)
     me = parts[rank]
@@ -337,8 +358,7 @@ def run_b200(args):
     rank, world, local = _rank()
     dist = world > 1
     if dist:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        _init_nccl(local, 120)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
@@ -477,8 +497,7 @@ def run_c4(args):
     rank, world, local = _rank()
     dist = world > 1
     if dist:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        _init_nccl(local, 300)
     torch.cuda.set_device(local)
     inst = B.random_cavities(args.instances, seed=20250)
     groups = B.build_groups(inst)
