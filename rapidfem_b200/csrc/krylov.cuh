@@ -440,15 +440,22 @@ __device__ void block_matmul(const double* A, const double* B, double* C, int d)
 }
 
 // a: d*d input (shared), out: d*d result (shared), b, term, term2 scratch (shared).
+// Each Taylor term and each squaring is one block-wide pass (the term's
+// division by k and its addition to the sum ride along with the product,
+// into the other buffer of a ping-pong pair), with the same operations in the
+// same order per entry as a product followed by an update pass.
 __device__ void block_expm(const double* a, int d, double* out, double* b, double* term, double* term2) {
   __shared__ int s_sq;
+  __shared__ double s_row[kKrylovMaxDim];
+  for (int i = threadIdx.x; i < d; i += blockDim.x) {
+    double row = 0.0;
+    for (int j = 0; j < d; ++j) row += fabs(a[i * d + j]);
+    s_row[i] = row;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     double nrm = 0.0;
-    for (int i = 0; i < d; ++i) {
-      double row = 0.0;
-      for (int j = 0; j < d; ++j) row += fabs(a[i * d + j]);
-      nrm = fmax(nrm, row);
-    }
+    for (int i = 0; i < d; ++i) nrm = fmax(nrm, s_row[i]);
     // squarings: ceil(log2 |a|) + 1 for |a| > 1/2; a non-finite norm (a
     // Hessenberg matrix that overflowed) gets none, so the result is
     // non-finite and the caller rejects it, and a finite norm needs at most
@@ -468,21 +475,39 @@ __device__ void block_expm(const double* a, int d, double* out, double* b, doubl
     term[idx] = out[idx];
   }
   __syncthreads();
+  double* cur = term;
+  double* nxt = term2;
   for (int k = 1; k <= 18; ++k) {
-    block_matmul(term, b, term2, d);
-    __syncthreads();
     const double inv = 1.0 / (double)k;
     for (int idx = threadIdx.x; idx < d * d; idx += blockDim.x) {
-      const double t2 = term2[idx] * inv;
+      const int i = idx / d, j = idx - i * d;
+      double s = 0.0;
+      for (int q = 0; q < d; ++q) {
+        const double aik = cur[i * d + q];
+        if (aik == 0.0) continue;
+        s = __dadd_rn(s, __dmul_rn(aik, b[q * d + j]));
+      }
+      const double t2 = s * inv;
       out[idx] += t2;
-      term[idx] = t2;
+      nxt[idx] = t2;
     }
     __syncthreads();
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
   }
+  // squarings, ping-ponging between out and term2
+  double* src = out;
+  double* dst = term2;
   for (int q = 0; q < sq; ++q) {
-    block_matmul(out, out, term2, d);
+    block_matmul(src, src, dst, d);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < d * d; idx += blockDim.x) out[idx] = term2[idx];
+    double* t = src;
+    src = dst;
+    dst = t;
+  }
+  if (src != out) {
+    for (int idx = threadIdx.x; idx < d * d; idx += blockDim.x) out[idx] = src[idx];
     __syncthreads();
   }
 }
