@@ -107,7 +107,7 @@ typedef struct {
  * N = 4, above the 1e-5 bar, and are not offered.) */
 typedef enum {
     DGTD_ENGINE_FP32 = 0,      /* FP32 FMA on the CUDA cores, orders 1-5 */
-    DGTD_ENGINE_TF32X3 = 1,    /* 3xTF32 split products on tcgen05 tensor cores, FP32 accumulate, orders 1-4 */
+    DGTD_ENGINE_TF32X3 = 1,    /* 3xTF32 split products on tcgen05 tensor cores, FP32 accumulate, orders 1-5 */
     DGTD_ENGINE_FP32_SMALL_TILES = 2  /* DGTD_ENGINE_FP32 with half as many elements per tile */
 } dgtd_engine;
 
@@ -190,8 +190,8 @@ int dgtd_functional_series(dgtd_op *op, int64_t n_rows, double *out);
 int dgtd_lserk_stage(dgtd_op *op, float h, int32_t stage, int drive, int64_t src_dof, float g);
 /* dgtd_lserk_stage on the elements [e_begin, e_end) only, for a partitioned
  * run that overlaps its halo exchange with the elements that do not need the
- * halo: e_begin a multiple of 20 (the tensor-core tile), e_end a multiple of
- * 20 or n_elem.  flip != 0 makes the stage's output the current state (the
+ * halo: e_begin a multiple of the op's tensor-core tile (20 elements at
+ * orders 1-4, 8 at order 5), e_end a multiple of it or n_elem.  flip != 0 makes the stage's output the current state (the
  * last range of a stage); the ranges of one stage read the same input.  No
  * counterpart in the reference. */
 int dgtd_lserk_stage_range(dgtd_op *op, float h, int32_t stage, int64_t e_begin, int64_t e_end, int32_t flip,
@@ -379,8 +379,8 @@ int dgtd_apply_device(dgtd_op *op, const float *d_y, float *d_dy);
  * scratch -- two SoA state buffers and the residual register -- is a
  * file-scope device array of 3 x 2,097,152 floats (24 MiB) that every GPU
  * loading the library holds until exit.  The kernels work on whole tiles of
- * 20 elements, so the limit applies to n_elem rounded up to a multiple of 20,
- * times 6*Np: an op above it is rejected with DGTD_ERR_BAD_ARG.  The first
+ * 20 elements (8 at order 5), so the limit applies to n_elem rounded up to a
+ * multiple of the tile, times 6*Np: an op above it is rejected with DGTD_ERR_BAD_ARG.  The first
  * call on a device takes the array's device address (cudaGetSymbolAddress),
  * so make that first call before any stream capture.  All calls share the one
  * array: calls whose work overlaps on the GPU (other streams, other threads)
@@ -440,11 +440,12 @@ int dgtd_mlp_train(dgtd_mlp *mlp, const float *x, const float *t, int64_t batch,
  * Dense exp(A) of a d x d row-major matrix (d <= 64) by the device kernel the
  * Krylov finisher uses (Taylor-18 + scaling and squaring, propagator.rs:69-114). */
 int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
-/* One-CTA tcgen05 GEMM C[128 x n] = A[128 x k] * B[n x k]^T (row-major f32)
+/* One-CTA tcgen05 GEMM C[M x n] = A[M x k] * B[n x k]^T (row-major f32)
  * through the operand layout, descriptors and TMEM path of the tensor-core RHS
  * kernel.  flags bit 0: 3xTF32 split products (else one tf32 product); bit 1:
- * A operand in TMEM (else shared memory).
- * 16 <= n <= 256 (n % 16 == 0), 8 <= k <= 64 (k % 8 == 0). */
+ * A operand in TMEM (else shared memory); bit 2: M = 64 (else 128).  c gets
+ * the 128 TMEM lanes x n: at M = 64 row 16 q + r (r < 16) is lane 32 q + r.
+ * n <= 256 a multiple of 16 (of 8 at M = 64), 8 <= k <= 64 (k % 8 == 0). */
 int dgtd_debug_tc_gemm(dgtd_ctx *ctx, const float *a, const float *b, float *c, int32_t n, int32_t k,
                        int32_t flags);
 /* The bounded wait of the tensor-core kernels, run by one thread on an

@@ -10,8 +10,8 @@ would alone: its geometric factors are computed from the same coordinates.
 Every element carries its instance's own LSERK4 step as a per-element
 multiplier of the stage step (element record word 43), so one fused stage
 launch per order group steps every instance with its own dt.  An autotuner
-times the stage kernels available for each group (tensor-core for orders
-1-4, FP32 CUDA cores) and keeps the faster; the steps are then captured into a
+times the stage kernels for each group (tensor cores, FP32 CUDA cores with
+the full or the half tile) and keeps the fastest; the steps are then captured into a
 CUDA graph (an even number per graph, so that the ping-pong state buffers end
 where they started) and replayed.
 """
@@ -222,7 +222,7 @@ class BatchRunner:
         self.tuning = []
         self.stream.synchronize()
         for k, (g, gop) in enumerate(zip(self.groups, self.gops)):
-            cands = [nat.ENGINE_FP32, nat.ENGINE_FP32_SMALL_TILES] + ([nat.ENGINE_TF32X3] if g.order <= 4 else [])
+            cands = [nat.ENGINE_FP32, nat.ENGINE_FP32_SMALL_TILES, nat.ENGINE_TF32X3]
             times = {}
             for eng in cands:
                 gop.set_engine(eng)

@@ -405,7 +405,8 @@ int launch_rhs(dgtd_op* op, const RhsParams& P) {
         case 2: return launch_rhs_tc_n<2, MODE>(op, P);
         case 3: return launch_rhs_tc_n<3, MODE>(op, P);
         case 4: return launch_rhs_tc_n<4, MODE>(op, P);
-        default: return set_error(DGTD_ERR_UNSUPPORTED, "tensor-core engine covers orders 1..4");
+        case 5: return launch_rhs_tc_n<5, MODE>(op, P);
+        default: return set_error(DGTD_ERR_UNSUPPORTED, "order outside 1..5");
       }
     }
   }
@@ -494,7 +495,8 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   const int N = d->order, np = dgtd::np_of(N), nfp = dgtd::nfp_of(N);
   const int64_t K = d->n_elem;
   // Host-side packing: element records, gather tables.
-  const int64_t Kpad = ((K + dgtd::kTcTileE - 1) / dgtd::kTcTileE) * dgtd::kTcTileE;
+  const int64_t tile_e = dgtd::tc_tile_e(N);  // tensor-core tile of this order
+  const int64_t Kpad = ((K + tile_e - 1) / tile_e) * tile_e;
   std::vector<float> meta((size_t)Kpad * dgtd::kMetaWords, 0.f);
   // the same records in f64 for the FP64 path, integer words as exact values
   std::vector<double> meta64((size_t)Kpad * dgtd::kMetaWords, 0.0);
@@ -646,7 +648,7 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   if (!e) e = cudaMemsetAsync(op->y[1].p, 0, op->y[1].n * 4, s);
   if (!e) e = cudaMemsetAsync(op->p.p, 0, op->p.n * 4, s);
   if (!e) e = cudaMemsetAsync(op->err.p, 0, sizeof(int), s);
-  if (!e && N <= 4) {
+  if (!e) {
     // 3xTF32 constant operands: tf32 hi/lo of D_k (rows (k,i), K = node j) and
     // LIFT (rows i, K = face node s), chunk-major K-major layout.
     auto tf32 = [](double x) {
@@ -671,8 +673,8 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
     };
     // LIFT K is laid out per face, each face padded to KLF = Nfp rounded up to 8,
     // so the MMAs of a face pair can start while the other pair's flux is formed.
-    const int KV = dgtd::tc_r8(np), NV = dgtd::tc_r16(3 * np), KLF = dgtd::tc_r8(nfp), KL = 4 * KLF;
-    const int NL = dgtd::tc_r16(np);
+    const int KV = dgtd::tc_r8(np), NV = dgtd::tc_nv(N), KLF = dgtd::tc_r8(nfp), KL = 4 * KLF;
+    const int NL = dgtd::tc_nl(N);
     std::vector<float> bv, bl;
     build(NV, KV, [&](int r, int k) -> double {
       if (r >= 3 * np || k >= np) return 0.0;
@@ -739,7 +741,7 @@ extern "C" int dgtd_op_n_dof(const dgtd_op* op, int64_t* n) {
 extern "C" int dgtd_op_set_engine(dgtd_op* op, int engine) {
   if (!op) return set_error(DGTD_ERR_BAD_ARG, "op_set_engine: null op");
   if (engine == DGTD_ENGINE_FP32 || engine == DGTD_ENGINE_FP32_SMALL_TILES ||
-      (engine == DGTD_ENGINE_TF32X3 && op->order <= 4)) {
+      engine == DGTD_ENGINE_TF32X3) {
     op->engine = engine;
     return DGTD_OK;
   }
@@ -973,10 +975,12 @@ extern "C" int dgtd_lserk_stage_range(dgtd_op* op, float h, int32_t stage, int64
                                       int32_t flip, int drive, int64_t src_dof, float g) {
   if (!op || stage < 0 || stage > 4) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: stage must be 0..4");
   if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "lserk_stage: step must be positive");
-  if (e_begin < 0 || e_end > op->n_elem || e_begin >= e_end || (e_begin % kTcTileE) != 0 ||
-      ((e_end % kTcTileE) != 0 && e_end != op->n_elem))
+  const int64_t tile = tc_tile_e(op->order);
+  if (e_begin < 0 || e_end > op->n_elem || e_begin >= e_end || (e_begin % tile) != 0 ||
+      ((e_end % tile) != 0 && e_end != op->n_elem))
     return set_error(DGTD_ERR_BAD_ARG, "lserk_stage_range: need 0 <= e_begin < e_end <= n_elem, e_begin a "
-                                       "multiple of 20 and e_end a multiple of 20 or n_elem");
+                                       "multiple of the op's tile (" + std::to_string(tile) +
+                                       " elements) and e_end one or n_elem");
   CUDA_TRY(cudaSetDevice(op->ctx->device));
   int64_t src_idx;
   DGTD_TRY(check_drive(op, drive, src_dof, &g, 1, &src_idx));
@@ -2536,7 +2540,7 @@ extern "C" int dgtd_run_lserk_static(dgtd_op* op, const float* d_y_in, float* d_
   if (!(std::isfinite(h) && h > 0.f)) return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: step must be positive");
   const int64_t padded = op->n_elem_pad * 6 * op->np;  // the kernels touch whole tiles
   if (padded > kStaticMaxDof)
-    return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: the op's state padded to whole 20-element tiles (" +
+    return set_error(DGTD_ERR_BAD_ARG, "run_lserk_static: the op's state padded to whole tiles (" +
                                            std::to_string(op->n_elem_pad) + " elements x " +
                                            std::to_string(6 * op->np) + " = " + std::to_string(padded) +
                                            " values, n_dof " + std::to_string(op->n_dof) +
@@ -2601,9 +2605,11 @@ extern "C" int dgtd_debug_wait_timeout(dgtd_ctx* ctx, int64_t max_polls, double*
 
 extern "C" int dgtd_debug_tc_gemm(dgtd_ctx* ctx, const float* a, const float* b, float* c, int32_t n, int32_t k,
                                   int32_t flags) {
-  if (!ctx || !a || !b || !c || n < 16 || n > dgtd::kSelftestMaxN || (n % 16) || k < 8 ||
+  const int n_step = (flags & 4) ? 8 : 16;  // MMA N granularity at M = 64 / 128
+  if (!ctx || !a || !b || !c || n < n_step || n > dgtd::kSelftestMaxN || (n % n_step) || k < 8 ||
       k > dgtd::kSelftestMaxK || (k % 8))
-    return set_error(DGTD_ERR_BAD_ARG, "debug_tc_gemm: need 16 <= N <= 256 (N % 16 == 0), 8 <= K <= 64 (K % 8 == 0)");
+    return set_error(DGTD_ERR_BAD_ARG, "debug_tc_gemm: need N <= 256 a multiple of 16 (of 8 at M = 64), "
+                                       "8 <= K <= 64 (K % 8 == 0)");
   CUDA_TRY(cudaSetDevice(ctx->device));
   DevBuf<float> da, db, dc;
   DevBuf<int> derr;

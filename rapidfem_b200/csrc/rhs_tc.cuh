@@ -1,12 +1,20 @@
 // rhs_tc.cuh -- fused DG Maxwell right-hand side with the element contractions
 // on the tcgen05 tensor cores (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulate
-// in TMEM).  Orders 1..4.
+// in TMEM).  Orders 1..5.
 //
-// One persistent CTA per SM walks tiles of E = 20 elements.  The MMA M
-// dimension is the 128 rows (element, component): lane quarter q holds elements
-// 5q..5q+4 in rows 32q + 6*(e%5) + c (rows 30, 31 of each quarter are padding),
-// so the six components of an element sit in one warp's TMEM lanes and the
-// curl can be combined with warp shuffles.
+// One persistent CTA per SM walks tiles of E elements.  The MMA M dimension is
+// the rows (element, component), split into four lane quarters of QR = M/4
+// rows; quarter q holds elements EQ q .. EQ q + EQ - 1 in rows
+// QR q + 6 (e % EQ) + c, so the six components of an element sit in one warp's
+// TMEM lanes and the curl can be combined with warp shuffles.
+//   orders 1-4: M = 128, EQ = 5 (E = 20; rows 30, 31 of a quarter are padding),
+//               two TMEM accumulator sets;
+//   order 5:    M = 64, EQ = 2 (E = 8; rows 12..15 of a quarter are padding),
+//               one accumulator set.  A 64-row MMA keeps row 16 q + r of its
+//               accumulator (and of a TMEM A operand) in lane 32 q + r, so a
+//               quarter's rows stay in its own TMEM sub-partition.  Order 5 at
+//               128 rows would need 608 TMEM columns for two accumulator sets and
+//               about 370 KB of shared memory for its operands and state slots.
 //
 //   volume:  C_v[(e,c)][(k,i)] = sum_j F[(e,c)][j] * D_k[i][j]        (rhs.rs:39-85)
 //   LIFT:    C_l[(e,c)][i]     = sum_s Flux[(e,c)][s] * LIFT[i][s]    (rhs.rs:1433-1439)
@@ -21,8 +29,9 @@
 //                   LSERK4 stage of explicit.rs:122-133 on y and p);
 //   control lane    issues the bulk async loads (state + element records three
 //                   tiles deep, residual register two deep), the MMAs of both
-//                   contractions into one of two TMEM accumulator sets, and the
-//                   bulk async stores.
+//                   contractions into one of the accumulator sets, and the bulk
+//                   async stores.  With one accumulator set the MMAs of tile t
+//                   wait for the epilogue of tile t-1 to have read it.
 // The LIFT operand is formed and multiplied in two halves (faces 0-1, 2-3),
 // each released by its own MMA completion, so the LIFT MMAs of one half run
 // while the flux warps form the other half (or the next tile's volume operand).
@@ -55,7 +64,7 @@
 
 namespace dgtd {
 
-constexpr int kTcTileE = 20;
+constexpr int kTcTileE = 20;  // elements per tile at orders 1-4 (8 at order 5)
 constexpr int kTcFluxWarps = 12;                          // warps 0..11
 constexpr int kTcEpiWarps = 12;                           // warps 12..23
 constexpr int kTcCtlWarp = kTcFluxWarps + kTcEpiWarps;    // warp 24, lane 0
@@ -70,23 +79,38 @@ __host__ __device__ constexpr int tc_r8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int tc_r16(int x) { return (x + 15) & ~15; }
 __host__ __device__ constexpr int tc_r128(int x) { return (x + 127) & ~127; }
 
+// Tile shape of an order: MMA rows, elements per lane quarter, accumulator sets
+// (the file header says why order 5 differs).
+__host__ __device__ constexpr int tc_m(int n) { return n == 5 ? 64 : 128; }
+__host__ __device__ constexpr int tc_eq(int n) { return n == 5 ? 2 : 5; }
+__host__ __device__ constexpr int tc_nacc(int n) { return n == 5 ? 1 : 2; }
+__host__ __device__ constexpr int tc_tile_e(int n) { return 4 * tc_eq(n); }
+// MMA N of the volume and LIFT B operands (a 128-row MMA takes N in steps of 16,
+// a 64-row one in steps of 8); the host lays out the constant operands with these.
+__host__ __device__ constexpr int tc_nv(int n) { return tc_m(n) == 64 ? tc_r8(3 * np_of(n)) : tc_r16(3 * np_of(n)); }
+__host__ __device__ constexpr int tc_nl(int n) { return tc_m(n) == 64 ? tc_r8(np_of(n)) : tc_r16(np_of(n)); }
+
 template <int N>
 struct TcCfg {
   static constexpr int NP = np_of(N), NFP = nfp_of(N), NF = 4 * NFP;
-  static constexpr int E = kTcTileE;
-  static constexpr int M = 128;
+  static constexpr int M = tc_m(N);
+  static constexpr int EQ = tc_eq(N);         // elements per lane quarter
+  static constexpr int E = 4 * EQ;            // elements per tile
+  static constexpr int QR = M / 4;            // MMA rows per lane quarter
+  static constexpr int RL = 6 * EQ;           // real rows (lanes) per quarter
+  static constexpr int NACC = tc_nacc(N);     // TMEM accumulator sets
   static constexpr int KV = tc_r8(NP);        // volume K (nodes)
-  static constexpr int NV = tc_r16(3 * NP);   // volume N ((k,i) pairs)
+  static constexpr int NV = tc_nv(N);         // volume N ((k,i) pairs)
   static constexpr int KLF = tc_r8(NFP);      // LIFT K per face
   static constexpr int KL = 4 * KLF;          // LIFT K (face nodes, per-face padded)
-  static constexpr int NL = tc_r16(NP);       // LIFT N (nodes)
+  static constexpr int NL = tc_nl(N);         // LIFT N (nodes)
   // The LIFT B operand stacks LIFT hi (rows 0..NL-1) over LIFT lo (rows NL..2NL-1),
   // so one MMA forms both products of an A half: N = 2 NL.
   static constexpr int NL2 = 2 * NL;
-  // TMEM columns: two accumulator sets [vol | lift hi | lift lo], then the volume
-  // A operand (hi, lo)
+  // TMEM columns: NACC accumulator sets [vol | lift hi | lift lo], then the
+  // volume A operand (hi, lo)
   static constexpr int ACC = NV + NL2;
-  static constexpr int T_AHI = 2 * ACC;
+  static constexpr int T_AHI = NACC * ACC;
   static constexpr int T_ALO = T_AHI + KV;
   static constexpr int TMEM_COLS = 512;
   static constexpr int TILE_F = E * 6 * NP;   // floats of state per tile
@@ -122,7 +146,14 @@ struct TcCfg {
   static_assert(SMEM <= 232448 - 1024, "shared memory per CTA (dynamic + static)");
   static_assert(T_ALO + KV <= TMEM_COLS, "TMEM columns");
   static_assert((TILE_B % 16) == 0 && (META_B % 16) == 0, "bulk copies need 16-byte sizes");
-  static_assert(NV <= 256 && NL2 <= 256 && (NV % 16) == 0 && (NL2 % 16) == 0, "MMA N limits");
+  static_assert(NV <= 256 && NL2 <= 256 && (NV % (M == 128 ? 16 : 8)) == 0 && (NL2 % (M == 128 ? 16 : 8)) == 0,
+                "MMA N limits");
+  static_assert((M == 128 || M == 64) && RL <= QR && (NACC == 1 || NACC == 2), "tile shape");
+  static_assert(NP <= NL && 3 * NP <= NV, "accumulator columns");
+  // flux slot packing: element (5 bits), face (2), face node (MB), state offset
+  static constexpr int MB = NFP <= 16 ? 4 : 5;
+  static constexpr int OFF_SHIFT = 7 + MB;
+  static_assert(E <= 32 && NFP <= (1 << MB) && TILE_F < (1 << (31 - OFF_SHIFT)), "flux slot packing");
   static_assert(ITEMS_H <= 2 && VCH_PER <= 4 && ECH_PER <= 8, "per-thread work tables");
   static_assert((KL % 16) == 0, "LIFT halves are whole k-steps");
 };
@@ -137,8 +168,11 @@ struct TcTables {
   int n_gather;
 };
 
-// Row of (element le, component c) in the 128-row MMA tile.
-__device__ __forceinline__ int tc_row(int le, int c) { return (le / 5) * 32 + (le % 5) * 6 + c; }
+// MMA row of (element le, component c) of a tile.
+template <class C>
+__device__ __forceinline__ int tc_row(int le, int c) {
+  return (le / C::EQ) * C::QR + (le % C::EQ) * 6 + c;
+}
 
 // Bounded waits.  A wait gives up after `limit` polls or once another role has
 // raised the abort flag; the warp form is warp-uniform.  A poll that finds the
@@ -278,15 +312,15 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   if (is_flux) {
     // ================= flux warps: volume operand -> TMEM, fluxes -> LIFT operand
     const int q4 = warp & 3, vg = warp >> 2;
-    const bool lane_real = lane < 30;
-    const int v_src = lane_real ? ((q4 * 5 + lane / 6) * 6 + lane % 6) * NP : 0;
+    const bool lane_real = lane < C::RL;
+    const int v_src = lane_real ? ((q4 * C::EQ + lane / 6) * 6 + lane % 6) * NP : 0;
     const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
     // flux slots q = (le, face, node-group, node-in-group) of each half (faces
     // 0-1, then 2-3).  What does not change from tile to tile is packed once:
     // f_item = le | f << 5 | m << 7 | (offset of the face node's state in the
-    // tile) << 11, -1 idle; f_off = byte offset of the slot's entry (component 0)
-    // in the LIFT operand.
-    static_assert(E <= 32 && NFP <= 16 && C::TILE_F < (1 << 20), "flux slot packing");
+    // tile) << (7 + MB), -1 idle; f_off = byte offset of the slot's entry
+    // (component 0) in the LIFT operand.
+    constexpr int kMMask = (1 << C::MB) - 1, kOffShift = C::OFF_SHIFT;
     int f_item[2][C::ITEMS_H];
     uint32_t f_off[2][C::ITEMS_H];
 #pragma unroll
@@ -301,9 +335,9 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           const int s4 = q & 3, le = (q >> 2) % E, rest = (q >> 2) / E;  // rest = f * (KLF/4) + mg
           const int f = rest / (KLF / 4), m = (rest % (KLF / 4)) * 4 + s4;
           if (m < NFP) {
-            f_item[hh][u] = le | (f << 5) | (m << 7) | ((le * 6 * NP + sFn[f * NFP + m]) << 11);
+            f_item[hh][u] = le | (f << 5) | (m << 7) | ((le * 6 * NP + sFn[f * NFP + m]) << kOffShift);
             const int sl = f * KLF + m;
-            f_off[hh][u] = (uint32_t)((sl >> 2) * (M / 8) * 128 + (sl & 3) * 4 + tc_row(le, 0) * 16);
+            f_off[hh][u] = (uint32_t)((sl >> 2) * (M / 8) * 128 + (sl & 3) * 4 + tc_row<C>(le, 0) * 16);
           }
         }
       }
@@ -323,7 +357,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
         zi[u] = -2;
         if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
         const int x = f_item[hh][u];
-        const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & 15;
+        const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & kMMask;
         const float* Me = sM + le * kMetaWords;
         const uint32_t codes = __float_as_uint(Me[41 + (f >> 1)]);
         const uint32_t code = (f & 1) ? (codes >> 16) : (codes & 0xffffu);
@@ -411,12 +445,12 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             const int u = v;
             if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
             const int x = f_item[hh][u];
-            const int le = x & 31, f = (x >> 5) & 3, m = (x >> 7) & 15;
+            const int le = x & 31, f = (x >> 5) & 3;
             const float* Me = sM + le * kMetaWords;
             const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
             const float coef = 0.5f * Me[21 + f];
             const int zi = zi_h[hh][u];
-            const float* Y = sY + (x >> 11);
+            const float* Y = sY + (x >> kOffShift);
             const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
             const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
             float jex, jey, jez, jhx, jhy, jhz;
@@ -481,8 +515,8 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   } else if (is_epi) {
     // ================= epilogue warps: TMEM -> dy -> mode update, in place
     const int q4 = warp & 3, eg = (warp - kTcFluxWarps) >> 2;
-    const bool lane_real = lane < 30;
-    const int e_le = q4 * 5 + (lane_real ? lane / 6 : 4);
+    const bool lane_real = lane < C::RL;
+    const int e_le = q4 * C::EQ + (lane_real ? lane / 6 : C::EQ - 1);
     const int e_c = lane_real ? lane % 6 : 5;
     const int e_fld = e_c / 3, e_t = e_c % 3;
     const int e_srcA = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
@@ -531,7 +565,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const bool src_here = (MODE == kModeLserk || MODE == kModeKrylov || MODE == kModeKcl) &&
                             (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
       const int64_t g_row = t0 + e_row_off;  // SoA index of node 0 of this row
-      const uint32_t acc = tmem + (uint32_t)(ps * C::ACC) + ((uint32_t)(q4 * 32) << 16);
+      const uint32_t acc = tmem + (uint32_t)((C::NACC == 2 ? ps : 0) * C::ACC) + ((uint32_t)(q4 * 32) << 16);
 #pragma unroll
       for (int cc = 0; cc < C::ECH_PER; ++cc) {
         const int ch = eg + kTcEpiGroups * cc;
@@ -651,10 +685,17 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     bool ok = true;
     for (int64_t it = 0; it < n_my && ok; ++it) {
       const int as = (int)(it & 1);
-      const uint32_t acc = tmem + (uint32_t)(as * C::ACC);
+      const uint32_t acc = tmem + (uint32_t)((C::NACC == 2 ? as : 0) * C::ACC);
       // volume MMAs: A = state hi/lo (TMEM), B = D hi/lo (shared)
       ok = tc_wait1(&bar_avol, (uint32_t)(it & 1), abort_flag);
       if (!ok) break;
+      if (C::NACC == 1 && it > 0) {
+        // one accumulator set: the epilogue of the previous tile must have read
+        // it; that tile's results then go out
+        ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
+        if (!ok) break;
+        store(it - 1);
+      }
       tc::tc_fence_after();
       DGTD_TC_MARK(6);
 #pragma unroll
@@ -667,12 +708,16 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       }
       tc::mma_commit(&bar_vdone);
       ++n_vd;
-      // Refills: the newest store group is tile it-2's (issued in the previous
-      // iteration); once it has read its slots, they take tile it+1's state
-      // (slot (it+1) % 3) and tile it's residual (slot it & 1).  Waiting after
-      // the volume MMAs are issued keeps the wait off the tensor pipe's path.
+      // Refills: once tile it-2's store group (issued in the previous iteration;
+      // with one accumulator set tile it-1's was issued after it) has read its
+      // slots, they take tile it+1's state (slot (it+1) % 3) and tile it's
+      // residual (slot it & 1).  Waiting after the volume MMAs are issued keeps
+      // the wait off the tensor pipe's path.
       if (it > 0) {
-        tc::bulk_wait_read0();
+        if (C::NACC == 1)
+          tc::bulk_wait_read1();
+        else
+          tc::bulk_wait_read0();
         DGTD_TC_MARK(7);
         if (it + 1 < n_my) load_y(it + 1);
         if (use_p) load_p(it);
@@ -703,7 +748,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       }
       if (!ok) break;
       // results of the previous tile -> HBM
-      if (it > 0) {
+      if (C::NACC == 2 && it > 0) {
         ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
         if (!ok) break;
         DGTD_TC_MARK(6);

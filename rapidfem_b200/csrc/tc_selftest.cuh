@@ -1,9 +1,12 @@
 // tc_selftest.cuh -- a one-CTA tcgen05 GEMM through the same operand layout,
 // descriptors, TMEM allocation and TMEM loads as the tensor-core RHS kernel:
-// C[128 x N] = A[128 x K] * B[N x K]^T, with the 3xTF32 split products
+// C[M x N] = A[M x K] * B[N x K]^T, with the 3xTF32 split products
 // (hi*hi + hi*lo + lo*hi) or a single tf32 product, and the A operand in shared
 // memory or in TMEM (written by tcgen05.st, one row per lane).  Test hook only.
-// flags: bit 0 = 3xTF32, bit 1 = A from TMEM.
+// flags: bit 0 = 3xTF32, bit 1 = A from TMEM, bit 2 = M = 64 (else 128).
+// The output is the raw TMEM lanes: C[lane][n] for all 128 lanes.  At M = 128
+// row r is lane r; at M = 64 row 16 q + r (r < 16) is lane 32 q + r, and the
+// TMEM A operand is written in that layout (lanes 16..31 of a quarter zero).
 #pragma once
 #include <cstdint>
 
@@ -18,7 +21,7 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
                                                      float* __restrict__ C, int N, int K, int flags,
                                                      int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tc_sm[];
-  const int M = 128;
+  const int M = (flags & 4) ? 64 : 128;
   float* a_hi = reinterpret_cast<float*>(tc_sm);
   float* a_lo = a_hi + M * K;
   float* b_hi = a_lo + M * K;
@@ -61,11 +64,13 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
   if (a_tmem) {
     // row tid of A -> TMEM lane tid (warp w owns lanes 32w..32w+31)
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const int row = M == 128 ? tid : warp * 16 + lane;
+    const bool real = M == 128 || lane < 16;
     for (int k0 = 0; k0 < K; k0 += 8) {
       float h[8], l[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        const float v = A[tid * K + k0 + q];
+        const float v = real ? A[row * K + k0 + q] : 0.f;
         h[q] = tc::to_tf32(v);
         l[q] = tc::to_tf32(v - h[q]);
       }

@@ -72,7 +72,7 @@ def morton_partition(mesh: Mesh, n_parts: int) -> np.ndarray:
     return part
 
 
-TILE = 20  # elements per tensor-core tile: stage ranges start on a tile
+TILE = 40  # a whole number of tensor-core tiles (20 elements, 8 at order 5): stage ranges start on one
 
 
 @dataclass
