@@ -100,9 +100,9 @@ typedef struct {
 } dgtd_op_desc;
 
 /* Contraction engine of the stage / RHS / Krylov-matvec kernels.  A new op
- * uses TF32X3 for orders 1-4 and FP32 for order 5.  The two FP32 engines
- * differ only in the elements per CTA tile (the same arithmetic, so the same
- * results to the bit); batch autotuning picks per order group.
+ * uses TF32X3 (every order).  The two FP32 engines differ only in the
+ * elements per CTA tile (the same arithmetic, so the same results to the
+ * bit); batch autotuning picks per order group.
  * (Split-BF16 products were measured at 1-3e-5 relative error per RHS at
  * N = 4, above the 1e-5 bar, and are not offered.) */
 typedef enum {
@@ -443,8 +443,10 @@ int dgtd_debug_expm(dgtd_ctx *ctx, const double *a, int32_t d, double *out);
 /* One-CTA tcgen05 GEMM C[M x n] = A[M x k] * B[n x k]^T (row-major f32)
  * through the operand layout, descriptors and TMEM path of the tensor-core RHS
  * kernel.  flags bit 0: 3xTF32 split products (else one tf32 product); bit 1:
- * A operand in TMEM (else shared memory); bit 2: M = 64 (else 128).  c gets
- * the 128 TMEM lanes x n: at M = 64 row 16 q + r (r < 16) is lane 32 q + r.
+ * A operand in TMEM (else shared memory); bit 2: M = 64 (else 128); bit 3
+ * (with bit 2): accumulator and TMEM A operand at lane offset o = 16 (else 0).
+ * c gets the 128 TMEM lanes x n: at M = 64 row 16 q + r (r < 16) is lane
+ * 32 q + o + r.
  * n <= 256 a multiple of 16 (of 8 at M = 64), 8 <= k <= 64 (k % 8 == 0). */
 int dgtd_debug_tc_gemm(dgtd_ctx *ctx, const float *a, const float *b, float *c, int32_t n, int32_t k,
                        int32_t flags);

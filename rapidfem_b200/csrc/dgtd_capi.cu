@@ -615,7 +615,7 @@ extern "C" int dgtd_op_create(dgtd_ctx* ctx, const dgtd_op_desc* d, dgtd_op** ou
   auto* op = new dgtd_op;
   op->ctx = ctx;
   op->device = ctx->device;
-  op->engine = N <= 4 ? DGTD_ENGINE_TF32X3 : DGTD_ENGINE_FP32;
+  op->engine = DGTD_ENGINE_TF32X3;
   op->order = N;
   op->np = np;
   op->nfp = nfp;
@@ -1641,7 +1641,6 @@ int kcl_run(dgtd_op* op, float dt, int64_t steps, int drive, int64_t src_dof, co
   c.log = op->kcl_log.p;
   KclCtl* dc = op->kcl_ctl.p;
   CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
-  const int* d_skip = &dc->skip;
   const float* sv = drive == DGTD_DRIVE_VECTOR ? op->src_vec.p : nullptr;
   float* y = op->y[op->cur].p;
   auto attempt = [&]() -> int {

@@ -8,12 +8,16 @@
 // QR q + 6 (e % EQ) + c, so the six components of an element sit in one warp's
 // TMEM lanes and the curl can be combined with warp shuffles.
 //   orders 1-4: M = 128, EQ = 5 (E = 20; rows 30, 31 of a quarter are padding),
-//               two TMEM accumulator sets;
-//   order 5:    M = 64, EQ = 2 (E = 8; rows 12..15 of a quarter are padding),
-//               one accumulator set.  A 64-row MMA keeps row 16 q + r of its
-//               accumulator (and of a TMEM A operand) in lane 32 q + r, so a
-//               quarter's rows stay in its own TMEM sub-partition.  Order 5 at
-//               128 rows would need 608 TMEM columns for two accumulator sets and
+//               two TMEM accumulator sets side by side in the columns;
+//   order 5:    M = 64, EQ = 2 (E = 8; rows 12..15 of a quarter are padding).
+//               A 64-row MMA keeps row 16 q + r of its accumulator (and of a
+//               TMEM A operand, which must sit at the accumulator's lane offset)
+//               in lane 32 q + o + r, o = 0 or 16, so a quarter's rows stay in
+//               its own TMEM sub-partition and the two accumulator sets (each
+//               with its own volume A operand) take the two lane halves of the
+//               same columns; TMEM is read and written with the 16-lane shapes,
+//               a warp's two thread halves on two column ranges.  Order 5 at 128
+//               rows would need 608 TMEM columns for two accumulator sets and
 //               about 370 KB of shared memory for its operands and state slots.
 //
 //   volume:  C_v[(e,c)][(k,i)] = sum_j F[(e,c)][j] * D_k[i][j]        (rhs.rs:39-85)
@@ -29,9 +33,8 @@
 //                   LSERK4 stage of explicit.rs:122-133 on y and p);
 //   control lane    issues the bulk async loads (state + element records three
 //                   tiles deep, residual register two deep), the MMAs of both
-//                   contractions into one of the accumulator sets, and the bulk
-//                   async stores.  With one accumulator set the MMAs of tile t
-//                   wait for the epilogue of tile t-1 to have read it.
+//                   contractions into one of two TMEM accumulator sets, and the
+//                   bulk async stores.
 // The LIFT operand is formed and multiplied in two halves (faces 0-1, 2-3),
 // each released by its own MMA completion, so the LIFT MMAs of one half run
 // while the flux warps form the other half (or the next tile's volume operand).
@@ -83,7 +86,6 @@ __host__ __device__ constexpr int tc_r128(int x) { return (x + 127) & ~127; }
 // (the file header says why order 5 differs).
 __host__ __device__ constexpr int tc_m(int n) { return n == 5 ? 64 : 128; }
 __host__ __device__ constexpr int tc_eq(int n) { return n == 5 ? 2 : 5; }
-__host__ __device__ constexpr int tc_nacc(int n) { return n == 5 ? 1 : 2; }
 __host__ __device__ constexpr int tc_tile_e(int n) { return 4 * tc_eq(n); }
 // MMA N of the volume and LIFT B operands (a 128-row MMA takes N in steps of 16,
 // a 64-row one in steps of 8); the host lays out the constant operands with these.
@@ -98,7 +100,9 @@ struct TcCfg {
   static constexpr int E = 4 * EQ;            // elements per tile
   static constexpr int QR = M / 4;            // MMA rows per lane quarter
   static constexpr int RL = 6 * EQ;           // real rows (lanes) per quarter
-  static constexpr int NACC = tc_nacc(N);     // TMEM accumulator sets
+  // the two accumulator sets: side by side in the columns (M = 128), or in the
+  // lane halves of the same columns (M = 64), each with its own A operand
+  static constexpr bool LANE_SETS = M == 64;
   static constexpr int KV = tc_r8(NP);        // volume K (nodes)
   static constexpr int NV = tc_nv(N);         // volume N ((k,i) pairs)
   static constexpr int KLF = tc_r8(NFP);      // LIFT K per face
@@ -107,11 +111,13 @@ struct TcCfg {
   // The LIFT B operand stacks LIFT hi (rows 0..NL-1) over LIFT lo (rows NL..2NL-1),
   // so one MMA forms both products of an A half: N = 2 NL.
   static constexpr int NL2 = 2 * NL;
-  // TMEM columns: NACC accumulator sets [vol | lift hi | lift lo], then the
-  // volume A operand (hi, lo)
+  // TMEM columns: the accumulator sets [vol | lift hi | lift lo], then the
+  // volume A operand (hi, lo; at M = 64 each padded to whole 16-column pairs of
+  // the 16-lane stores)
   static constexpr int ACC = NV + NL2;
-  static constexpr int T_AHI = NACC * ACC;
-  static constexpr int T_ALO = T_AHI + KV;
+  static constexpr int KVP = LANE_SETS ? tc_r16(KV) : KV;
+  static constexpr int T_AHI = LANE_SETS ? ACC : 2 * ACC;
+  static constexpr int T_ALO = T_AHI + KVP;
   static constexpr int TMEM_COLS = 512;
   static constexpr int TILE_F = E * 6 * NP;   // floats of state per tile
   static constexpr int TILE_B = TILE_F * 4;
@@ -125,6 +131,9 @@ struct TcCfg {
   static constexpr int VCH_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
   static constexpr int ECH = (NP + 3) / 4;                                     // epilogue node chunks of 4
   static constexpr int ECH_PER = (ECH + kTcEpiGroups - 1) / kTcEpiGroups;
+  // M = 64: a 16-lane TMEM access serves two chunks (one per thread half)
+  static constexpr int VPAIRS = (VCH + 1) / 2, VPAIR_PER = (VPAIRS + kTcVolGroups - 1) / kTcVolGroups;
+  static constexpr int EPAIRS = (ECH + 1) / 2, EPAIR_PER = (EPAIRS + kTcEpiGroups - 1) / kTcEpiGroups;
   // byte sizes of the shared-memory operands (hi or lo)
   static constexpr int BV_B = NV * KV * 4;
   static constexpr int BL_B = NL2 * KL * 4;   // stacked hi/lo
@@ -144,11 +153,11 @@ struct TcCfg {
   static constexpr int TAB_B = 4 * NFP + kMaxGather * NFP;
   static constexpr int SMEM = O_TAB + tc_r128(TAB_B);
   static_assert(SMEM <= 232448 - 1024, "shared memory per CTA (dynamic + static)");
-  static_assert(T_ALO + KV <= TMEM_COLS, "TMEM columns");
+  static_assert(T_ALO + KVP <= TMEM_COLS, "TMEM columns");
   static_assert((TILE_B % 16) == 0 && (META_B % 16) == 0, "bulk copies need 16-byte sizes");
   static_assert(NV <= 256 && NL2 <= 256 && (NV % (M == 128 ? 16 : 8)) == 0 && (NL2 % (M == 128 ? 16 : 8)) == 0,
                 "MMA N limits");
-  static_assert((M == 128 || M == 64) && RL <= QR && (NACC == 1 || NACC == 2), "tile shape");
+  static_assert((M == 128 || M == 64) && RL <= QR && (!LANE_SETS || (RL <= 16 && ECH % 2 == 0)), "tile shape");
   static_assert(NP <= NL && 3 * NP <= NV, "accumulator columns");
   // flux slot packing: element (5 bits), face (2), face node (MB), state offset
   static constexpr int MB = NFP <= 16 ? 4 : 5;
@@ -167,6 +176,12 @@ struct TcTables {
   const uint8_t* gtab;
   int n_gather;
 };
+
+// TMEM address offset of accumulator set s (and, at M = 64, of its A operand).
+template <class C>
+__device__ __forceinline__ uint32_t tc_set_off(int s) {
+  return C::LANE_SETS ? ((uint32_t)(16 * s) << 16) : (uint32_t)(s * C::ACC);
+}
 
 // MMA row of (element le, component c) of a tile.
 template <class C>
@@ -312,8 +327,11 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   if (is_flux) {
     // ================= flux warps: volume operand -> TMEM, fluxes -> LIFT operand
     const int q4 = warp & 3, vg = warp >> 2;
-    const bool lane_real = lane < C::RL;
-    const int v_src = lane_real ? ((q4 * C::EQ + lane / 6) * 6 + lane % 6) * NP : 0;
+    // the TMEM row this lane writes: its own lane, or (16-lane stores at M = 64)
+    // lane & 15 of the set's lane half, the thread half choosing the chunk
+    const int v_row = C::LANE_SETS ? (lane & 15) : lane;
+    const bool lane_real = v_row < C::RL;
+    const int v_src = lane_real ? ((q4 * C::EQ + v_row / 6) * 6 + v_row % 6) * NP : 0;
     const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
     // flux slots q = (le, face, node-group, node-in-group) of each half (faces
     // 0-1, then 2-3).  What does not change from tile to tile is packed once:
@@ -399,21 +417,44 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       tc::tc_fence_after();
       DGTD_TC_MARK(0);
       // ---- volume operand: row (e,c) of this lane, K = nodes, tf32 hi/lo -> TMEM
+      if constexpr (C::LANE_SETS) {
+        // chunk pair pr: this thread half's chunk 2 pr + (lane >> 4), in the
+        // lane half of the tile's accumulator set
+        const uint32_t a_taddr = v_taddr + tc_set_off<C>((int)(it & 1));
 #pragma unroll
-      for (int cc = 0; cc < C::VCH_PER; ++cc) {
-        const int ch = vg + kTcVolGroups * cc;
-        if (ch < C::VCH) {
-          float h[8], l[8];
+        for (int cc = 0; cc < C::VPAIR_PER; ++cc) {
+          const int pr = vg + kTcVolGroups * cc;
+          if (pr < C::VPAIRS) {
+            const int ch = 2 * pr + (lane >> 4);
+            float h[8], l[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int k = ch * 8 + q;
-            const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
-            // hi/lo split as for the LIFT operand (flux section below)
-            h[q] = tc::tf32_round(v);
-            l[q] = v - h[q];
+            for (int q = 0; q < 8; ++q) {
+              const int k = ch * 8 + q;
+              const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+              h[q] = tc::tf32_round(v);
+              l[q] = v - h[q];
+            }
+            tc::tmem_st16x2_8(a_taddr + (uint32_t)(C::T_AHI + pr * 16), h);
+            tc::tmem_st16x2_8(a_taddr + (uint32_t)(C::T_ALO + pr * 16), l);
           }
-          tc::tmem_st8(v_taddr + (uint32_t)(C::T_AHI + ch * 8), h);
-          tc::tmem_st8(v_taddr + (uint32_t)(C::T_ALO + ch * 8), l);
+        }
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < C::VCH_PER; ++cc) {
+          const int ch = vg + kTcVolGroups * cc;
+          if (ch < C::VCH) {
+            float h[8], l[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int k = ch * 8 + q;
+              const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+              // hi/lo split as for the LIFT operand (flux section below)
+              h[q] = tc::tf32_round(v);
+              l[q] = v - h[q];
+            }
+            tc::tmem_st8(v_taddr + (uint32_t)(C::T_AHI + ch * 8), h);
+            tc::tmem_st8(v_taddr + (uint32_t)(C::T_ALO + ch * 8), l);
+          }
         }
       }
       tc::tmem_st_wait();
@@ -515,12 +556,15 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
   } else if (is_epi) {
     // ================= epilogue warps: TMEM -> dy -> mode update, in place
     const int q4 = warp & 3, eg = (warp - kTcFluxWarps) >> 2;
-    const bool lane_real = lane < C::RL;
-    const int e_le = q4 * C::EQ + (lane_real ? lane / 6 : C::EQ - 1);
-    const int e_c = lane_real ? lane % 6 : 5;
+    // the TMEM row of this lane: its own lane, or (16-lane loads at M = 64)
+    // lane & 15, the thread half (hb = 0 | 16) reading the second chunk of a pair
+    const int e_row = C::LANE_SETS ? (lane & 15) : lane, hb = C::LANE_SETS ? (lane & 16) : 0;
+    const bool lane_real = e_row < C::RL;
+    const int e_le = q4 * C::EQ + (lane_real ? e_row / 6 : C::EQ - 1);
+    const int e_c = lane_real ? e_row % 6 : 5;
     const int e_fld = e_c / 3, e_t = e_c % 3;
-    const int e_srcA = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
-    const int e_srcB = lane_real ? (lane / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
+    const int e_srcA = lane_real ? hb + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
+    const int e_srcB = lane_real ? hb + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
     const float e_sign = e_fld == 0 ? 1.f : -1.f;
     const int e_cA = (e_t + 2) % 3, e_cB = (e_t + 1) % 3;
     const int e_row_off = (e_le * 6 + e_c) * NP;
@@ -565,18 +609,30 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       const bool src_here = (MODE == kModeLserk || MODE == kModeKrylov || MODE == kModeKcl) &&
                             (P.src_vec != nullptr || (P.src_idx >= t0 && P.src_idx < t0 + C::TILE_F));
       const int64_t g_row = t0 + e_row_off;  // SoA index of node 0 of this row
-      const uint32_t acc = tmem + (uint32_t)((C::NACC == 2 ? ps : 0) * C::ACC) + ((uint32_t)(q4 * 32) << 16);
+      const uint32_t acc = tmem + tc_set_off<C>(ps) + ((uint32_t)(q4 * 32) << 16);
+      // node chunks of 4 (M = 128), or pairs of them, one per thread half (M = 64)
+      constexpr int kIters = C::LANE_SETS ? C::EPAIR_PER : C::ECH_PER;
+      constexpr int kUnits = C::LANE_SETS ? C::EPAIRS : C::ECH;
 #pragma unroll
-      for (int cc = 0; cc < C::ECH_PER; ++cc) {
+      for (int cc = 0; cc < kIters; ++cc) {
         const int ch = eg + kTcEpiGroups * cc;
-        if (ch < C::ECH) {
-          const int i0 = ch * 4;
+        if (ch < kUnits) {
+          const int c0 = C::LANE_SETS ? ch * 8 : ch * 4;  // first column of the access
+          const int i0 = c0 + (hb >> 2);                  // this thread's first node
           float r0[4], r1[4], r2[4], lf[4], lg[4];
-          tc::tmem_ldw<4>(acc + (uint32_t)i0, r0);
-          tc::tmem_ldw<4>(acc + (uint32_t)(NP + i0), r1);
-          tc::tmem_ldw<4>(acc + (uint32_t)(2 * NP + i0), r2);
-          tc::tmem_ldw<4>(acc + (uint32_t)(NV + i0), lf);
-          tc::tmem_ldw<4>(acc + (uint32_t)(NV + NL + i0), lg);
+          if constexpr (C::LANE_SETS) {
+            tc::tmem_ld16x2_4(acc + (uint32_t)c0, r0);
+            tc::tmem_ld16x2_4(acc + (uint32_t)(NP + c0), r1);
+            tc::tmem_ld16x2_4(acc + (uint32_t)(2 * NP + c0), r2);
+            tc::tmem_ld16x2_4(acc + (uint32_t)(NV + c0), lf);
+            tc::tmem_ld16x2_4(acc + (uint32_t)(NV + NL + c0), lg);
+          } else {
+            tc::tmem_ldw<4>(acc + (uint32_t)i0, r0);
+            tc::tmem_ldw<4>(acc + (uint32_t)(NP + i0), r1);
+            tc::tmem_ldw<4>(acc + (uint32_t)(2 * NP + i0), r2);
+            tc::tmem_ldw<4>(acc + (uint32_t)(NV + i0), lf);
+            tc::tmem_ldw<4>(acc + (uint32_t)(NV + NL + i0), lg);
+          }
           tc::tmem_ld_wait();
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
@@ -685,22 +741,17 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     bool ok = true;
     for (int64_t it = 0; it < n_my && ok; ++it) {
       const int as = (int)(it & 1);
-      const uint32_t acc = tmem + (uint32_t)((C::NACC == 2 ? as : 0) * C::ACC);
+      const uint32_t acc = tmem + tc_set_off<C>(as);
+      // the volume A operand: one for both sets (M = 128) or the set's own (M = 64)
+      const uint32_t a_base = tmem + (C::LANE_SETS ? tc_set_off<C>(as) : 0u);
       // volume MMAs: A = state hi/lo (TMEM), B = D hi/lo (shared)
       ok = tc_wait1(&bar_avol, (uint32_t)(it & 1), abort_flag);
       if (!ok) break;
-      if (C::NACC == 1 && it > 0) {
-        // one accumulator set: the epilogue of the previous tile must have read
-        // it; that tile's results then go out
-        ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
-        if (!ok) break;
-        store(it - 1);
-      }
       tc::tc_fence_after();
       DGTD_TC_MARK(6);
 #pragma unroll
       for (int ks = 0; ks < KV / 8; ++ks) {
-        const uint32_t a_h = tmem + (uint32_t)(C::T_AHI + 8 * ks), a_l = tmem + (uint32_t)(C::T_ALO + 8 * ks);
+        const uint32_t a_h = a_base + (uint32_t)(C::T_AHI + 8 * ks), a_l = a_base + (uint32_t)(C::T_ALO + 8 * ks);
         const uint64_t bh = dvh + (uint64_t)(2 * NV * ks), bo = dvl + (uint64_t)(2 * NV * ks);
         tc::mma_tf32_ta(acc, a_h, bh, idv, ks > 0 ? 1u : 0u);
         tc::mma_tf32_ta(acc, a_h, bo, idv, 1u);
@@ -708,16 +759,12 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       }
       tc::mma_commit(&bar_vdone);
       ++n_vd;
-      // Refills: once tile it-2's store group (issued in the previous iteration;
-      // with one accumulator set tile it-1's was issued after it) has read its
-      // slots, they take tile it+1's state (slot (it+1) % 3) and tile it's
-      // residual (slot it & 1).  Waiting after the volume MMAs are issued keeps
-      // the wait off the tensor pipe's path.
+      // Refills: the newest store group is tile it-2's (issued in the previous
+      // iteration); once it has read its slots, they take tile it+1's state
+      // (slot (it+1) % 3) and tile it's residual (slot it & 1).  Waiting after
+      // the volume MMAs are issued keeps the wait off the tensor pipe's path.
       if (it > 0) {
-        if (C::NACC == 1)
-          tc::bulk_wait_read1();
-        else
-          tc::bulk_wait_read0();
+        tc::bulk_wait_read0();
         DGTD_TC_MARK(7);
         if (it + 1 < n_my) load_y(it + 1);
         if (use_p) load_p(it);
@@ -748,7 +795,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       }
       if (!ok) break;
       // results of the previous tile -> HBM
-      if (C::NACC == 2 && it > 0) {
+      if (it > 0) {
         ok = tc_wait1(&bar_epi[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1), abort_flag);
         if (!ok) break;
         DGTD_TC_MARK(6);

@@ -3,10 +3,12 @@
 // C[M x N] = A[M x K] * B[N x K]^T, with the 3xTF32 split products
 // (hi*hi + hi*lo + lo*hi) or a single tf32 product, and the A operand in shared
 // memory or in TMEM (written by tcgen05.st, one row per lane).  Test hook only.
-// flags: bit 0 = 3xTF32, bit 1 = A from TMEM, bit 2 = M = 64 (else 128).
+// flags: bit 0 = 3xTF32, bit 1 = A from TMEM, bit 2 = M = 64 (else 128),
+// bit 3 (with bit 2) = accumulator and TMEM A operand at lane offset 16.
 // The output is the raw TMEM lanes: C[lane][n] for all 128 lanes.  At M = 128
-// row r is lane r; at M = 64 row 16 q + r (r < 16) is lane 32 q + r, and the
-// TMEM A operand is written in that layout (lanes 16..31 of a quarter zero).
+// row r is lane r; at M = 64 row 16 q + r (r < 16) is lane 32 q + o + r, o the
+// lane offset (0 or 16), and the TMEM A operand is written in that layout (the
+// other 16 lanes of a quarter zero).
 #pragma once
 #include <cstdint>
 
@@ -64,8 +66,8 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
   if (a_tmem) {
     // row tid of A -> TMEM lane tid (warp w owns lanes 32w..32w+31)
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-    const int row = M == 128 ? tid : warp * 16 + lane;
-    const bool real = M == 128 || lane < 16;
+    const int row = M == 128 ? tid : warp * 16 + (lane & 15);
+    const bool real = M == 128 || (lane >> 4) == ((flags >> 3) & 1);
     for (int k0 = 0; k0 < K; k0 += 8) {
       float h[8], l[8];
 #pragma unroll
@@ -82,15 +84,17 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
     __syncthreads();
     tc::tc_fence_after();
   }
+  // lane offset of the accumulator (and of a TMEM A operand): 16 only at M = 64
+  const uint32_t d_tm = tmem + ((M == 64 && (flags & 8)) ? (16u << 16) : 0u);
   if (tid == 0 && a_tmem) {
     const uint32_t id = tc::idesc_tf32(M, N);
     const uint32_t bh = tc::smem_u32(b_hi), bl = tc::smem_u32(b_lo);
     for (int ks = 0; ks < K / 8; ++ks) {
-      const uint32_t ah = tmem + (uint32_t)(a_hi_col + 8 * ks), al = tmem + (uint32_t)(a_lo_col + 8 * ks);
-      tc::mma_tf32_ta(tmem, ah, tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
+      const uint32_t ah = d_tm + (uint32_t)(a_hi_col + 8 * ks), al = d_tm + (uint32_t)(a_lo_col + 8 * ks);
+      tc::mma_tf32_ta(d_tm, ah, tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
       if (split3) {
-        tc::mma_tf32_ta(tmem, ah, tc::tf32_step_desc(bl, N, ks), id, 1u);
-        tc::mma_tf32_ta(tmem, al, tc::tf32_step_desc(bh, N, ks), id, 1u);
+        tc::mma_tf32_ta(d_tm, ah, tc::tf32_step_desc(bl, N, ks), id, 1u);
+        tc::mma_tf32_ta(d_tm, al, tc::tf32_step_desc(bh, N, ks), id, 1u);
       }
     }
     tc::mma_commit(&s_bar);
@@ -99,10 +103,10 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float* __restrict__ A
     const uint32_t ah = tc::smem_u32(a_hi), al = tc::smem_u32(a_lo);
     const uint32_t bh = tc::smem_u32(b_hi), bl = tc::smem_u32(b_lo);
     for (int ks = 0; ks < K / 8; ++ks) {
-      tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
+      tc::mma_tf32(d_tm, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bh, N, ks), id, ks > 0 ? 1u : 0u);
       if (split3) {
-        tc::mma_tf32(tmem, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, N, ks), id, 1u);
-        tc::mma_tf32(tmem, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, N, ks), id, 1u);
+        tc::mma_tf32(d_tm, tc::tf32_step_desc(ah, M, ks), tc::tf32_step_desc(bl, N, ks), id, 1u);
+        tc::mma_tf32(d_tm, tc::tf32_step_desc(al, M, ks), tc::tf32_step_desc(bh, N, ks), id, 1u);
       }
     }
     tc::mma_commit(&s_bar);
