@@ -227,7 +227,7 @@ def test_bad_arguments_raise(ctx):
 
 
 @pytest.mark.parametrize("engine", [0, 1])
-@pytest.mark.parametrize("order", [1, 2, 3, 4])
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
 def test_single_cell_mesh_one_padded_tile(ctx, order, engine):
     # 6 tets: fewer elements than one tile of either kernel, so most of the tile
     # is inert padding; every face of the cube is a PEC boundary face
