@@ -112,12 +112,10 @@ struct TcCfg {
   // so one MMA forms both products of an A half: N = 2 NL.
   static constexpr int NL2 = 2 * NL;
   // TMEM columns: the accumulator sets [vol | lift hi | lift lo], then the
-  // volume A operand (hi, lo; at M = 64 each padded to whole 16-column pairs of
-  // the 16-lane stores)
+  // volume A operand (hi, lo)
   static constexpr int ACC = NV + NL2;
-  static constexpr int KVP = LANE_SETS ? tc_r16(KV) : KV;
   static constexpr int T_AHI = LANE_SETS ? ACC : 2 * ACC;
-  static constexpr int T_ALO = T_AHI + KVP;
+  static constexpr int T_ALO = T_AHI + KV;
   static constexpr int TMEM_COLS = 512;
   static constexpr int TILE_F = E * 6 * NP;   // floats of state per tile
   static constexpr int TILE_B = TILE_F * 4;
@@ -131,8 +129,10 @@ struct TcCfg {
   static constexpr int VCH_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
   static constexpr int ECH = (NP + 3) / 4;                                     // epilogue node chunks of 4
   static constexpr int ECH_PER = (ECH + kTcEpiGroups - 1) / kTcEpiGroups;
-  // M = 64: a 16-lane TMEM access serves two chunks (one per thread half)
-  static constexpr int VPAIRS = (VCH + 1) / 2, VPAIR_PER = (VPAIRS + kTcVolGroups - 1) / kTcVolGroups;
+  // M = 64: a 16-lane TMEM access serves two chunks of 4 columns (one per
+  // thread half): the volume operand's K in VCH units of 8, the accumulator's
+  // nodes in EPAIRS units of 8
+  static constexpr int VU_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
   static constexpr int EPAIRS = (ECH + 1) / 2, EPAIR_PER = (EPAIRS + kTcEpiGroups - 1) / kTcEpiGroups;
   // byte sizes of the shared-memory operands (hi or lo)
   static constexpr int BV_B = NV * KV * 4;
@@ -153,11 +153,12 @@ struct TcCfg {
   static constexpr int TAB_B = 4 * NFP + kMaxGather * NFP;
   static constexpr int SMEM = O_TAB + tc_r128(TAB_B);
   static_assert(SMEM <= 232448 - 1024, "shared memory per CTA (dynamic + static)");
-  static_assert(T_ALO + KVP <= TMEM_COLS, "TMEM columns");
+  static_assert(T_ALO + KV <= TMEM_COLS, "TMEM columns");
   static_assert((TILE_B % 16) == 0 && (META_B % 16) == 0, "bulk copies need 16-byte sizes");
   static_assert(NV <= 256 && NL2 <= 256 && (NV % (M == 128 ? 16 : 8)) == 0 && (NL2 % (M == 128 ? 16 : 8)) == 0,
                 "MMA N limits");
-  static_assert((M == 128 || M == 64) && RL <= QR && (!LANE_SETS || (RL <= 16 && ECH % 2 == 0)), "tile shape");
+  // at M = 64 quarter q's rows start at offset q (see tc_row)
+  static_assert((M == 128 || M == 64) && RL <= QR && (!LANE_SETS || (3 + RL <= 16 && ECH % 2 == 0)), "tile shape");
   static_assert(NP <= NL && 3 * NP <= NV, "accumulator columns");
   // flux slot packing: element (5 bits), face (2), face node (MB), state offset
   static constexpr int MB = NFP <= 16 ? 4 : 5;
@@ -183,10 +184,31 @@ __device__ __forceinline__ uint32_t tc_set_off(int s) {
   return C::LANE_SETS ? ((uint32_t)(16 * s) << 16) : (uint32_t)(s * C::ACC);
 }
 
+// Row offset of lane quarter q's elements.  At M = 64 the flux warps store the
+// LIFT operand of eight elements at once; starting quarter q's rows at q spreads
+// their rows over more 16-byte bank groups (row mod 8) than a common start.
+template <class C>
+__device__ __forceinline__ int tc_qoff(int q) {
+  return C::LANE_SETS ? q : 0;
+}
+
 // MMA row of (element le, component c) of a tile.
 template <class C>
 __device__ __forceinline__ int tc_row(int le, int c) {
-  return (le / C::EQ) * C::QR + (le % C::EQ) * 6 + c;
+  return (le / C::EQ) * C::QR + tc_qoff<C>(le / C::EQ) + (le % C::EQ) * 6 + c;
+}
+
+// Rotation of a row's node order at M = 64.  The element rows of a state tile
+// are Np = 56 floats apart, so the twelve (element j, component c) rows a warp
+// touches fall into four bank groups of three ((16 j + 24 c) mod 32); the
+// three rows of a group start their four nodes at 0, 1 and 2.
+__device__ __forceinline__ int tc_node_rot(int j, int c) { return j == 0 ? (c >= 4 ? 1 : 0) : (c >= 2 ? 2 : 1); }
+
+// a[(v + k) & 3] for a compile-time v and a runtime k in 0..3, without
+// indexing the register array at run time.
+__device__ __forceinline__ float tc_pick4(const float (&a)[4], int v, int k) {
+  const float x0 = a[v & 3], x1 = a[(v + 1) & 3], x2 = a[(v + 2) & 3], x3 = a[(v + 3) & 3];
+  return k == 0 ? x0 : k == 1 ? x1 : k == 2 ? x2 : x3;
 }
 
 // Bounded waits.  A wait gives up after `limit` polls or once another role has
@@ -328,10 +350,12 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     // ================= flux warps: volume operand -> TMEM, fluxes -> LIFT operand
     const int q4 = warp & 3, vg = warp >> 2;
     // the TMEM row this lane writes: its own lane, or (16-lane stores at M = 64)
-    // lane & 15 of the set's lane half, the thread half choosing the chunk
-    const int v_row = C::LANE_SETS ? (lane & 15) : lane;
-    const bool lane_real = v_row < C::RL;
+    // lane & 15 of the set's lane half, the thread half choosing the columns;
+    // v_row = 6 (element in quarter) + component
+    const int v_row = (C::LANE_SETS ? (lane & 15) : lane) - tc_qoff<C>(q4);
+    const bool lane_real = v_row >= 0 && v_row < C::RL;
     const int v_src = lane_real ? ((q4 * C::EQ + v_row / 6) * 6 + v_row % 6) * NP : 0;
+    const int v_rot = (C::LANE_SETS && lane_real) ? tc_node_rot(v_row / 6, v_row % 6) : 0;
     const uint32_t v_taddr = tmem + ((uint32_t)(q4 * 32) << 16);
     // flux slots q = (le, face, node-group, node-in-group) of each half (faces
     // 0-1, then 2-3).  What does not change from tile to tile is packed once:
@@ -418,24 +442,29 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       DGTD_TC_MARK(0);
       // ---- volume operand: row (e,c) of this lane, K = nodes, tf32 hi/lo -> TMEM
       if constexpr (C::LANE_SETS) {
-        // chunk pair pr: this thread half's chunk 2 pr + (lane >> 4), in the
-        // lane half of the tile's accumulator set
+        // 8-column unit w: this thread half's 4 columns 8 w + 4 (lane >> 4) ..,
+        // in the lane half of the tile's accumulator set; the four nodes are
+        // read from node v_rot on (no bank replays) and put back in order
         const uint32_t a_taddr = v_taddr + tc_set_off<C>((int)(it & 1));
 #pragma unroll
-        for (int cc = 0; cc < C::VPAIR_PER; ++cc) {
-          const int pr = vg + kTcVolGroups * cc;
-          if (pr < C::VPAIRS) {
-            const int ch = 2 * pr + (lane >> 4);
-            float h[8], l[8];
+        for (int cc = 0; cc < C::VU_PER; ++cc) {
+          const int w = vg + kTcVolGroups * cc;
+          if (w < C::VCH) {
+            const int n0 = 8 * w + 4 * (lane >> 4);
+            float v4[4], h[4], l[4];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int k = ch * 8 + q;
-              const float v = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+            for (int q = 0; q < 4; ++q) {
+              const int k = n0 + ((q + v_rot) & 3);
+              v4[q] = (lane_real && k < NP) ? sY[v_src + k] : 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float v = tc_pick4(v4, q, (4 - v_rot) & 3);  // node n0 + q
               h[q] = tc::tf32_round(v);
               l[q] = v - h[q];
             }
-            tc::tmem_st16x2_8(a_taddr + (uint32_t)(C::T_AHI + pr * 16), h);
-            tc::tmem_st16x2_8(a_taddr + (uint32_t)(C::T_ALO + pr * 16), l);
+            tc::tmem_st16x2_4(a_taddr + (uint32_t)(C::T_AHI + w * 8), h);
+            tc::tmem_st16x2_4(a_taddr + (uint32_t)(C::T_ALO + w * 8), l);
           }
         }
       } else {
@@ -557,14 +586,17 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
     // ================= epilogue warps: TMEM -> dy -> mode update, in place
     const int q4 = warp & 3, eg = (warp - kTcFluxWarps) >> 2;
     // the TMEM row of this lane: its own lane, or (16-lane loads at M = 64)
-    // lane & 15, the thread half (hb = 0 | 16) reading the second chunk of a pair
-    const int e_row = C::LANE_SETS ? (lane & 15) : lane, hb = C::LANE_SETS ? (lane & 16) : 0;
-    const bool lane_real = e_row < C::RL;
+    // lane & 15, the thread half (hb = 0 | 16) reading the second chunk of a
+    // pair; e_row = 6 (element in quarter) + component
+    const int qo = tc_qoff<C>(q4), hb = C::LANE_SETS ? (lane & 16) : 0;
+    const int e_row = (C::LANE_SETS ? (lane & 15) : lane) - qo;
+    const bool lane_real = e_row >= 0 && e_row < C::RL;
     const int e_le = q4 * C::EQ + (lane_real ? e_row / 6 : C::EQ - 1);
     const int e_c = lane_real ? e_row % 6 : 5;
     const int e_fld = e_c / 3, e_t = e_c % 3;
-    const int e_srcA = lane_real ? hb + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
-    const int e_srcB = lane_real ? hb + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
+    const int e_srcA = lane_real ? hb + qo + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 2) % 3 : lane;
+    const int e_srcB = lane_real ? hb + qo + (e_row / 6) * 6 + 3 * (1 - e_fld) + (e_t + 1) % 3 : lane;
+    const int e_rot = (C::LANE_SETS && lane_real) ? tc_node_rot(e_row / 6, e_c) : 0;
     const float e_sign = e_fld == 0 ? 1.f : -1.f;
     const int e_cA = (e_t + 2) % 3, e_cB = (e_t + 1) % 3;
     const int e_row_off = (e_le * 6 + e_c) * NP;
@@ -634,54 +666,79 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
             tc::tmem_ldw<4>(acc + (uint32_t)(NV + NL + i0), lg);
           }
           tc::tmem_ld_wait();
+          // the mode's update of node i of this row from its dy (yv: y at node i)
+          const auto update = [&](int i, float dy, float yv) {
+            if (MODE == kModeLserk) {
+              // LSERK4 stage (explicit.rs:122-133): p = a p + dt (dy + src); y += b p
+              float k = dy;
+              if (src_here) {
+                if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g_row + i), k);
+                if (P.src_idx == g_row + i) k += P.src_g;
+              }
+              float pv = dt_e * k;
+              if (P.read_p) pv = fmaf(P.a, prow[i], pv);
+              prow[i] = pv;
+              yrow[i] = fmaf(P.b, pv, yv);
+            } else if (MODE == kModeKcl) {
+              // KCL stage (explicit_adaptive.rs:84-152) straight to global
+              // memory, in the operation order of the separate stage kernel
+              // (kcl.cuh k_kcl_stage); nothing is staged for the bulk store
+              const int64_t g = g_row + i;
+              float kk = dy;
+              if (src_here) {
+                if (P.src_vec != nullptr) kk += __ldg(P.src_vec + g) * kcl_gs;
+                if (P.src_idx == g) kk += kcl_gs;
+              }
+              const float f = kcl_h * kk;
+              const float yn = P.kcl_y[g] + P.kcl_b * f;
+              P.kcl_y[g] = yn;
+              P.kcl_e[g] = P.kcl_stage == 0 ? P.kcl_ew * f : P.kcl_e[g] + P.kcl_ew * f;
+              if (P.kcl_next != nullptr) P.kcl_next[g] = yn + P.kcl_amb * f;
+            } else if (MODE == kModeKrylov) {
+              // Krylov matvec of a stored basis vector: its scale and the
+              // augmented source coefficient from device memory
+              float w = kry_sig * dy;
+              if (src_here) {
+                if (P.src_vec != nullptr) w = fmaf(kry_g, __ldg(P.src_vec + g_row + i), w);
+                if (P.src_idx == g_row + i) w += kry_g;
+              }
+              prow[i] = w;
+            } else {
+              prow[i] = dy;
+            }
+          };
+          if constexpr (C::LANE_SETS) {
+            // curl and LIFT sums node by node (the shuffles pair one node), then
+            // the row's four nodes from node e_rot on (no bank replays on the
+            // state and residual tiles); same arithmetic as below
+            float sc[4], sl[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            // my contributions: A to curl component (t+1)%3, B to (t+2)%3
-            const float A = fmaf(gA2, r2[u], fmaf(gA1, r1[u], gA0 * r0[u]));
-            const float B = fmaf(gB2, r2[u], fmaf(gB1, r1[u], gB0 * r0[u]));
-            const float pa = __shfl_sync(0xffffffffu, A, e_srcA);
-            const float pb = __shfl_sync(0xffffffffu, B, e_srcB);
-            const int i = i0 + u;
-            if (lane_real && i < NP) {
-              const float yv = yrow[i];
-              const float dy = fmaf(w_curl, pa + pb, fmaf(inv_w, lf[u] + lg[u], -sig_w * yv));
-              if (MODE == kModeLserk) {
-                // LSERK4 stage (explicit.rs:122-133): p = a p + dt (dy + src); y += b p
-                float k = dy;
-                if (src_here) {
-                  if (P.src_vec != nullptr) k = fmaf(P.src_g, __ldg(P.src_vec + g_row + i), k);
-                  if (P.src_idx == g_row + i) k += P.src_g;
-                }
-                float pv = dt_e * k;
-                if (P.read_p) pv = fmaf(P.a, prow[i], pv);
-                prow[i] = pv;
-                yrow[i] = fmaf(P.b, pv, yv);
-              } else if (MODE == kModeKcl) {
-                // KCL stage (explicit_adaptive.rs:84-152) straight to global
-                // memory, in the operation order of the separate stage kernel
-                // (kcl.cuh k_kcl_stage); nothing is staged for the bulk store
-                const int64_t g = g_row + i;
-                float kk = dy;
-                if (src_here) {
-                  if (P.src_vec != nullptr) kk += __ldg(P.src_vec + g) * kcl_gs;
-                  if (P.src_idx == g) kk += kcl_gs;
-                }
-                const float f = kcl_h * kk;
-                const float yn = P.kcl_y[g] + P.kcl_b * f;
-                P.kcl_y[g] = yn;
-                P.kcl_e[g] = P.kcl_stage == 0 ? P.kcl_ew * f : P.kcl_e[g] + P.kcl_ew * f;
-                if (P.kcl_next != nullptr) P.kcl_next[g] = yn + P.kcl_amb * f;
-              } else if (MODE == kModeKrylov) {
-                // Krylov matvec of a stored basis vector: its scale and the
-                // augmented source coefficient from device memory
-                float w = kry_sig * dy;
-                if (src_here) {
-                  if (P.src_vec != nullptr) w = fmaf(kry_g, __ldg(P.src_vec + g_row + i), w);
-                  if (P.src_idx == g_row + i) w += kry_g;
-                }
-                prow[i] = w;
-              } else {
-                prow[i] = dy;
+            for (int u = 0; u < 4; ++u) {
+              const float A = fmaf(gA2, r2[u], fmaf(gA1, r1[u], gA0 * r0[u]));
+              const float B = fmaf(gB2, r2[u], fmaf(gB1, r1[u], gB0 * r0[u]));
+              sc[u] = __shfl_sync(0xffffffffu, A, e_srcA) + __shfl_sync(0xffffffffu, B, e_srcB);
+              sl[u] = lf[u] + lg[u];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              const int i = i0 + ((v + e_rot) & 3);
+              if (lane_real && i < NP) {
+                const float yv = yrow[i];
+                update(i, fmaf(w_curl, tc_pick4(sc, v, e_rot), fmaf(inv_w, tc_pick4(sl, v, e_rot), -sig_w * yv)), yv);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              // my contributions: A to curl component (t+1)%3, B to (t+2)%3
+              const float A = fmaf(gA2, r2[u], fmaf(gA1, r1[u], gA0 * r0[u]));
+              const float B = fmaf(gB2, r2[u], fmaf(gB1, r1[u], gB0 * r0[u]));
+              const float pa = __shfl_sync(0xffffffffu, A, e_srcA);
+              const float pb = __shfl_sync(0xffffffffu, B, e_srcB);
+              const int i = i0 + u;
+              if (lane_real && i < NP) {
+                const float yv = yrow[i];
+                update(i, fmaf(w_curl, pa + pb, fmaf(inv_w, lf[u] + lg[u], -sig_w * yv)), yv);
               }
             }
           }
