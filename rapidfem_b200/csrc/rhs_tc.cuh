@@ -82,8 +82,8 @@ __host__ __device__ constexpr int tc_r8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int tc_r16(int x) { return (x + 15) & ~15; }
 __host__ __device__ constexpr int tc_r128(int x) { return (x + 127) & ~127; }
 
-// Tile shape of an order: MMA rows, elements per lane quarter, accumulator sets
-// (the file header says why order 5 differs).
+// Tile shape of an order: MMA rows and elements per lane quarter (the file
+// header says why order 5 differs).
 __host__ __device__ constexpr int tc_m(int n) { return n == 5 ? 64 : 128; }
 __host__ __device__ constexpr int tc_eq(int n) { return n == 5 ? 2 : 5; }
 __host__ __device__ constexpr int tc_tile_e(int n) { return 4 * tc_eq(n); }
@@ -132,7 +132,6 @@ struct TcCfg {
   // M = 64: a 16-lane TMEM access serves two chunks of 4 columns (one per
   // thread half): the volume operand's K in VCH units of 8, the accumulator's
   // nodes in EPAIRS units of 8
-  static constexpr int VU_PER = (VCH + kTcVolGroups - 1) / kTcVolGroups;
   static constexpr int EPAIRS = (ECH + 1) / 2, EPAIR_PER = (EPAIRS + kTcEpiGroups - 1) / kTcEpiGroups;
   // byte sizes of the shared-memory operands (hi or lo)
   static constexpr int BV_B = NV * KV * 4;
@@ -447,7 +446,7 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
         // read from node v_rot on (no bank replays) and put back in order
         const uint32_t a_taddr = v_taddr + tc_set_off<C>((int)(it & 1));
 #pragma unroll
-        for (int cc = 0; cc < C::VU_PER; ++cc) {
+        for (int cc = 0; cc < C::VCH_PER; ++cc) {
           const int w = vg + kTcVolGroups * cc;
           if (w < C::VCH) {
             const int n0 = 8 * w + 4 * (lane >> 4);
