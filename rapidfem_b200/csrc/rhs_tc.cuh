@@ -495,6 +495,77 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
       // that half are done; its own MMAs then run while the next half is formed.
       // half 1's traces: before the wait for half 0's operand to be free
       nb_fetch(sM, e0, 1, nb_h[1], zi_h[1]);
+      // the numerical flux of slot u of half hh (false: an idle slot)
+      const auto flux_of = [&](int hh, int u, float (&fl)[6]) -> bool {
+        if (u >= C::ITEMS_H || f_item[hh][u] < 0) return false;
+        const int x = f_item[hh][u];
+        const int le = x & 31, f = (x >> 5) & 3;
+        const float* Me = sM + le * kMetaWords;
+        const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
+        const float coef = 0.5f * Me[21 + f];
+        const int zi = zi_h[hh][u];
+        const float* Y = sY + (x >> kOffShift);
+        const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
+        const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
+        float jex, jey, jez, jhx, jhy, jhz;
+        float a = P.alpha;
+        if (zi == -3) {
+          // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
+          jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
+          a = 1.0f;
+        } else if (zi == -2) {
+          // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
+          const float edn = nx * ex + ny * ey + nz * ez;
+          const float hdn = nx * hx + ny * hy + nz * hz;
+          jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
+          jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
+        } else {
+          const float (&nb)[6] = nb_h[hh][u];
+          float px = nb[0], py = nb[1], pz = nb[2];
+          float qx = nb[3], qy = nb[4], qz = nb[5];
+          if (zi >= 0) {
+            const float* Z = sY + zi;
+            px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
+            qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
+          }
+          jex = ex - px; jey = ey - py; jez = ez - pz;
+          jhx = hx - qx; jhy = hy - qy; jhz = hz - qz;
+        }
+        // fe = coef (-n x [H] + a n x (n x [E])), fh = coef (n x [E] + a n x (n x [H]))
+        // (rhs.rs:1420-1432), with n x (n x v) = n (n.v) - v for the unit normal.
+        const float ca = coef * a;
+        const float de = ca * (nx * jex + ny * jey + nz * jez);
+        const float dh = ca * (nx * jhx + ny * jhy + nz * jhz);
+        fl[0] = fmaf(de, nx, fmaf(-ca, jex, -coef * (ny * jhz - nz * jhy)));
+        fl[1] = fmaf(de, ny, fmaf(-ca, jey, -coef * (nz * jhx - nx * jhz)));
+        fl[2] = fmaf(de, nz, fmaf(-ca, jez, -coef * (nx * jhy - ny * jhx)));
+        fl[3] = fmaf(dh, nx, fmaf(-ca, jhx, coef * (ny * jez - nz * jey)));
+        fl[4] = fmaf(dh, ny, fmaf(-ca, jhy, coef * (nz * jex - nx * jez)));
+        fl[5] = fmaf(dh, nz, fmaf(-ca, jhz, coef * (nx * jey - ny * jex)));
+        return true;
+      };
+      // ... into the LIFT operand: hi = tf32(fl), lo = fl - hi (exact,
+      // |lo| <= 2^-11 |fl|).  lo is stored unrounded: the tf32 MMA reads only
+      // its top 19 bits, an error below 2^-10 |lo| <= 2^-21 |fl|, under the
+      // 3xTF32 products' own 2^-22-class terms in the sum of many products.
+      const auto store_of = [&](int hh, int u, const float (&fl)[6]) {
+        const uint32_t off = f_off[hh][u];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const float h = tc::tf32_round(fl[c]);
+          *reinterpret_cast<float*>(alh + off + c * 16) = h;
+          *reinterpret_cast<float*>(all + off + c * 16) = fl[c] - h;
+        }
+      };
+      // At M = 64 (one slot per thread and half) both halves' fluxes are formed
+      // before the waits for their operand halves to be free: two independent
+      // chains per thread, and no flux arithmetic behind an MMA completion.
+      float fe[2][6];
+      bool fe_on[2] = {false, false};
+      if constexpr (C::LANE_SETS) {
+        fe_on[0] = flux_of(0, 0, fe[0]);
+        fe_on[1] = flux_of(1, 0, fe[1]);
+      }
       bool half_ok = true;
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
@@ -507,67 +578,13 @@ rhs_tc_kernel(RhsParams P, TcTables T, int64_t n_tiles, int* err) {
           }
         }
         DGTD_TC_MARK(2);
-        {
-          const float (&nb)[2][6] = nb_h[hh];
+        if constexpr (C::LANE_SETS) {
+          if (fe_on[hh]) store_of(hh, 0, fe[hh]);
+        } else {
 #pragma unroll
-          for (int v = 0; v < 2; ++v) {
-            const int u = v;
-            if (u >= C::ITEMS_H || f_item[hh][u] < 0) continue;
-            const int x = f_item[hh][u];
-            const int le = x & 31, f = (x >> 5) & 3;
-            const float* Me = sM + le * kMetaWords;
-            const float nx = Me[9 + 3 * f], ny = Me[10 + 3 * f], nz = Me[11 + 3 * f];
-            const float coef = 0.5f * Me[21 + f];
-            const int zi = zi_h[hh][u];
-            const float* Y = sY + (x >> kOffShift);
-            const float ex = Y[0 * NP], ey = Y[1 * NP], ez = Y[2 * NP];
-            const float hx = Y[3 * NP], hy = Y[4 * NP], hz = Y[5 * NP];
-            float jex, jey, jez, jhx, jhy, jhz;
-            float a = P.alpha;
-            if (zi == -3) {
-              // characteristic boundary against a zero incident field (rhs.rs:1380-1386)
-              jex = ex; jey = ey; jez = ez; jhx = hx; jhy = hy; jhz = hz;
-              a = 1.0f;
-            } else if (zi == -2) {
-              // PEC ghost: [E] = 2 E_tan, [H] = 2 H_n (rhs.rs:1387-1402)
-              const float edn = nx * ex + ny * ey + nz * ez;
-              const float hdn = nx * hx + ny * hy + nz * hz;
-              jex = 2.0f * (ex - edn * nx); jey = 2.0f * (ey - edn * ny); jez = 2.0f * (ez - edn * nz);
-              jhx = 2.0f * (hdn * nx); jhy = 2.0f * (hdn * ny); jhz = 2.0f * (hdn * nz);
-            } else {
-              float px = nb[v][0], py = nb[v][1], pz = nb[v][2];
-              float qx = nb[v][3], qy = nb[v][4], qz = nb[v][5];
-              if (zi >= 0) {
-                const float* Z = sY + zi;
-                px = Z[0 * NP]; py = Z[1 * NP]; pz = Z[2 * NP];
-                qx = Z[3 * NP]; qy = Z[4 * NP]; qz = Z[5 * NP];
-              }
-              jex = ex - px; jey = ey - py; jez = ez - pz;
-              jhx = hx - qx; jhy = hy - qy; jhz = hz - qz;
-            }
-            // fe = coef (-n x [H] + a n x (n x [E])), fh = coef (n x [E] + a n x (n x [H]))
-            // (rhs.rs:1420-1432), with n x (n x v) = n (n.v) - v for the unit normal.
-            const float ca = coef * a;
-            const float de = ca * (nx * jex + ny * jey + nz * jez);
-            const float dh = ca * (nx * jhx + ny * jhy + nz * jhz);
+          for (int u = 0; u < 2; ++u) {
             float fl[6];
-            fl[0] = fmaf(de, nx, fmaf(-ca, jex, -coef * (ny * jhz - nz * jhy)));
-            fl[1] = fmaf(de, ny, fmaf(-ca, jey, -coef * (nz * jhx - nx * jhz)));
-            fl[2] = fmaf(de, nz, fmaf(-ca, jez, -coef * (nx * jhy - ny * jhx)));
-            fl[3] = fmaf(dh, nx, fmaf(-ca, jhx, coef * (ny * jez - nz * jey)));
-            fl[4] = fmaf(dh, ny, fmaf(-ca, jhy, coef * (nz * jex - nx * jez)));
-            fl[5] = fmaf(dh, nz, fmaf(-ca, jhz, coef * (nx * jey - ny * jex)));
-            const uint32_t off = f_off[hh][u];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) {
-              // hi = tf32(fl), lo = fl - hi (exact, |lo| <= 2^-11 |fl|).  lo is
-              // stored unrounded: the tf32 MMA reads only its top 19 bits, an
-              // error below 2^-10 |lo| <= 2^-21 |fl|, under the 3xTF32
-              // products' own 2^-22-class terms in the sum of many products.
-              const float h = tc::tf32_round(fl[c]);
-              *reinterpret_cast<float*>(alh + off + c * 16) = h;
-              *reinterpret_cast<float*>(all + off + c * 16) = fl[c] - h;
-            }
+            if (flux_of(hh, u, fl)) store_of(hh, u, fl);
           }
         }
         tc::fence_proxy_async_smem();
