@@ -1,14 +1,14 @@
 """Batched instances on the device: every instance of an autotuned, graph-
-captured batch ends where its own solo run with its own dt ends (the same to
-the bit on the FP32 engine, to f32 rounding on the tensor-core engine), and
-graph replays equal direct launches."""
+captured batch ends where its own solo run with its own dt on the engine the
+autotuner chose ends (the same to the bit on both FP32 engines, to f32
+rounding on the tensor-core engine), and graph replays equal direct launches."""
 import numpy as np
 import pytest
 
 from rapidfem_b200 import batch as B
 from rapidfem_b200 import gpu as G
 from rapidfem_b200 import operator as O
-from rapidfem_b200._native import ENGINE_FP32
+from rapidfem_b200._native import ENGINE_FP32, ENGINE_FP32_SMALL_TILES, ENGINE_TF32X3
 
 from .conftest import rel_l2
 
@@ -42,11 +42,13 @@ def test_batch_matches_solo_runs(ctx):
             solo = G.GpuOperator(ctx, O.MaxwellOperator(O.structured_box(inst[i].cells, inst[i].cells,
                                                                          inst[i].cells), g.order, 1.0,
                                                         materials=inst[i].materials))
-            solo.set_engine(ENGINE_FP32 if t["engine"] == "fp32" else 1)
+            engine = {"fp32": ENGINE_FP32, "fp32_small_tiles": ENGINE_FP32_SMALL_TILES,
+                      "tf32x3": ENGINE_TF32X3}[t["engine"]]
+            solo.set_engine(engine)
             solo.upload(g.y0[g.dof_slice(j)])
             solo.run_lserk(np.float32(inst[i].dt), 4)
             want = solo.download()
-            if t["engine"] == "fp32":
+            if engine != ENGINE_TF32X3:
                 assert np.array_equal(got[i], want)
             else:
                 assert rel_l2(got[i], want) < 1e-6
