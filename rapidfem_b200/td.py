@@ -24,6 +24,7 @@ from . import operator as O
 C_LIGHT = 299_792_458.0
 RESONANCE_STATIC_FRACTION = 1e-3  # constants.rs:305: modes below this share of max |Im| are static
 RESONANCE_MERGE_REL = 1e-3        # constants.rs:308: resonances this close (relative) are one
+TRANSFER_BAND_FRACTION = 1e-2     # constants.rs:313: H is zero where |G| is below this share of its peak
 KRYLOV_TOL = 1e-10
 _CTX = {}
 
@@ -72,6 +73,28 @@ def _sample(waveform, t):
     except Exception:
         pass
     return np.array([float(waveform(float(x))) for x in np.ravel(t)])
+
+
+def transfer(g, r, dt):
+    """The frequency response of a drive series g and a response series r of
+    equal length sampled every dt (session.rs:1238-1261): the one-sided
+    spectra of both (forward real FFT, length n // 2 + 1), frequencies
+    k / (n dt), and H = R / G where |G| exceeds TRANSFER_BAND_FRACTION of its
+    peak, zero elsewhere."""
+    g = np.asarray(g, dtype=np.float64).ravel()
+    r = np.asarray(r, dtype=np.float64).ravel()
+    if g.size != r.size:
+        raise ValueError("drive and response lengths differ")
+    n = g.size
+    if n == 0:
+        return np.zeros(0), np.zeros(0, dtype=np.complex128)
+    sg, sr = np.fft.rfft(g), np.fft.rfft(r)
+    peak = float(np.max(np.abs(sg)))
+    freqs = np.arange(sg.size) / (n * dt)
+    band = np.abs(sg) > TRANSFER_BAND_FRACTION * peak
+    h = np.zeros(sg.size, dtype=np.complex128)
+    h[band] = sr[band] / sg[band]
+    return freqs, h
 
 
 def _distance2_colors(nbr: np.ndarray) -> np.ndarray:
@@ -309,6 +332,18 @@ class TdSession:
             out[q] = rows[:, idx] @ w
         return out
 
+    def transfer_function(self, source_dof, probe_dof, pulse, dt, steps, method=None, device="gpu",
+                          krylov_dim=40, verbose=True):
+        """(frequencies, H) of the field at probe_dof driven by the soft point
+        source `pulse` at source_dof (td.rs:331-350, session.rs:985-999): one
+        driven transient of `steps` frames from rest recording the probe, the
+        drive sampled at the frame times k dt, k = 0..steps, then `transfer`."""
+        frames, _ = self.transient(None, dt=dt, steps=steps, source_dof=source_dof, waveform=pulse,
+                                   probes=[probe_dof], method=method, device=device, krylov_dim=krylov_dim,
+                                   verbose=verbose)
+        g = _sample(pulse, np.arange(steps + 1) * float(dt))
+        return transfer(g, frames[:, 0], float(dt))
+
     # ---- runs
     def transient(self, y0=None, *, dt, steps, source_dof=None, port=None, waveform=None, probes=None,
                   port_probes=None, method=None, device="gpu", krylov_dim=40, warmup=0, verbose=True):
@@ -414,6 +449,30 @@ class TdSession:
                 rows.extend(list(traj[1:].astype(np.float64)))
                 y = traj[-1].astype(np.float64)
         return np.array(rows), None
+
+
+class TdTransfer:
+    """A field-to-field frequency response (problem/td.py:140-167): iterates
+    as (frequencies, H); the labels name the source and probe points."""
+
+    def __init__(self, frequencies, H, *, source_label="", probe_label=""):
+        self.frequencies = np.asarray(frequencies)
+        self.H = np.asarray(H)
+        self.source_label = source_label
+        self.probe_label = probe_label
+
+    def __iter__(self):
+        return iter((self.frequencies, self.H))
+
+    def __repr__(self):
+        return f"TdTransfer(n_freq={self.frequencies.size})"
+
+
+def _point_label(spec):
+    """'E_z @ (x, y, z)' for a (point, field, component) spec (problem/td.py:101-106)."""
+    p, f, c = spec
+    coords = ", ".join(f"{v:g}" for v in np.asarray(p, dtype=float).ravel())
+    return f"{f}_{c} @ ({coords})"
 
 
 class TdTrajectory(np.ndarray):
@@ -562,6 +621,18 @@ class ProblemTD:
                                        probes=pr, device=device, method=method, krylov_dim=int(krylov_dim),
                                        verbose=verbose)
         return np.arange(steps + 1) * dt, frames.T
+
+    def transfer_function(self, *, source, probe, pulse, dt, steps, krylov_dim=40, device="gpu", verbose=True):
+        """Field-to-field frequency response H(f) = R(f) / G(f) from one run
+        driven by the broadband `pulse` at `source` and recorded at `probe`,
+        both (point, field, component) (problem/td.py:549-598).  A TdTransfer:
+        the steps + 1 frames give frequencies k / ((steps + 1) dt),
+        k = 0 .. (steps + 1) // 2, and H is zero outside the pulse's band."""
+        freqs, h = self._op.transfer_function(
+            self.probe_dof(source[0], field=source[1], component=source[2]),
+            self.probe_dof(probe[0], field=probe[1], component=probe[2]), pulse,
+            dt=float(dt), steps=int(steps), device=device, krylov_dim=int(krylov_dim), verbose=verbose)
+        return TdTransfer(freqs, h, source_label=_point_label(source), probe_label=_point_label(probe))
 
     def transient(self, y0=None, *, dt, steps, source=None, waveform=None, port=None, krylov_dim=40,
                   method="exponential", warmup=0, device="gpu", verbose=True, port_probes=None):

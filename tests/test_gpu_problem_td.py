@@ -146,3 +146,38 @@ def test_driven_transient_from_a_model_port():
     assert rows.shape == (1, 21) and np.abs(rows).max() > 0.0
     with pytest.raises(ValueError, match="not a port"):
         p.transient(port=99, waveform=pulse, dt=3e-12, steps=1, verbose=False)
+
+
+def test_transfer_function_matches_the_oracle():
+    """ProblemTD.transfer_function (problem/td.py:549-598, session.rs:985-999):
+    the probe series of the driven run it makes equals the reference's LSERK4
+    run on the oracle with the source held per step, and H is the transfer of
+    that series with the pulse sampled at the frame times."""
+    from rapidfem_b200 import td as TD
+
+    p, orc, _ = _problem()
+    dt = 0.5 * p.cfl_dt()  # one LSERK4 step per frame
+    steps = 200
+    pulse = GaussianPulse(t0=1.0, tau=0.25, f0=0.8)
+    source, probe = ((0.3, 0.5, 0.5), "E", "z"), ((0.7, 0.5, 0.5), "E", "z")
+    tf = p.transfer_function(source=source, probe=probe, pulse=pulse, dt=dt, steps=steps, verbose=False)
+    assert isinstance(tf, TD.TdTransfer) and tf.source_label == "E_z @ (0.3, 0.5, 0.5)"
+    f, h = tf
+    assert f.shape == h.shape == ((steps + 1) // 2 + 1,)
+    t, series = p.driven_transient(source=source, waveform=pulse, probes=[probe], dt=dt, steps=steps, verbose=False)
+    f_ref, h_ref = TD.transfer(pulse(t), series[0], dt)
+    assert np.array_equal(f, f_ref) and np.array_equal(h, h_ref)
+    src = p.probe_dof(source[0], field="E", component="z")
+    pr = p.probe_dof(probe[0], field="E", component="z")
+    g32 = np.asarray(pulse(t), dtype=np.float32).astype(np.float64)
+    y = np.zeros(p.n_dofs)
+    want = [0.0]
+    for k in range(steps):
+        y = orc.lserk(y, dt, 1, src_dof=src, vals=g32[k:k + 1])
+        want.append(y[pr])
+    want = np.array(want)
+    assert rel_l2(series[0], want) < 1e-4
+    _, h_orc = TD.transfer(pulse(t), want, dt)
+    band = h_orc != 0
+    assert band.sum() > 5 and np.all(h[~band] == 0)
+    assert np.linalg.norm(h[band] - h_orc[band]) < 1e-3 * np.linalg.norm(h_orc[band])
