@@ -145,14 +145,7 @@ __device__ __forceinline__ void tmem_st16x2_4(uint32_t taddr, const float (&v)[4
                "r"(__float_as_uint(v[3]))
                : "memory");
 }
-__device__ __forceinline__ void tmem_st16x2_8(uint32_t taddr, const float (&v)[8]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.16x32bx2.x8.b32 [%0], 8, {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
-      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-      : "memory");
-}
+
 
 // Store 8 consecutive 32-bit TMEM columns of this thread's lane.
 __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
