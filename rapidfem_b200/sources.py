@@ -14,8 +14,6 @@
 """
 from __future__ import annotations
 
-import math
-
 import numpy as np
 
 LSERK_A = (0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
@@ -72,7 +70,3 @@ def step_polynomial(g, t: float, h: float, n_coef: int = 8):
     err = float(np.max(np.abs(np.polyval(cs[::-1], sm) - g(t + h * sm))))
     return coef, err
 
-
-def midpoint_gaussian_width(sigma_t: float) -> float:
-    """tau of exp(-((t-t0)/tau)^2) equal to exp(-(t-t0)^2/(2 sigma^2))."""
-    return sigma_t * math.sqrt(2.0)
