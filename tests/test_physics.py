@@ -1,7 +1,9 @@
-"""The reference's operator physics tests (rhs.rs:1995-2030 conductivity
-damping, :2366-2445 a port face drains energy, :2447-2520 the port operator
-only dissipates) on the f64 oracle; tests/test_gpu_physics.py runs them on
-the device path."""
+"""The reference's operator physics tests on the f64 oracle (whose host
+arrays the product's host build matches bit for bit): element curl exactness,
+dielectric and absorber spectra, energy conservation, the soft source,
+conductivity damping (rhs.rs:1995-2030), port dissipation (:2366-2520) and the
+waveguide port (:2522-2735); tests/test_gpu_physics.py runs the operator-level
+ones on the device path."""
 import numpy as np
 
 from oracle import oracle as R
@@ -219,3 +221,80 @@ def test_anisotropic_central_flux_conserves_energy():
     mesh, mat = anisotropic_box()
     orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, materials=mat)
     assert skew_defect(dense(orc.apply, orc.n_dof), energy_mass(orc)) < 1e-12
+
+
+# ---- element curl, dielectric and absorber physics, soft source (rhs.rs:1778-2110, :2223-2260)
+SHEARED_TET = np.array([[0.3, -0.2, 0.1], [1.4, 0.1, -0.2], [0.2, 1.3, 0.4], [-0.1, 0.2, 1.6]])
+ONE_TET = np.array([[0, 1, 2, 3]], dtype=np.int32)
+
+
+def test_curl_of_polynomial_field_is_exact():
+    """rhs.rs:1778-1813: on a sheared element the discrete curl of
+    F = (y z, 2 z x, 3 x y) is curl F = (x, -2 y, z) at the nodes (N = 2; the
+    field is in every higher order's space too, so N = 3..5 as well)."""
+    for order in (2, 3, 4, 5):
+        orc = R.Operator(SHEARED_TET, ONE_TET, order)
+        p = orc.node_coords()
+        field = np.stack([p[:, 1] * p[:, 2], 2.0 * p[:, 2] * p[:, 0], 3.0 * p[:, 0] * p[:, 1]], axis=1)
+        curl = R.curl_single(order, orc.get("jinv"), field).reshape(-1, 3)
+        want = np.stack([p[:, 0], -2.0 * p[:, 1], p[:, 2]], axis=1)
+        assert np.max(np.abs(curl - want)) < 1e-9, order
+
+
+def test_curl_of_constant_field_vanishes():
+    """rhs.rs:1815-1828: a constant field has zero curl (N = 3, and N = 5)."""
+    ref = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    for order in (3, 5):
+        orc = R.Operator(ref, ONE_TET, order)
+        curl = R.curl_single(order, orc.get("jinv"), np.full(3 * orc.np, 0.7))
+        assert np.max(np.abs(curl)) < 1e-10
+
+
+def test_uniform_dielectric_shifts_cavity_resonance():
+    """rhs.rs:1870-1898: filling the unit cube with eps_r = 4 scales the
+    fundamental to pi sqrt 2 / sqrt(eps_r) within 2 % (2^3 mesh, N = 2, upwind)."""
+    mesh = O.structured_box(2, 2, 2)
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 1.0, materials=O.isotropic_materials(np.full(mesh.n_tets, 4.0)))
+    ev = np.linalg.eigvals(dense(orc.apply, orc.n_dof))
+    ev = ev[np.abs(ev.imag) > 0.5]
+    im = float(abs(ev[np.argmax(ev.real)].imag))
+    assert abs(im - WANT_FUNDAMENTAL / 2.0) / (WANT_FUNDAMENTAL / 2.0) < 0.02
+
+
+def test_heterogeneous_central_flux_conserves_energy():
+    """rhs.rs:1899-1943: isotropic eps = 1 + 0.7 i, mu = 1 + 0.3 i by element
+    (unit cube, N = 2, central flux): M~A is skew to 1e-9 of its largest entry."""
+    mesh = O.structured_box(1, 1, 1)
+    i = np.arange(mesh.n_tets)
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 0.0, materials=O.isotropic_materials(1.0 + 0.7 * i, 1.0 + 0.3 * i))
+    ma = energy_mass(orc) @ dense(orc.apply, orc.n_dof)
+    assert np.max(np.abs(ma + ma.T)) < 1e-9 * max(np.max(np.abs(ma)), 1.0)
+
+
+def test_matched_absorber_damps_at_the_full_rate():
+    """rhs.rs:2075-2110: an impedance-matched loss (sigma / eps = sigma* / mu =
+    nu = 0.15) shifts the least-damped mode's real part by -nu within 8 %,
+    twice an electric-only loss (unit cube, N = 2, upwind)."""
+    mesh = O.structured_box(1, 1, 1)
+    ones = np.ones(mesh.n_tets)
+    res = []
+    for mat in (O.isotropic_materials(ones), O.isotropic_materials(ones, ones, 0.15 * ones, 0.15 * ones)):
+        orc = R.Operator(mesh.nodes, mesh.tets, 2, 1.0, materials=mat)
+        res.append(least_damped_re(dense(orc.apply, orc.n_dof)))
+    assert abs((res[1] - res[0]) + 0.15) / 0.15 < 0.08
+
+
+def test_soft_source_injects_energy():
+    """rhs.rs:2223-2260: a Gaussian pulse (t0 = 0.3, tau = 0.08) at the E_z DOF of
+    the unit cube's centre node, 80 ETD steps of 0.01 (m = 30) from rest,
+    leaves finite fields with energy > 1e-6."""
+    mesh = O.structured_box(1, 1, 1)
+    orc = R.Operator(mesh.nodes, mesh.tets, 2, 1.0)
+    sdof = O.MaxwellOperator(mesh, 2, 1.0).nearest_node_dof([0.5, 0.5, 0.5], 0, 2)
+    y = np.zeros(orc.n_dof)
+    for k in range(80):
+        b = np.zeros(orc.n_dof)
+        b[sdof] = np.exp(-(((k * 0.01) - 0.3) / 0.08) ** 2)
+        y, _ = orc.etd_step(y, b, 0.01, 30)
+    assert np.all(np.isfinite(y))
+    assert float(y @ energy_mass(orc) @ y) > 1e-6
