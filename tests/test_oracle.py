@@ -199,3 +199,46 @@ def test_expm_identities():
     a = np.array([[0.0, 1.0], [-1.0, 0.0]]) * 3.0
     e = R.expm(a)
     assert np.allclose(e, [[np.cos(3), np.sin(3)], [-np.sin(3), np.cos(3)]], atol=1e-13)
+
+
+def test_lserk4_is_fourth_order_on_a_linear_ode():
+    """explicit.rs:143-170: the oracle's LSERK4 coefficient table (the one the
+    product's stage-time table in sources.py matches exactly) integrates the
+    rotation dy/dt = [[0, -w], [w, 0]] y, w = 1.3, to T = 1.7 at fourth order:
+    halving the step from T/20 to T/40 cuts the error more than 12-fold."""
+    from rapidfem_b200 import sources as S
+
+    a, b = R.lserk_coeffs()
+    assert np.array_equal(a, S.LSERK_A) and np.array_equal(b, S.LSERK_B)
+    w, t_end = 1.3, 1.7
+    amat = np.array([[0.0, -w], [w, 0.0]])
+
+    def err(nsteps):
+        dt = t_end / nsteps
+        y, p = np.array([1.0, 0.4]), np.zeros(2)
+        for _ in range(nsteps):
+            for s in range(5):
+                p = a[s] * p + dt * (amat @ y)
+                y = y + b[s] * p
+        c, sn = np.cos(w * t_end), np.sin(w * t_end)
+        return float(np.linalg.norm(y - [c - 0.4 * sn, sn + 0.4 * c]))
+
+    assert err(20) / err(40) > 12.0
+
+
+def test_etd_step_matches_analytic_linear_ode():
+    """propagator.rs:536-559: dy/dt = A y + b with A the rotation (w = 1.3),
+    b = (0.4, -0.7), y0 = (1, 0.5), h = 0.6: the augmented exponential
+    exp(h [[A, b], [0, 0]]) [y0; 1] (the oracle's dense Krylov, m = 8 >= 3,
+    exact) gives exp(hA)(y0 + A^-1 b) - A^-1 b to 1e-12."""
+    w, h = 1.3, 0.6
+    amat = np.array([[0.0, -w], [w, 0.0]])
+    b, y0 = np.array([0.4, -0.7]), np.array([1.0, 0.5])
+    aug = np.zeros((3, 3))
+    aug[:2, :2], aug[:2, 2] = amat, b
+    got, _ = R.expmv_dense(aug, np.array([y0[0], y0[1], 1.0]), h, 8, 0.0)
+    ainv_b = np.array([b[1] / w, -b[0] / w])
+    c, s = np.cos(w * h), np.sin(w * h)
+    sh = y0 + ainv_b
+    want = np.array([c * sh[0] - s * sh[1], s * sh[0] + c * sh[1]]) - ainv_b
+    assert np.max(np.abs(got[:2] - want)) < 1e-12 and abs(got[2] - 1.0) < 1e-12
