@@ -242,3 +242,23 @@ def test_etd_step_matches_analytic_linear_ode():
     sh = y0 + ainv_b
     want = np.array([c * sh[0] - s * sh[1], s * sh[0] + c * sh[1]]) - ainv_b
     assert np.max(np.abs(got[:2] - want)) < 1e-12 and abs(got[2] - 1.0) < 1e-12
+
+
+def test_kcl_orders_on_the_dg_operator():
+    """explicit_adaptive.rs:160-217 (fourth order; the embedded error third
+    order), restated on the DG operator (2^3 box, N = 2, upwind) with the
+    exact step exp(hA) y from the oracle's Krylov: halving h = 0.1 / rho cuts
+    the one-step error of the KCL RK4(3)5 step by about 2^5 (> 24) and the
+    embedded error estimate by about 2^4 (> 12, the reference's bound 10)."""
+    nodes, tets = R.box_mesh(2, 2, 2)
+    orc = R.Operator(nodes, tets, 2, 1.0)
+    rho, _ = orc.power_rho(40)
+    y = np.sin(0.3 + 0.017 * np.arange(orc.n_dof))
+    step_err, est = [], []
+    for h in (0.1 / rho, 0.05 / rho):
+        yk, e = orc.kcl_step(y, h)
+        exact, _ = orc.expmv(y, h, 40, 0.0)
+        step_err.append(np.linalg.norm(yk - exact))
+        est.append(np.linalg.norm(e))
+    assert step_err[0] / step_err[1] > 24.0
+    assert est[0] / est[1] > 12.0
